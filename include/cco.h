@@ -1,0 +1,155 @@
+/*
+ * cco.h - C ABI of the B200-native collective-coordinate hot path.
+ *
+ * Plain pointers and sizes only. Every function returns an int status
+ * (CCO_OK = 0); per-lane outcomes are written as the reference's status
+ * codes 0..7 into caller-provided int64 arrays. Array arguments documented
+ * "device" are CUDA device pointers on the problem's device; "host" are
+ * ordinary host pointers. Streams are cudaStream_t passed as void*
+ * (NULL = the legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside sdawley1/xla-cco):
+ *   cco_problem_create   <- make_stealthy_energy          src/xla_cco/energy.py:361-414
+ *   cco_energy_grad      <- StealthyEnergy.value_grad_density / value_and_grad /
+ *                           __call__ (trig path)         src/xla_cco/energy.py:186-225,301-324
+ *                           and collective_density        src/xla_cco/energy.py:327-358
+ *   cco_relax_descent    <- relax(energy, s0, DescentSettings, chunk_iters)
+ *                                                         src/xla_cco/minimize/__init__.py:102-151
+ *                                                         src/xla_cco/minimize/descent.py:121-209
+ *   cco_relax_lbfgs      <- relax(energy, s0, LBFGSSettings, chunk_iters)
+ *                                                         src/xla_cco/minimize/lbfgs.py:163-350
+ *   cco_device_count     <- require_gpu                  src/xla_cco/_device.py:137-142
+ * The JAX FFI handlers a maintainer would register over these entry points
+ * are described in INTEGRATION.md.
+ */
+#ifndef CCO_H
+#define CCO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCO_ABI_VERSION 1
+
+/* return codes */
+#define CCO_OK 0
+#define CCO_ERR_ARG 1        /* bad argument (Python: ValueError / TypeError)      */
+#define CCO_ERR_OOM 2        /* device allocation failed                          */
+#define CCO_ERR_ADMISSION 3  /* request refused by the HBM admission budget       */
+#define CCO_ERR_DEVICE 4     /* CUDA error (Python: RuntimeError)                 */
+#define CCO_ERR_TIMEOUT 5    /* a bounded wait ran out                            */
+#define CCO_ERR_ROUNDS 6     /* relax did not finish within the round bound       */
+#define CCO_ERR_NODEVICE 7   /* no CUDA device visible (Python: RuntimeError)     */
+
+/* per-lane status codes (src/xla_cco/minimize/result.py:35-42) */
+#define CCO_STATUS_RUNNING 0
+#define CCO_STATUS_ENERGY_TOL 1
+#define CCO_STATUS_STEP_FLOOR 2
+#define CCO_STATUS_BUDGET 3
+#define CCO_STATUS_STAGNATED 4
+#define CCO_STATUS_LINESEARCH_FAIL 5
+#define CCO_STATUS_GRAD_TOL 6
+#define CCO_STATUS_DRIFT 7
+
+typedef struct cco_problem cco_problem;
+
+/* Library / device queries. */
+int cco_abi_version(void);
+const char* cco_error_string(int code);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* cco_last_error(void);
+int cco_device_count(int* n_devices);
+
+/*
+ * A problem is one energy: the integer k-set (M rows of d int32, any order,
+ * no all-zero row), per-row weights and the box volume, for N particles in
+ * d = 1, 2 or 3 dimensions. It is uploaded once to `device` and reused by
+ * every evaluation and relaxation. Outputs indexed by k use the caller's row
+ * order. Host pointers.
+ */
+int cco_problem_create(int device, int d, int n_particles, int m,
+                       const int32_t* n_vectors, const double* weights,
+                       double volume, cco_problem** out);
+int cco_problem_destroy(cco_problem* p);
+/* Sizes of the device k-set layout (runs split into pass-1/pass-2 segments). */
+int cco_problem_info(const cco_problem* p, int* d, int* n_particles, int* m,
+                     int* n_seg1, int* n_seg2, int* table_rows);
+
+/*
+ * Energy, gradient and collective density of `batch` configurations.
+ *   s      device [batch][N][d] fractional positions
+ *   phi    device [batch]        Phi = (1/V) sum_k w_k |rho_k|^2
+ *   grad   device [batch][N][d]  dPhi/ds (NULL: energy and density only)
+ *   rho_re, rho_im device [batch][M] (NULL: not returned)
+ * Deterministic: the same inputs give the same bits.
+ */
+int cco_energy_grad(cco_problem* p, void* stream, int batch, const double* s,
+                    double* phi, double* grad, double* rho_re, double* rho_im);
+
+/* Minimizer settings: same fields and meaning as the reference's settings. */
+typedef struct {
+  double step_init;    /* 1e-3  */
+  double step_min;     /* 1e-15 */
+  double shrink;       /* 0.5   */
+  double grow;         /* 1.0   */
+  double rel_tol;      /* 0.01  */
+  int64_t max_evals;   /* 10000 */
+  double energy_tol;   /* 0     */
+  int64_t record_every;
+  int64_t max_records;
+} cco_descent_settings;
+
+#define CCO_MAX_RESCALES 8
+typedef struct {
+  int64_t memory;                      /* 100 */
+  int32_t n_rescales;                  /* 3   */
+  int32_t pad_;
+  double rescales[CCO_MAX_RESCALES];   /* 1e4, 1, 1e-2 */
+  int64_t max_evals_per_pass;          /* 500000 */
+  double energy_tol;                   /* 0 */
+  double grad_tol;                     /* 0 */
+  int64_t stagnation_patience;         /* 50 */
+  int64_t max_linesearch_steps;        /* 30 */
+  int64_t record_every;
+  int64_t max_records;
+} cco_lbfgs_settings;
+
+/* Outputs of a relaxation: device arrays with a leading lane axis. */
+typedef struct {
+  double* s;            /* [B][N][d] final positions wrapped into [0, 1) */
+  double* energy;       /* [B] */
+  double* grad_norm;    /* [B] */
+  int64_t* n_evals;     /* [B] reference counting (descent: 2 per iteration) */
+  int64_t* n_iters;     /* [B] */
+  int64_t* status;      /* [B] CCO_STATUS_* */
+  /* trajectory (all NULL when recording is off; capacity max_records rows) */
+  double* traj_s;       /* [B][max_records][N][d] wrapped */
+  double* traj_energy;  /* [B][max_records] */
+  double* traj_step;    /* [B][max_records] */
+  int64_t* traj_iteration; /* [B][max_records] */
+  int64_t* traj_count;  /* [B] */
+  int64_t ticks;        /* out: device ticks (one energy evaluation per running lane each) */
+} cco_relax_out;
+
+/*
+ * Batched relaxation of `batch` configurations s0 (device [batch][N][d]).
+ * Each lane runs its own state machine on the device; finished lanes are
+ * frozen and skipped (on-device lane compaction). Results do not depend on
+ * `chunk_iters`, which only sets how many device ticks run between host
+ * completion checks. Returns CCO_ERR_ROUNDS if the reference's round bound
+ * is exceeded.
+ */
+int cco_relax_descent(cco_problem* p, void* stream, int batch, const double* s0,
+                      const cco_descent_settings* settings, int chunk_iters,
+                      cco_relax_out* out);
+int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const double* s0,
+                    const cco_lbfgs_settings* settings, int chunk_iters,
+                    cco_relax_out* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CCO_H */

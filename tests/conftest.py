@@ -1,0 +1,63 @@
+"""Shared test configuration.
+
+RNG policy (as the reference, tests/conftest.py:7-8 there): every random
+input uses an explicit seed through ``np.random.default_rng(seed)``.
+
+Markers: ``gpu`` tests run the CUDA kernels through the C ABI and need a
+B200; everything else runs on the CPU (oracle vs golden vectors, host logic,
+library loading and exports).
+"""
+
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+for p in (ROOT / "xla-cco_b200", ROOT / "oracle", ROOT / "tests"):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+GOLDEN = ROOT / "tests" / "golden"
+
+# tolerances (values and rationale follow the reference's tests/tolerances.py)
+RTOL_KERNEL_E = 1e-12       # energy vs FP64 direct sum
+RTOL_KERNEL_F = 1e-10       # forces vs FP64 direct sum (cancellation costs ~2 digits)
+C_E = 4.0                   # absolute energy floor C_E eps sqrt(N M E) for near-zero Phi
+ATOL_DESCENT_ITERATE = 1e-14
+ATOL_VMAP_S = 1e-12
+RTOL_VMAP_E = 1e-9
+RTOL_MD_CXX_PHI = 1e-8
+
+
+@pytest.fixture(scope="session")
+def golden():
+    """(arrays, meta) of tests/golden/golden.{npz,json}."""
+    with np.load(GOLDEN / "golden.npz") as z:
+        arrays = {k: np.asarray(z[k]) for k in z.files}
+    meta = json.loads((GOLDEN / "golden.json").read_text())
+    return arrays, meta
+
+
+@pytest.fixture
+def poisson_configs():
+    """Factory ``(seed, b, n, d) -> (b, n, d)`` uniform fractional positions."""
+
+    def make(seed: int, b: int, n: int, d: int) -> np.ndarray:
+        return np.random.default_rng(seed).uniform(size=(b, n, d))
+
+    return make
+
+
+def energy_atol(n: int, m: int, e: float) -> float:
+    """C_E eps sqrt(N M E): cancellation floor of M unit-weight terms."""
+    return C_E * np.finfo(float).eps * np.sqrt(n * m * max(e, 0.0))
+
+
+def pytest_collection_modifyitems(config, items):
+    """GPU tests fail loudly (never skip) if libcco.so is missing on a GPU box."""
+    return None

@@ -1,0 +1,195 @@
+"""Energy / gradient / density kernel (sm_100a) vs the FP64 oracle and golden data.
+
+Tolerances follow the reference (tests/tolerances.py there): energy 1e-12
+relative with the absolute floor C_E eps sqrt(N M E); Cartesian forces 1e-10
+relative to max|F|. Mirrors tests/unit/test_energy.py of the reference.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import RTOL_KERNEL_E, RTOL_KERNEL_F, RTOL_MD_CXX_PHI, energy_atol
+from xla_cco import _native
+from xla_cco.box import Box, cubic_box
+from xla_cco.energy import StealthyEnergy, collective_density, make_stealthy_energy
+from xla_cco.kvectors import enumerate_kvectors, k_outer_from_ka, ka_from_chi
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(n, d, chi=None, k2=None):
+    box = cubic_box(n, d)
+    if k2 is None:
+        k2 = k_outer_from_ka(ka_from_chi(chi, 0.05, d), 0.05, d)
+    ks = enumerate_kvectors(box.basis, 0.0, k2)
+    return box, ks, make_stealthy_energy(box, ks)
+
+
+def test_library_loaded_and_gpu_visible():
+    assert _native.load() is not None
+    assert _native.device_count() >= 1
+
+
+def test_energy_forces_vs_reference_oracle_golden(golden):
+    arrays, meta = golden
+    for c in meta["energy_cases"]:
+        i = c["i"]
+        s, n, basis = arrays[f"energy{i}_s"], arrays[f"energy{i}_n"], arrays[f"energy{i}_basis"]
+        box = Box(basis)
+        ks = enumerate_kvectors(basis, 0.0, c["k_outer"])
+        np.testing.assert_array_equal(ks.n, n)
+        en = make_stealthy_energy(box, ks)
+        val, grad = en.value_and_grad(s)
+        atol = energy_atol(c["n"], n.shape[0], c["phi"])
+        np.testing.assert_allclose(val, c["phi"], rtol=RTOL_KERNEL_E, atol=atol)
+        ref = arrays[f"energy{i}_forces"]
+        got = box.cartesian_forces(grad)
+        np.testing.assert_allclose(got, ref, rtol=RTOL_KERNEL_F, atol=RTOL_KERNEL_F * np.abs(ref).max())
+
+
+def test_cpp_golden_energies(golden):
+    arrays, meta = golden
+    basis = arrays["cxx_basis"]
+    box = Box(basis)
+    en = make_stealthy_energy(box, enumerate_kvectors(basis, 0.0, meta["cxx"]["K"]))
+    phi, _, _, _ = en.evaluate(arrays["cxx_s"], want_grad=False)
+    rel = np.abs(phi - arrays["cxx_phi"]) / arrays["cxx_phi"]
+    assert rel.max() <= RTOL_MD_CXX_PHI
+    assert rel.max() < 1e-12
+
+
+@pytest.mark.parametrize(
+    "n,d,chi,b",
+    [(100, 3, 0.05, 5), (1000, 2, 0.40, 3), (4000, 3, 0.45, 1), (8000, 1, 0.49, 1),
+     (300, 1, 0.2, 2), (777, 2, 0.13, 2), (500, 3, 0.3, 2)],
+)  # fmt: skip
+def test_baseline_sizes_vs_c_oracle(n, d, chi, b, poisson_configs):
+    box, ks, en = _system(n, d, chi)
+    s = poisson_configs(n + d, b, n, d)
+    phi, grad, re, im = en.evaluate(s, want_grad=True, want_rho=True)
+    m = ks.n.shape[0]
+    for i in range(b):
+        pr, gr, rr, ir = oracle.energy_grad(s[i], ks.n, ks.weights, box.volume, want_rho=True)
+        np.testing.assert_allclose(phi[i], pr, rtol=RTOL_KERNEL_E, atol=energy_atol(n, m, pr))
+        np.testing.assert_allclose(grad[i], gr, rtol=RTOL_KERNEL_F, atol=RTOL_KERNEL_F * np.abs(gr).max())
+        tol = 1e-12 * np.sqrt(n) * 8
+        np.testing.assert_allclose(re[i, :m], rr, rtol=0, atol=tol)
+        np.testing.assert_allclose(im[i, :m], ir, rtol=0, atol=tol)
+
+
+def test_unwrapped_positions_and_sheared_box():
+    basis = np.array([[2.0, 0.0, 0.0], [0.7, 1.5, 0.0], [0.3, -0.4, 1.8]])
+    box = Box(basis)
+    ks = enumerate_kvectors(basis, 0.5, 7.0)
+    en = make_stealthy_energy(box, ks)
+    s = np.random.default_rng(3).uniform(-2.0, 3.0, size=(40, 3))
+    val, grad = en.value_and_grad(s)
+    pr, gr = oracle.energy_grad(s, ks.n, ks.weights, box.volume)
+    np.testing.assert_allclose(val, pr, rtol=RTOL_KERNEL_E, atol=energy_atol(40, ks.n.shape[0], pr))
+    np.testing.assert_allclose(grad, gr, rtol=RTOL_KERNEL_F, atol=RTOL_KERNEL_F * np.abs(gr).max())
+
+
+def test_value_grad_density_padding_and_determinism(poisson_configs):
+    box, ks, _ = _system(64, 2, k2=4.5)
+    en = make_stealthy_energy(box, ks, pad_to=64)
+    assert en.n_vectors.shape[0] > ks.n.shape[0]
+    s = poisson_configs(5, 1, 64, 2)[0]
+    v1, g1, re1, im1 = en.value_grad_density(s)
+    v2, g2, re2, im2 = en.value_grad_density(s)
+    assert v1 == v2
+    for a, b in ((g1, g2), (re1, re2), (im1, im2)):
+        np.testing.assert_array_equal(a, b)
+    pad = en.weights == 0.0
+    assert np.all(re1[pad] == 64.0) and np.all(im1[pad] == 0.0)
+    va, ga = en.value_and_grad(s)
+    assert va == v1
+    np.testing.assert_array_equal(ga, g1)
+    assert en(s) == v1
+    rc, ic = collective_density(s, en.n_vectors)
+    np.testing.assert_allclose(rc, re1, atol=1e-12)
+    np.testing.assert_allclose(ic, im1, atol=1e-12)
+
+
+def test_batched_equals_single_bitwise(poisson_configs):
+    _, _, en = _system(200, 3, 0.2)
+    s = poisson_configs(9, 6, 200, 3)
+    phi, grad, _, _ = en.evaluate(s)
+    for i in range(6):
+        v, g = en.value_and_grad(s[i])
+        assert v == phi[i]
+        np.testing.assert_array_equal(g, grad[i])
+
+
+@pytest.mark.parametrize("dim,m", [(1, 6), (2, 4), (3, 3)])
+def test_lattice_ground_state(dim, m):
+    n = m**dim
+    grid = np.stack(np.meshgrid(*[np.arange(m)] * dim, indexing="ij"), -1)
+    s = grid.reshape(-1, dim).astype(np.float64) / m
+    box = cubic_box(n, dim)
+    k_out = 0.999 * 2.0 * np.pi * m / float(box.basis[0, 0])
+    en = make_stealthy_energy(box, enumerate_kvectors(box.basis, 0.0, k_out))
+    assert en(s) <= 1e-26
+
+
+def test_single_particle_energy():
+    box = cubic_box(1, 2)
+    ks = enumerate_kvectors(box.basis, 0.0, 9.0)
+    en = make_stealthy_energy(box, ks)
+    np.testing.assert_allclose(en(np.array([[0.37, 0.81]])), ks.weights.sum(), rtol=RTOL_KERNEL_E)
+
+
+def test_gradient_central_difference():
+    box, ks, en = _system(6, 2, k2=4.0)
+    s = np.random.default_rng(5).uniform(size=(6, 2))
+    _, grad = en.value_and_grad(s)
+    h = 1e-6
+    fd = np.zeros_like(s)
+    for i in range(6):
+        for c in range(2):
+            sp, sm = s.copy(), s.copy()
+            sp[i, c] += h
+            sm[i, c] -= h
+            fd[i, c] = (en(sp) - en(sm)) / (2 * h)
+    np.testing.assert_allclose(grad, fd, atol=1e-6 * max(1.0, np.abs(fd).max()))
+
+
+def test_invariances_translation_permutation_gradsum(poisson_configs):
+    box, ks, en = _system(300, 2, 0.3)
+    s = poisson_configs(2, 1, 300, 2)[0]
+    v, g = en.value_and_grad(s)
+    vt = en(s + np.array([0.123, -0.456]))
+    np.testing.assert_allclose(vt, v, rtol=1e-11)
+    perm = np.random.default_rng(0).permutation(300)
+    vp, gp = en.value_and_grad(s[perm])
+    np.testing.assert_allclose(vp, v, rtol=1e-12)
+    np.testing.assert_allclose(gp, g[perm], rtol=1e-9, atol=1e-10 * np.abs(g).max())
+    np.testing.assert_allclose(en(s + 3.0), v, rtol=1e-10)  # periodic images
+    assert np.all(np.abs(g.sum(0)) <= 1e-9 * np.abs(g).max() * 300)
+
+
+def test_rejects_bad_input():
+    box, ks, en = _system(4, 2, k2=4.0)
+    with pytest.raises(TypeError):
+        en(np.zeros((4, 2), np.float32))
+    with pytest.raises(TypeError):
+        en.value_and_grad(np.zeros((4, 2), np.float32))
+    with pytest.raises(ValueError):
+        StealthyEnergy(np.array([[0.5, 1.0]]), np.ones(1), np.float64(4.0))
+    with pytest.raises(ValueError, match="empty"):
+        make_stealthy_energy(box, enumerate_kvectors(box.basis, 0.0, 1e-3))
+
+
+def test_torch_device_path_matches_host(poisson_configs):
+    import torch
+
+    _, _, en = _system(1000, 2, 0.4)
+    s = poisson_configs(1, 4, 1000, 2)
+    phi_h, g_h, _, _ = en.evaluate(s)
+    st = torch.from_numpy(s).cuda()
+    phi_d, g_d, _, _ = en.evaluate(st)
+    assert phi_d.is_cuda and g_d.is_cuda
+    np.testing.assert_array_equal(phi_d.cpu().numpy(), phi_h)
+    np.testing.assert_array_equal(g_d.cpu().numpy(), g_h)

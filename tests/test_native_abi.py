@@ -1,0 +1,69 @@
+"""The C-ABI library loads and exports every symbol include/cco.h declares.
+
+Runs without a GPU: only argument validation and device queries are called
+(no compute). The Python binding's signature table must match the header.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from xla_cco import _native
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "cco.h"
+
+
+def declared_functions() -> list[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(cco_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for must in ("cco_problem_create", "cco_energy_grad", "cco_relax_descent", "cco_relax_lbfgs",
+                 "cco_device_count", "cco_last_error"):  # fmt: skip
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _native.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), f"libcco.so does not export {name}"
+        assert name in _native.SIGNATURES, f"binding lacks {name}"
+
+
+def test_struct_layouts_match_header():
+    assert ctypes.sizeof(_native.DescentSettingsC) == 9 * 8
+    assert ctypes.sizeof(_native.LBFGSSettingsC) == 8 + 8 + 8 * 8 + 7 * 8
+    assert ctypes.sizeof(_native.RelaxOutC) == 12 * 8
+
+
+def test_abi_version_and_errors():
+    lib = _native.load()
+    assert lib.cco_abi_version() == 1
+    assert lib.cco_error_string(_native.CCO_ERR_ROUNDS).decode().startswith("relax did not finish")
+    assert lib.cco_energy_grad(None, None, 1, None, None, None, None, None) == _native.CCO_ERR_ARG
+    assert b"null" in lib.cco_last_error()
+
+
+def test_problem_create_validates_before_touching_a_device():
+    lib = _native.load()
+    out = ctypes.c_void_p()
+    n = (ctypes.c_int32 * 2)(1, 0)
+    w = (ctypes.c_double * 1)(1.0)
+    assert lib.cco_problem_create(0, 4, 10, 1, n, w, 10.0, ctypes.byref(out)) == _native.CCO_ERR_ARG
+    assert lib.cco_problem_create(0, 2, 10, 0, n, w, 10.0, ctypes.byref(out)) == _native.CCO_ERR_ARG
+    assert b"empty" in lib.cco_last_error()
+    assert lib.cco_problem_create(0, 2, 10, 1, n, w, -1.0, ctypes.byref(out)) == _native.CCO_ERR_ARG
+
+
+def test_no_device_is_reported_not_hidden():
+    if _native.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    with pytest.raises(RuntimeError, match="needs a CUDA device"):
+        _native.require_gpu()

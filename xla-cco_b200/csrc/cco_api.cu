@@ -1,0 +1,715 @@
+// C ABI of libcco: problems, evaluation and the batched relax drivers.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cco_internal.cuh"
+#include "cco_opt.cuh"
+
+using namespace cco;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) return fail(CCO_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+  return fail(CCO_ERR_DEVICE, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CCO_CUDA(call)                                 \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+struct cco_problem {
+  int device = 0;
+  int d = 0, N = 0, M = 0;
+  ProbDev host{};         // pointers are device pointers
+  ProbDev* dev = nullptr; // device copy
+  SegHdr* seg1 = nullptr;
+  SegHdr* seg2 = nullptr;
+  double* w_run = nullptr;
+  int* run2ref = nullptr;
+  size_t smem1 = 0, smem2 = 0;
+};
+
+namespace {
+
+// ----------------------------------------------------------- problem build
+struct Digits {
+  int nlev, base;
+  int nent[kMaxLevels];
+};
+
+// Digit tables for |n| <= R on one axis: 1 level (z^0..z^R) for small R,
+// otherwise 2 or 3 levels of base b with b^levels > R. Level 0 always holds
+// z^0..z^(b-1); the run axis needs z^1 there, so its base is >= 2.
+Digits choose_digits(int R, bool run_axis) {
+  Digits g{};
+  const int nv = R + 1;
+  if (nv <= 16) {
+    g.nlev = 1;
+    g.base = std::max(nv, run_axis ? 2 : 1);
+    g.nent[0] = g.base;
+    return g;
+  }
+  g.nlev = nv <= 1024 ? 2 : 3;
+  g.base = (int)std::ceil(std::pow((double)nv, 1.0 / g.nlev));
+  while ((g.nlev == 2 ? g.base * g.base : g.base * g.base * g.base) < nv) ++g.base;
+  int scale = 1;
+  for (int l = 0; l < g.nlev - 1; ++l) {
+    g.nent[l] = g.base;
+    scale *= g.base;
+  }
+  g.nent[g.nlev - 1] = R / scale + 1;
+  return g;
+}
+
+int pack_digits(int v, const Digits& g) {
+  const int neg = v < 0;
+  int a = v < 0 ? -v : v;
+  int out = 0;
+  for (int l = 0; l < g.nlev; ++l) {
+    int dl;
+    if (l == g.nlev - 1) dl = a;
+    else {
+      dl = a % g.base;
+      a /= g.base;
+    }
+    out |= (dl & 255) << (8 * l);
+  }
+  return out | (neg << 24);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cco_abi_version(void) { return CCO_ABI_VERSION; }
+
+const char* cco_error_string(int code) {
+  switch (code) {
+    case CCO_OK: return "ok";
+    case CCO_ERR_ARG: return "invalid argument";
+    case CCO_ERR_OOM: return "out of device memory";
+    case CCO_ERR_ADMISSION: return "refused by the HBM admission budget";
+    case CCO_ERR_DEVICE: return "CUDA error";
+    case CCO_ERR_TIMEOUT: return "timed out";
+    case CCO_ERR_ROUNDS: return "relax did not finish within the round bound";
+    case CCO_ERR_NODEVICE: return "no CUDA device";
+    default: return "unknown error";
+  }
+}
+
+const char* cco_last_error(void) { return g_last_error.c_str(); }
+
+int cco_device_count(int* n_devices) {
+  if (!n_devices) return fail(CCO_ERR_ARG, "n_devices is null");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    *n_devices = 0;
+    cudaGetLastError();
+    return fail(CCO_ERR_NODEVICE, "no CUDA device visible (%s)",
+                e == cudaSuccess ? "count 0" : cudaGetErrorString(e));
+  }
+  *n_devices = n;
+  return CCO_OK;
+}
+
+int cco_problem_create(int device, int d, int n_particles, int m, const int32_t* n_vectors,
+                       const double* weights, double volume, cco_problem** out) {
+  if (!out) return fail(CCO_ERR_ARG, "out is null");
+  *out = nullptr;
+  if (d < 1 || d > 3) return fail(CCO_ERR_ARG, "d must be 1, 2 or 3, got %d", d);
+  if (n_particles < 1) return fail(CCO_ERR_ARG, "n_particles must be >= 1");
+  if (m < 1) return fail(CCO_ERR_ARG, "empty k-set: no k-vectors in the shell");
+  if (!n_vectors || !weights) return fail(CCO_ERR_ARG, "null k-set arrays");
+  if (!(volume > 0.0) || !std::isfinite(volume)) return fail(CCO_ERR_ARG, "volume must be finite and > 0");
+  int ndev = 0;
+  if (cco_device_count(&ndev) != CCO_OK) return CCO_ERR_NODEVICE;
+  if (device < 0 || device >= ndev) return fail(CCO_ERR_ARG, "device %d out of range", device);
+
+  // validate rows
+  std::vector<int> R(3, 0);
+  for (int k = 0; k < m; ++k) {
+    bool nz = false;
+    for (int a = 0; a < d; ++a) {
+      const int v = n_vectors[(size_t)k * d + a];
+      if (v < -65535 || v > 65535) return fail(CCO_ERR_ARG, "|n| too large at row %d", k);
+      R[a] = std::max(R[a], std::abs(v));
+      nz |= v != 0;
+    }
+    if (!nz) return fail(CCO_ERR_ARG, "row %d is the zero vector (padding rows are handled by the caller)", k);
+    if (!std::isfinite(weights[k])) return fail(CCO_ERR_ARG, "non-finite weight at row %d", k);
+  }
+  // run order: prefix lexicographic, then the last axis ascending
+  std::vector<int> order(m);
+  for (int k = 0; k < m; ++k) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    for (int a = 0; a < d; ++a) {
+      const int u = n_vectors[(size_t)x * d + a], v = n_vectors[(size_t)y * d + a];
+      if (u != v) return u < v;
+    }
+    return false;
+  });
+  for (int k = 1; k < m; ++k) {
+    bool same = true;
+    for (int a = 0; a < d; ++a)
+      same &= n_vectors[(size_t)order[k] * d + a] == n_vectors[(size_t)order[k - 1] * d + a];
+    if (same) return fail(CCO_ERR_ARG, "duplicate k row (rows %d and %d)", order[k - 1], order[k]);
+  }
+  Digits dg[3];
+  for (int a = 0; a < d; ++a) dg[a] = choose_digits(R[a], a == d - 1);
+
+  ProbDev P{};
+  P.d = d;
+  P.N = n_particles;
+  P.M = m;
+  int row = 0;
+  for (int a = 0; a < 3; ++a) {
+    if (a < d) {
+      P.nlev[a] = dg[a].nlev;
+      P.base[a] = dg[a].base;
+      for (int l = 0; l < kMaxLevels; ++l) {
+        P.nent[a][l] = l < dg[a].nlev ? dg[a].nent[l] : 0;
+        P.row[a][l] = row;
+        if (l < dg[a].nlev) row += dg[a].nent[l];
+      }
+    } else {
+      P.nlev[a] = 1;
+      P.base[a] = 1;
+    }
+  }
+  P.nrows = row;
+  P.ntile1 = (n_particles + kPass1Tile - 1) / kPass1Tile;
+  P.ntile2 = (n_particles + kPass2Tile - 1) / kPass2Tile;
+  P.vol = volume;
+  P.gpref = (2.0 * (2.0 * M_PI)) / volume;
+
+  // runs -> segments
+  std::vector<SegHdr> s1, s2;
+  auto emit = [&](std::vector<SegHdr>& dst, int kstart, int len, int maxlen) {
+    for (int off = 0; off < len; off += maxlen) {
+      SegHdr h{};
+      h.kstart = kstart + off;
+      h.len = std::min(maxlen, len - off);
+      const int* nv = n_vectors + (size_t)order[h.kstart] * d;
+      for (int a = 0; a < 3; ++a) {
+        if (a < d) {
+          h.n[a] = nv[a];
+          h.dig[a] = pack_digits(nv[a], dg[a]);
+        }
+      }
+      dst.push_back(h);
+    }
+  };
+  int start = 0;
+  for (int k = 1; k <= m; ++k) {
+    bool brk = (k == m);
+    if (!brk) {
+      const int* p = n_vectors + (size_t)order[k - 1] * d;
+      const int* c = n_vectors + (size_t)order[k] * d;
+      for (int a = 0; a < d - 1; ++a) brk |= p[a] != c[a];
+      brk |= c[d - 1] != p[d - 1] + 1;
+    }
+    if (brk) {
+      emit(s1, start, k - start, kSeg1Len);
+      emit(s2, start, k - start, kSeg2Len);
+      start = k;
+    }
+  }
+  // longest pass-1 segments first: a warp's threads then share a trip count
+  std::stable_sort(s1.begin(), s1.end(), [](const SegHdr& x, const SegHdr& y) { return x.len > y.len; });
+  P.nseg1 = (int)s1.size();
+  P.nseg2 = (int)s2.size();
+
+  const size_t smem1 = eval_smem1(P), smem2 = eval_smem2(P);
+  if (smem1 > 220 * 1024 || smem2 > 220 * 1024)
+    return fail(CCO_ERR_ARG, "k-set digit tables too large for shared memory (%d rows)", P.nrows);
+
+  DeviceGuard guard(device);
+  static std::once_flag once;
+  static cudaError_t cfg_err = cudaSuccess;
+  std::call_once(once, [] { cfg_err = eval_configure(); });
+  if (cfg_err != cudaSuccess) return cuda_fail(cfg_err, "eval_configure");
+
+  auto* pr = new cco_problem();
+  pr->device = device;
+  pr->d = d;
+  pr->N = n_particles;
+  pr->M = m;
+  std::vector<double> w_run(m);
+  std::vector<int> r2r(m);
+  for (int k = 0; k < m; ++k) {
+    w_run[k] = weights[order[k]];
+    r2r[k] = order[k];
+  }
+  cudaError_t e = cudaSuccess;
+  e = cudaMalloc(&pr->seg1, s1.size() * sizeof(SegHdr));
+  if (e == cudaSuccess) e = cudaMalloc(&pr->seg2, s2.size() * sizeof(SegHdr));
+  if (e == cudaSuccess) e = cudaMalloc(&pr->w_run, m * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&pr->run2ref, m * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&pr->dev, sizeof(ProbDev));
+  if (e == cudaSuccess) e = cudaMemcpy(pr->seg1, s1.data(), s1.size() * sizeof(SegHdr), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(pr->seg2, s2.data(), s2.size() * sizeof(SegHdr), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(pr->w_run, w_run.data(), m * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(pr->run2ref, r2r.data(), m * sizeof(int), cudaMemcpyHostToDevice);
+  P.seg1 = pr->seg1;
+  P.seg2 = pr->seg2;
+  P.w_run = pr->w_run;
+  P.run2ref = pr->run2ref;
+  if (e == cudaSuccess) e = cudaMemcpy(pr->dev, &P, sizeof(ProbDev), cudaMemcpyHostToDevice);
+  pr->host = P;
+  pr->smem1 = smem1;
+  pr->smem2 = smem2;
+  if (e != cudaSuccess) {
+    cco_problem_destroy(pr);
+    return cuda_fail(e, "cco_problem_create upload");
+  }
+  *out = pr;
+  return CCO_OK;
+}
+
+int cco_problem_destroy(cco_problem* p) {
+  if (!p) return CCO_OK;
+  DeviceGuard guard(p->device);
+  cudaFree(p->seg1);
+  cudaFree(p->seg2);
+  cudaFree(p->w_run);
+  cudaFree(p->run2ref);
+  cudaFree(p->dev);
+  delete p;
+  return CCO_OK;
+}
+
+int cco_problem_info(const cco_problem* p, int* d, int* n_particles, int* m, int* n_seg1,
+                     int* n_seg2, int* table_rows) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (d) *d = p->d;
+  if (n_particles) *n_particles = p->N;
+  if (m) *m = p->M;
+  if (n_seg1) *n_seg1 = p->host.nseg1;
+  if (n_seg2) *n_seg2 = p->host.nseg2;
+  if (table_rows) *table_rows = p->host.nrows;
+  return CCO_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ eval workspace
+namespace {
+
+__global__ void k_make_lanes(EvalLane* lanes, EvalItem* it1, EvalItem* it2, int B, int nt1,
+                             int nt2, int total, const double* s, size_t s_stride, double* f,
+                             size_t f_stride, double* g, size_t g_stride, double2* rho,
+                             double2* rhow, double2* part, int M, const int64_t* status,
+                             size_t status_stride) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    if (i < B) {
+      EvalLane L;
+      L.s = s + (size_t)i * s_stride;
+      L.f = f + (size_t)i * f_stride;
+      L.g = g ? g + (size_t)i * g_stride : nullptr;
+      L.rho = rho + (size_t)i * M;
+      L.rhow = rhow + (size_t)i * M;
+      L.part = part + (size_t)i * nt1 * M;
+      L.status = status ? status + (size_t)i * status_stride : nullptr;
+      L.prob = 0;
+      L.pad_ = 0;
+      lanes[i] = L;
+    }
+    const int j = i - B;
+    if (j >= 0) {
+      if (j < B * nt1) it1[j] = EvalItem{j / nt1, j % nt1};
+      if (j < B * nt2) it2[j] = EvalItem{j / nt2, j % nt2};
+    }
+  }
+}
+
+// Device buffers of one batched evaluation: densities, partials and the plan.
+struct EvalWS {
+  EvalLane* lanes = nullptr;
+  EvalItem* it1 = nullptr;
+  EvalItem* it2 = nullptr;
+  double2* rho = nullptr;
+  double2* rhow = nullptr;
+  double2* part = nullptr;
+  EvalPlan plan{};
+
+  cudaError_t alloc(const cco_problem* p, int B, cudaStream_t st) {
+    const int M = p->M, nt1 = p->host.ntile1, nt2 = p->host.ntile2;
+    cudaError_t e = cudaMallocAsync(&lanes, sizeof(EvalLane) * B, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&it1, sizeof(EvalItem) * (size_t)B * nt1, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&it2, sizeof(EvalItem) * (size_t)B * nt2, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&rho, sizeof(double2) * (size_t)B * M, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&rhow, sizeof(double2) * (size_t)B * M, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&part, sizeof(double2) * (size_t)B * nt1 * M, st);
+    return e;
+  }
+  cudaError_t build(const cco_problem* p, int B, const double* s, size_t s_stride, double* f,
+                    size_t f_stride, double* g, size_t g_stride, const int64_t* status,
+                    size_t status_stride, cudaStream_t st) {
+    const int nt1 = p->host.ntile1, nt2 = p->host.ntile2;
+    const int total = B * std::max(nt1, nt2) + B;
+    const int blocks = std::min(1024, (total + 255) / 256);
+    k_make_lanes<<<blocks, 256, 0, st>>>(lanes, it1, it2, B, nt1, nt2, total, s, s_stride, f, f_stride,
+                                         g, g_stride, rho, rhow, part, p->M, status,
+                                         status_stride);
+    plan.probs = p->dev;
+    plan.lanes = lanes;
+    plan.items1 = it1;
+    plan.items2 = it2;
+    plan.n_lanes = B;
+    plan.n_items1 = B * nt1;
+    plan.n_items2 = B * nt2;
+    plan.max_d = p->d;
+    plan.smem1 = p->smem1;
+    plan.smem2 = p->smem2;
+    plan.want_grad = g != nullptr;
+    return cudaGetLastError();
+  }
+  void release(cudaStream_t st) {
+    cudaFreeAsync(lanes, st);
+    cudaFreeAsync(it1, st);
+    cudaFreeAsync(it2, st);
+    cudaFreeAsync(rho, st);
+    cudaFreeAsync(rhow, st);
+    cudaFreeAsync(part, st);
+    lanes = nullptr;
+  }
+};
+
+}  // namespace
+
+extern "C" int cco_energy_grad(cco_problem* p, void* stream, int batch, const double* s,
+                               double* phi, double* grad, double* rho_re, double* rho_im) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (batch < 0) return fail(CCO_ERR_ARG, "batch must be >= 0");
+  if (batch == 0) return CCO_OK;
+  if (!s || !phi) return fail(CCO_ERR_ARG, "null s or phi");
+  DeviceGuard guard(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  EvalWS ws;
+  CCO_CUDA(ws.alloc(p, batch, st));
+  const size_t nd = (size_t)p->N * p->d;
+  CCO_CUDA(ws.build(p, batch, s, nd, phi, 1, grad, nd, nullptr, 0, st));
+  CCO_CUDA(eval_launch(ws.plan, st));
+  if (rho_re || rho_im)
+    CCO_CUDA(rho_scatter(ws.rho, p->run2ref, p->M, batch, p->M, rho_re, rho_im, st));
+  ws.release(st);
+  CCO_CUDA(cudaGetLastError());
+  return CCO_OK;
+}
+
+// ------------------------------------------------------------ relax drivers
+namespace {
+
+// Runs ticks (one evaluation + one update per running lane) in captured CUDA
+// graphs of kGraphTicks ticks until no lane is RUNNING or the tick bound is
+// reached. Completion is checked one graph behind so the device never idles
+// on the host.
+constexpr int kGraphTicks = 16;
+
+template <class TickFn>
+int run_ticks(cudaStream_t st, TickFn tick, const int64_t* status, size_t stride, int B,
+              int64_t max_ticks, int64_t* ticks_out) {
+  int* d_count = nullptr;
+  int* h_count = nullptr;
+  CCO_CUDA(cudaMallocAsync(&d_count, 2 * sizeof(int), st));
+  CCO_CUDA(cudaMallocHost(&h_count, 2 * sizeof(int)));
+  cudaEvent_t ev[2];
+  CCO_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+  CCO_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int rc = CCO_OK;
+  // capture kGraphTicks ticks on a side stream ordered after `st`
+  cudaStream_t cap;
+  CCO_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    for (int t = 0; t < kGraphTicks && e == cudaSuccess; ++t) e = tick(cap);
+    cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  int64_t ticks = 0;
+  int launched = 0;
+  bool done = false;
+  while (e == cudaSuccess && !done) {
+    if (ticks >= max_ticks) break;
+    e = cudaGraphLaunch(exec, st);
+    if (e != cudaSuccess) break;
+    ticks += kGraphTicks;
+    const int slot = launched & 1;
+    e = count_running(status, stride, B, d_count + slot, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_count + slot, d_count + slot, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[slot], st);
+    ++launched;
+    if (e == cudaSuccess && launched >= 2) {
+      const int prev = (launched - 2) & 1;
+      e = cudaEventSynchronize(ev[prev]);
+      if (e == cudaSuccess && h_count[prev] == 0) done = true;
+    }
+  }
+  if (e == cudaSuccess && !done) {
+    // drain: the last launch's count
+    if (launched >= 1) {
+      const int last = (launched - 1) & 1;
+      e = cudaEventSynchronize(ev[last]);
+      if (e == cudaSuccess && h_count[last] == 0) done = true;
+    }
+  }
+  if (e != cudaSuccess) rc = cuda_fail(e, "relax ticks");
+  else if (!done) rc = fail(CCO_ERR_ROUNDS, "relax did not finish within the round bound (%lld ticks)", (long long)max_ticks);
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  cudaStreamDestroy(cap);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  cudaFreeAsync(d_count, st);
+  cudaStreamSynchronize(st);
+  cudaFreeHost(h_count);
+  if (ticks_out) *ticks_out = ticks;
+  return rc;
+}
+
+bool out_ok(const cco_relax_out* o) {
+  return o && o->s && o->energy && o->grad_norm && o->n_evals && o->n_iters && o->status;
+}
+
+}  // namespace
+
+extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const double* s0,
+                                 const cco_descent_settings* cfg, int chunk_iters,
+                                 cco_relax_out* out) {
+  if (!p || !cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
+  if (!out_ok(out)) return fail(CCO_ERR_ARG, "incomplete output struct");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  if (cfg->max_evals < 0) return fail(CCO_ERR_ARG, "max_evals must be >= 0");
+  const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
+  if (rec && (!out->traj_s || !out->traj_energy || !out->traj_step || !out->traj_iteration || !out->traj_count))
+    return fail(CCO_ERR_ARG, "trajectory recording needs the traj_* outputs");
+  DeviceGuard guard(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int B = batch;
+  const size_t nd = (size_t)p->N * p->d;
+  DescentArgs a{};
+  a.B = B;
+  a.N = p->N;
+  a.d = p->d;
+  a.nd = (int)nd;
+  a.step_init = cfg->step_init;
+  a.step_min = cfg->step_min;
+  a.shrink = cfg->shrink;
+  a.grow = cfg->grow;
+  a.rel_tol = cfg->rel_tol;
+  a.energy_tol = cfg->energy_tol;
+  a.max_iters = cfg->max_evals / 2;
+  a.rec_every = rec ? cfg->record_every : 1;
+  a.rec_cap = rec ? cfg->max_records : 0;
+  double* vec = nullptr;   // s, g, ps, pg
+  double* sc = nullptr;    // f, step, norm, pf
+  int64_t* ic = nullptr;   // it, n_evals, status
+  int* ph = nullptr;       // phase, nonzero
+  CCO_CUDA(cudaMallocAsync(&vec, sizeof(double) * nd * B * 4, st));
+  CCO_CUDA(cudaMallocAsync(&sc, sizeof(double) * B * 4, st));
+  CCO_CUDA(cudaMallocAsync(&ic, sizeof(int64_t) * B * 3, st));
+  CCO_CUDA(cudaMallocAsync(&ph, sizeof(int) * B * 2, st));
+  a.s = vec;
+  a.g = vec + nd * B;
+  a.ps = vec + 2 * nd * B;
+  double* pg = vec + 3 * nd * B;
+  a.pg = pg;
+  a.f = sc;
+  a.step = sc + B;
+  a.norm = sc + 2 * B;
+  double* pf = sc + 3 * B;
+  a.pf = pf;
+  a.it = ic;
+  a.n_evals = ic + B;
+  a.status = ic + 2 * B;
+  a.phase = ph;
+  a.nonzero = ph + B;
+  if (rec) {
+    a.traj_s = out->traj_s;
+    a.traj_e = out->traj_energy;
+    a.traj_step = out->traj_step;
+    a.traj_it = out->traj_iteration;
+    a.traj_count = out->traj_count;
+  }
+  EvalWS ws;
+  CCO_CUDA(ws.alloc(p, B, st));
+  CCO_CUDA(ws.build(p, B, a.ps, nd, pf, 1, pg, nd, a.status, 1, st));
+  CCO_CUDA(descent_init(a, s0, st));
+  auto tick = [&](cudaStream_t s) -> cudaError_t {
+    cudaError_t e = eval_launch(ws.plan, s);
+    if (e == cudaSuccess) e = descent_update(a, s);
+    return e;
+  };
+  const int64_t max_ticks = 1 + a.max_iters + kGraphTicks;
+  int64_t ticks = 0;
+  int rc = run_ticks(st, tick, a.status, 1, B, max_ticks, &ticks);
+  if (rc == CCO_OK) {
+    cudaError_t e = descent_finalize(a, out->s, out->energy, out->grad_norm, out->n_evals,
+                                     out->n_iters, out->status, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "descent_finalize");
+  }
+  out->ticks = ticks;
+  ws.release(st);
+  cudaFreeAsync(vec, st);
+  cudaFreeAsync(sc, st);
+  cudaFreeAsync(ic, st);
+  cudaFreeAsync(ph, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "relax descent");
+  return rc;
+}
+
+extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const double* s0,
+                               const cco_lbfgs_settings* cfg, int chunk_iters,
+                               cco_relax_out* out) {
+  if (!p || !cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
+  if (!out_ok(out)) return fail(CCO_ERR_ARG, "incomplete output struct");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  if (cfg->n_rescales < 1 || cfg->n_rescales > CCO_MAX_RESCALES)
+    return fail(CCO_ERR_ARG, "need 1..%d rescale passes", CCO_MAX_RESCALES);
+  if (cfg->memory < 1) return fail(CCO_ERR_ARG, "memory must be >= 1");
+  if (cfg->max_linesearch_steps < 1) return fail(CCO_ERR_ARG, "max_linesearch_steps must be >= 1");
+  const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
+  if (rec && (!out->traj_s || !out->traj_energy || !out->traj_step || !out->traj_iteration || !out->traj_count))
+    return fail(CCO_ERR_ARG, "trajectory recording needs the traj_* outputs");
+  DeviceGuard guard(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int B = batch;
+  const size_t nd = (size_t)p->N * p->d;
+  const int m = (int)cfg->memory;
+  LbArgs A{};
+  A.B = B;
+  A.N = p->N;
+  A.d = p->d;
+  A.nd = (int)nd;
+  A.m = m;
+  A.n_pass = cfg->n_rescales;
+  for (int i = 0; i < CCO_MAX_RESCALES; ++i) A.rescales[i] = i < cfg->n_rescales ? cfg->rescales[i] : 1.0;
+  A.energy_tol = cfg->energy_tol;
+  A.grad_tol = cfg->grad_tol;
+  A.budget = cfg->max_evals_per_pass;
+  A.patience = cfg->stagnation_patience;
+  A.max_ls = cfg->max_linesearch_steps;
+  A.rec_every = rec ? cfg->record_every : 1;
+  A.rec_cap = rec ? cfg->max_records : 0;
+  const size_t tri_bytes = lbfgs_update_smem(m);
+  const bool in_smem = tri_bytes <= 200 * 1024;
+  A.smem_tri = in_smem ? tri_bytes : 0;
+  if (in_smem) {
+    static std::mutex mu;
+    static size_t configured = 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (tri_bytes > configured) {
+      CCO_CUDA(lbfgs_configure(200 * 1024));
+      configured = 200 * 1024;
+    }
+  }
+  LbState* stv = nullptr;
+  double* vec = nullptr;   // x, s, g, dir, glo, ps, pg
+  double* hist = nullptr;  // S, Y
+  double* dots = nullptr;  // SY, YY
+  double* pf = nullptr;
+  double* trig = nullptr;
+  CCO_CUDA(cudaMallocAsync(&stv, sizeof(LbState) * B, st));
+  CCO_CUDA(cudaMallocAsync(&vec, sizeof(double) * nd * B * 7, st));
+  CCO_CUDA(cudaMallocAsync(&hist, sizeof(double) * nd * B * m * 2, st));
+  CCO_CUDA(cudaMallocAsync(&dots, sizeof(double) * (size_t)B * m * m * 2, st));
+  CCO_CUDA(cudaMallocAsync(&pf, sizeof(double) * B, st));
+  if (!in_smem) CCO_CUDA(cudaMallocAsync(&trig, tri_bytes * B, st));
+  A.st = stv;
+  A.x = vec;
+  A.s = vec + nd * B;
+  A.g = vec + 2 * nd * B;
+  A.dir = vec + 3 * nd * B;
+  A.glo = vec + 4 * nd * B;
+  A.ps = vec + 5 * nd * B;
+  double* pg = vec + 6 * nd * B;
+  A.pg = pg;
+  A.pf = pf;
+  A.Sh = hist;
+  A.Yh = hist + nd * B * m;
+  A.SYs = dots;
+  A.YYs = dots + (size_t)B * m * m;
+  A.tri_g = trig;
+  if (rec) {
+    A.traj_s = out->traj_s;
+    A.traj_e = out->traj_energy;
+    A.traj_step = out->traj_step;
+    A.traj_it = out->traj_iteration;
+    A.traj_count = out->traj_count;
+  }
+  const size_t st_stride = sizeof(LbState) / sizeof(int64_t);
+  const int64_t* status0 = &stv->status;
+  EvalWS ws;
+  CCO_CUDA(ws.alloc(p, B, st));
+  CCO_CUDA(ws.build(p, B, A.ps, nd, pf, 1, pg, nd, status0, st_stride, st));
+  CCO_CUDA(lbfgs_init(A, s0, st));
+  auto tick = [&](cudaStream_t s) -> cudaError_t {
+    cudaError_t e = eval_launch(ws.plan, s);
+    if (e == cudaSuccess) e = lbfgs_update(A, s);
+    return e;
+  };
+  const int64_t max_ticks =
+      1 + (int64_t)cfg->n_rescales * (cfg->max_evals_per_pass + cfg->max_linesearch_steps + 1) +
+      kGraphTicks;
+  int64_t ticks = 0;
+  int rc = run_ticks(st, tick, status0, st_stride, B, max_ticks, &ticks);
+  if (rc == CCO_OK) {
+    cudaError_t e = lbfgs_finalize(A, out->s, out->energy, out->grad_norm, out->n_evals,
+                                   out->n_iters, out->status, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "lbfgs_finalize");
+  }
+  out->ticks = ticks;
+  ws.release(st);
+  cudaFreeAsync(stv, st);
+  cudaFreeAsync(vec, st);
+  cudaFreeAsync(hist, st);
+  cudaFreeAsync(dots, st);
+  cudaFreeAsync(pf, st);
+  if (trig) cudaFreeAsync(trig, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "relax lbfgs");
+  return rc;
+}

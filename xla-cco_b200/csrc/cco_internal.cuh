@@ -1,0 +1,124 @@
+// Internal declarations shared by the CUDA translation units of libcco.
+//
+// HBM layout of one problem (built once by cco_problem_create):
+//   seg1[nseg1], seg2[nseg2]  32-byte segment headers (runs of consecutive
+//                             last-axis n, split at <= 8 / <= 256 rows)
+//   w_run[M]                  weights in run order
+//   run2ref[M]                run-order row -> caller row
+// Per evaluated configuration (lane):
+//   s[N][d] in, phi out, g[N][d] out, rho[M] / rhow[M] (complex, run order),
+//   part[ntile1][M] pass-1 partial densities (one row per particle tile).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cco.h"
+
+namespace cco {
+
+constexpr int kSeg1Len = 8;     // pass-1 segment length (register accumulators)
+constexpr int kSeg2Len = 256;   // pass-2 segment length (phase re-seed interval)
+constexpr int kPass1Threads = 256;
+constexpr int kPass1Tile = 128; // particles per pass-1 CTA
+constexpr int kPass2Threads = 64;
+constexpr int kPass2PerThread = 2;
+constexpr int kPass2Tile = kPass2Threads * kPass2PerThread;
+constexpr int kMaxLevels = 3;
+
+// One segment: rows kstart .. kstart+len-1 (run order) share the prefix
+// n_0..n_{d-2}; the last axis runs n_{d-1} = n[d-1] + i.
+// dig[a] packs the digit-table indices of |n_a| (start value for the last
+// axis): level l in bits 8l..8l+7, sign (n_a < 0) in bit 24.
+struct SegHdr {
+  int dig[3];
+  int kstart;
+  int n[3];
+  int len;
+};
+static_assert(sizeof(SegHdr) == 32, "segment header is two 16-byte loads");
+
+// Device-resident problem descriptor.
+struct ProbDev {
+  int d, N, M, nseg1, nseg2;
+  int nlev[3];          // digit levels per axis
+  int base[3];          // digit base per axis
+  int nent[3][kMaxLevels];   // entries per level
+  int row[3][kMaxLevels];    // first table row of (axis, level)
+  int nrows;                 // table rows per particle
+  int ntile1, ntile2;        // particle tiles of pass 1 / pass 2
+  double vol;                // V
+  double gpref;              // 2 (2 pi) / V
+  const SegHdr* seg1;
+  const SegHdr* seg2;
+  const double* w_run;
+  const int* run2ref;
+};
+
+// One configuration evaluated by a launch.
+struct EvalLane {
+  const double* s;        // [N][d]
+  double* f;              // [1]
+  double* g;              // [N][d] or null
+  double2* rho;           // [M] run order
+  double2* rhow;          // [M] weighted density (pass-2 input)
+  double2* part;          // [ntile1][M]
+  const int64_t* status;  // evaluate iff null or *status == RUNNING
+  int prob;
+  int pad_;
+};
+
+struct EvalItem {
+  int lane;
+  int tile;
+};
+
+// ---------------------------------------------------------------- complex
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ __forceinline__ bool lane_active(const int64_t* status) {
+  return status == nullptr || *status == CCO_STATUS_RUNNING;
+}
+
+// Deterministic block sum (fixed shuffle tree, then fixed warp order).
+// `red` holds >= 32 doubles; every thread gets the total.
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < nw; ++w) t += red[w];
+  return t;
+}
+
+// ---------------------------------------------------------------- launches
+// Three launches per evaluation: partial densities, reduction + energy,
+// gradient. Items index (lane, tile); lanes whose status is not RUNNING exit.
+struct EvalPlan {
+  const ProbDev* probs;     // device
+  const EvalLane* lanes;    // device
+  const EvalItem* items1;   // device
+  const EvalItem* items2;   // device
+  int n_lanes, n_items1, n_items2;
+  int max_d;                // largest d in the plan (template dispatch)
+  size_t smem1, smem2;      // dynamic shared memory of pass 1 / pass 2
+  bool want_grad;
+};
+
+cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream);
+size_t eval_smem1(const ProbDev& p);
+size_t eval_smem2(const ProbDev& p);
+cudaError_t eval_configure();   // opt-in to large dynamic shared memory
+
+// Copy the run-order density of lane i out in the caller's row order.
+cudaError_t rho_scatter(const double2* rho_run, const int* run2ref, int M,
+                        int batch, size_t lane_stride, double* re, double* im,
+                        cudaStream_t stream);
+
+}  // namespace cco

@@ -1,0 +1,736 @@
+// Batched minimizers as per-lane device state machines (sm_100a, FP64).
+//
+// A relaxation advances in ticks; each tick evaluates the energy and gradient
+// of every RUNNING lane at its probe point (cco_eval.cu) and then runs one
+// update CTA per lane that consumes the result. Finished lanes keep their
+// state untouched (status != RUNNING makes every kernel skip them), which is
+// the reference's bit-exact lane freeze (src/xla_cco/minimize/_loop.py:105-153)
+// and its compaction (minimize/__init__.py:75-99) without a host round trip:
+// the lane order never changes, so results come back in input order.
+//
+// Descent (src/xla_cco/minimize/descent.py:92-197): one iteration per tick.
+// L-BFGS (src/xla_cco/minimize/lbfgs.py:163-329): one line-search probe per
+// tick. The direction is the two-loop recursion of optax's scale_by_lbfgs
+// written through inner products: with a_p = s_p.g, b_p = y_p.g,
+// SY[p][q] = s_p.y_q (p older than q) and YY = y.y maintained as pairs arrive,
+//   alpha_p = rho_p (a_p - sum_{q>p} alpha_q SY[p][q])             (loop 1)
+//   beta_p  = rho_p (gamma (b_p - sum_q alpha_q YY[p][q])
+//                    + sum_{q<p} (alpha_q - beta_q) SY[q][p])       (loop 2)
+//   dir     = -gamma g + sum_q gamma alpha_q y_q - sum_q (alpha_q - beta_q) s_q
+// which is algebraically the two-loop recursion. Each iteration streams the
+// history twice (dots, then the combination) with no serial reduction chain
+// over the history, so the update is HBM-bound instead of latency-bound.
+#include <cmath>
+
+#include "cco_opt.cuh"
+
+namespace cco {
+
+namespace {
+
+constexpr int kUpdThreads = 256;
+
+__device__ __forceinline__ double wrap01(double v) {
+  const double w = v - floor(v);
+  const double below_one = 0x1.fffffffffffffp-1;
+  return w < below_one ? w : below_one;
+}
+
+// ============================================================ descent
+
+__device__ int descent_status(double f, bool nonzero, double step, int64_t it,
+                              const DescentArgs& a) {
+  int code = it >= a.max_iters ? CCO_STATUS_BUDGET : CCO_STATUS_RUNNING;
+  if (step <= a.step_min) code = CCO_STATUS_STEP_FLOOR;
+  if (!nonzero) code = CCO_STATUS_GRAD_TOL;
+  if (f < a.energy_tol) code = CCO_STATUS_ENERGY_TOL;
+  return code;
+}
+
+__device__ void descent_record(const DescentArgs& a, int lane, int64_t it, const double* s,
+                               double f, double step) {
+  if (a.traj_count == nullptr) return;
+  __shared__ int64_t row;
+  if (threadIdx.x == 0) {
+    const int64_t c = a.traj_count[lane];
+    row = ((it % a.rec_every) == 0 && c < a.rec_cap) ? c : -1;
+    if (row >= 0) {
+      a.traj_e[lane * a.rec_cap + row] = f;
+      a.traj_step[lane * a.rec_cap + row] = step;
+      a.traj_it[lane * a.rec_cap + row] = it;
+      a.traj_count[lane] = c + 1;
+    }
+  }
+  __syncthreads();
+  if (row >= 0) {
+    double* o = a.traj_s + ((size_t)lane * a.rec_cap + row) * a.nd;
+    for (int e = threadIdx.x; e < a.nd; e += blockDim.x) o[e] = wrap01(s[e]);
+  }
+}
+
+__global__ void k_descent_init(DescentArgs a, const double* __restrict__ s0) {
+  const int lane = blockIdx.x;
+  const size_t off = (size_t)lane * a.nd;
+  for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+    const double v = s0[off + e];
+    a.ps[off + e] = v;
+    a.s[off + e] = v;
+  }
+  if (threadIdx.x == 0) {
+    a.phase[lane] = PH_INIT;
+    a.status[lane] = CCO_STATUS_RUNNING;
+    a.it[lane] = 0;
+    a.n_evals[lane] = 0;
+    a.step[lane] = a.step_init;
+    if (a.traj_count) a.traj_count[lane] = 0;
+  }
+}
+
+// Gradient norm and the exact all-zero test of the accepted gradient.
+__device__ void descent_norm(const DescentArgs& a, int lane, double* red) {
+  const double* g = a.g + (size_t)lane * a.nd;
+  double ss = 0.0;
+  int nz = 0;
+  for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+    const double v = g[e];
+    ss += v * v;
+    nz |= (v != 0.0);
+  }
+  ss = block_sum(ss, red);
+  nz = __syncthreads_or(nz);
+  if (threadIdx.x == 0) {
+    a.norm[lane] = sqrt(ss);
+    a.nonzero[lane] = nz;
+  }
+}
+
+__global__ void __launch_bounds__(kUpdThreads) k_descent_update(DescentArgs a) {
+  __shared__ double red[32];
+  __shared__ int s_reject, s_status;
+  const int lane = blockIdx.x;
+  if (a.status[lane] != CCO_STATUS_RUNNING) return;
+  const size_t off = (size_t)lane * a.nd;
+  double* s = a.s + off;
+  double* g = a.g + off;
+  double* ps = a.ps + off;
+  const double* pg = a.pg + off;
+  if (a.phase[lane] == PH_INIT) {
+    // init_one (descent.py:121-141): one evaluation at s0, no iteration
+    for (int e = threadIdx.x; e < a.nd; e += blockDim.x) g[e] = pg[e];
+    descent_norm(a, lane, red);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      a.f[lane] = a.pf[lane];
+      a.phase[lane] = PH_ITER;
+      s_status = descent_status(a.f[lane], a.nonzero[lane] != 0, a.step[lane], 0, a);
+      a.status[lane] = s_status;
+    }
+    __syncthreads();
+    descent_record(a, lane, 0, s, a.f[lane], a.step[lane]);
+  } else {
+    // step_fn (descent.py:153-175) with the probe evaluated at xn
+    if (threadIdx.x == 0) {
+      const double f = a.f[lane], f2 = a.pf[lane];
+      const double step = a.step[lane], norm = a.norm[lane];
+      const double df = f - f2;
+      const double df2 = step * norm;
+      const bool reject = fabs(df - df2) / df2 > a.rel_tol;  // NaN accepts
+      a.step[lane] = reject ? step * a.shrink : step * a.grow;
+      if (!reject) a.f[lane] = f2;
+      a.it[lane] += 1;
+      a.n_evals[lane] += 2;
+      s_reject = reject;
+    }
+    __syncthreads();
+    if (!s_reject) {
+      for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+        s[e] = ps[e];
+        g[e] = pg[e];
+      }
+      descent_norm(a, lane, red);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_status = descent_status(a.f[lane], a.nonzero[lane] != 0, a.step[lane], a.it[lane], a);
+      a.status[lane] = s_status;
+    }
+    __syncthreads();
+    descent_record(a, lane, a.it[lane], s, a.f[lane], a.step[lane]);
+  }
+  __syncthreads();
+  if (s_status == CCO_STATUS_RUNNING) {
+    // next probe: xn = s - (g / |g|) * step  (0 * g when |g| = 0)
+    const double norm = a.norm[lane], step = a.step[lane];
+    for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+      const double gn = norm > 0.0 ? __ddiv_rn(g[e], norm) : 0.0 * g[e];
+      ps[e] = __dsub_rn(s[e], __dmul_rn(gn, step));
+    }
+  }
+}
+
+__global__ void k_descent_finalize(DescentArgs a, double* s_out, double* e_out, double* gn_out,
+                                   int64_t* ne_out, int64_t* ni_out, int64_t* st_out) {
+  __shared__ double red[32];
+  const int lane = blockIdx.x;
+  const size_t off = (size_t)lane * a.nd;
+  double ss = 0.0;
+  for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+    const double v = a.g[off + e];
+    ss += v * v;
+    s_out[off + e] = wrap01(a.s[off + e]);
+  }
+  ss = block_sum(ss, red);
+  if (threadIdx.x == 0) {
+    e_out[lane] = a.f[lane];
+    gn_out[lane] = sqrt(ss);
+    ne_out[lane] = a.n_evals[lane];
+    ni_out[lane] = a.it[lane];
+    st_out[lane] = a.status[lane];
+  }
+}
+
+// ============================================================ L-BFGS
+
+enum : int { LS_CONTINUE = 0, LS_ACCEPT_PROBE = 1, LS_ACCEPT_LO = 2, LS_FAIL = 3 };
+
+constexpr double kC1 = 1e-4, kC2 = 0.9, kApproxEps = 1e-6, kGrow = 2.0;
+
+__device__ __forceinline__ bool sufficient(const LbState& L, double a, double f, double d) {
+  if (!isfinite(f) || !isfinite(d)) return false;
+  const double armijo = f - (L.f0 + kC1 * a * L.dphi0);
+  const double approx = fmax(d - (2.0 * kC1 - 1.0) * L.dphi0, f - L.f0 - kApproxEps * fabs(L.f0));
+  return fmin(armijo, approx) <= 0.0;
+}
+
+__device__ __forceinline__ bool curvature_ok(const LbState& L, double d) {
+  return fabs(d) <= kC2 * fabs(L.dphi0);
+}
+
+// Safeguarded cubic step between lo and hi (Nocedal & Wright eq. 3.59),
+// bisection when the cubic is undefined or leaves the inner 80% of the bracket.
+__device__ double zoom_trial(const LbState& L) {
+  const double al = L.a_lo, ah = L.a_hi;
+  const double dlt = ah - al;
+  const double lo_b = fmin(al, ah) + 0.1 * fabs(dlt);
+  const double hi_b = fmax(al, ah) - 0.1 * fabs(dlt);
+  if (isfinite(L.f_hi) && isfinite(L.d_hi) && dlt != 0.0) {
+    const double d1 = L.d_lo + L.d_hi - 3.0 * (L.f_lo - L.f_hi) / (al - ah);
+    const double disc = d1 * d1 - L.d_lo * L.d_hi;
+    if (disc >= 0.0 && isfinite(disc)) {
+      const double d2 = copysign(sqrt(disc), dlt);
+      const double den = L.d_hi - L.d_lo + 2.0 * d2;
+      const double a = ah - dlt * (L.d_hi + d2 - d1) / den;
+      if (isfinite(a) && a >= lo_b && a <= hi_b) return a;
+    }
+  }
+  return al + 0.5 * dlt;
+}
+
+// One probe result (alpha, f, d) -> decision. Sets *new_lo when the probe
+// becomes the best point with sufficient decrease (its gradient is kept).
+__device__ int ls_decide(LbState& L, double f, double d, int64_t max_ls, int* new_lo) {
+  const double a = L.alpha;
+  const bool suff = sufficient(L, a, f, d);
+  *new_lo = 0;
+  int out = LS_CONTINUE;
+  if (L.phase == PH_EXPAND) {
+    if (!suff || (L.ls_steps > 1 && f >= L.f_prev)) {
+      L.a_lo = L.a_prev; L.f_lo = L.f_prev; L.d_lo = L.d_prev;   // (have_lo unchanged)
+      L.a_hi = a; L.f_hi = f; L.d_hi = d;
+      L.phase = PH_ZOOM;
+    } else if (curvature_ok(L, d)) {
+      return LS_ACCEPT_PROBE;
+    } else if (d >= 0.0) {
+      L.a_hi = L.a_prev; L.f_hi = L.f_prev; L.d_hi = L.d_prev;
+      L.a_lo = a; L.f_lo = f; L.d_lo = d; L.have_lo = 1; *new_lo = 1;
+      L.phase = PH_ZOOM;
+    } else {
+      L.a_prev = a; L.f_prev = f; L.d_prev = d;
+      L.a_lo = a; L.f_lo = f; L.d_lo = d; L.have_lo = 1; *new_lo = 1;
+      L.alpha = kGrow * a;
+    }
+  } else {
+    if (!suff || f >= L.f_lo) {
+      L.a_hi = a; L.f_hi = f; L.d_hi = d;
+    } else {
+      if (curvature_ok(L, d)) return LS_ACCEPT_PROBE;
+      if (d * (L.a_hi - L.a_lo) >= 0.0) { L.a_hi = L.a_lo; L.f_hi = L.f_lo; L.d_hi = L.d_lo; }
+      L.a_lo = a; L.f_lo = f; L.d_lo = d; L.have_lo = 1; *new_lo = 1;
+    }
+  }
+  if (L.phase == PH_ZOOM) L.alpha = zoom_trial(L);
+  if (L.ls_steps >= max_ls) out = L.have_lo ? LS_ACCEPT_LO : LS_FAIL;
+  return out;
+}
+
+__device__ __forceinline__ int tri(int p, int q) { return q * (q + 1) / 2 + p; }  // p <= q
+
+struct LbShared {
+  LbState L;
+  double red[32];
+  int outcome, new_lo;
+};
+
+__device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double* s) {
+  if (A.traj_count == nullptr) return;
+  __shared__ int64_t row;
+  if (threadIdx.x == 0) {
+    const int64_t c = A.traj_count[lane];
+    const int64_t it = sh.L.it;
+    row = ((it % A.rec_every) == 0 && c < A.rec_cap) ? c : -1;
+    if (row >= 0) {
+      A.traj_e[lane * A.rec_cap + row] = sh.L.f;
+      A.traj_step[lane * A.rec_cap + row] = sh.L.last_step;
+      A.traj_it[lane * A.rec_cap + row] = it;
+      A.traj_count[lane] = c + 1;
+    }
+  }
+  __syncthreads();
+  if (row >= 0) {
+    double* o = A.traj_s + ((size_t)lane * A.rec_cap + row) * A.nd;
+    for (int e = threadIdx.x; e < A.nd; e += blockDim.x) o[e] = wrap01(s[e]);
+  }
+  __syncthreads();
+}
+
+// Direction for the current (x, g) and the first probe at alpha = 1.
+__device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, double* tsm) {
+  LbState& L = sh.L;
+  const int nd = A.nd, m = A.m;
+  const size_t off = (size_t)lane * nd;
+  const double* g = A.g + off;
+  const double* x = A.x + off;
+  double* dir = A.dir + off;
+  double* ps = A.ps + off;
+  const double* Sh = A.Sh + (size_t)lane * m * nd;
+  const double* Yh = A.Yh + (size_t)lane * m * nd;
+  double* SYs = A.SYs + (size_t)lane * m * m;
+  double* YYs = A.YYs + (size_t)lane * m * m;
+  const int k = L.hk;
+  // scalar arrays live after the triangles
+  double* triSY = tsm;
+  double* triYY = tsm + (size_t)m * (m + 1) / 2;
+  double* av = tsm + (size_t)m * (m + 1);
+  double* bv = av + m;
+  double* alp = bv + m;
+  double* bet = alp + m;
+  double* rh = bet + m;
+  double* cy = rh + m;
+  double* cs = cy + m;
+  const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  auto slot = [&](int p) { return (L.hhead - k + p + m) % m; };
+
+  // ---- pass A: a_p = s_p.g, b_p = y_p.g, and the new pair's column
+  if (k > 0) {
+    const int n = k - 1;
+    const int sn = slot(n);
+    const double* yn = Yh + (size_t)sn * nd;
+    const bool np = L.newpair != 0;
+    for (int p = warp; p < k; p += nwarps) {
+      const int sp = slot(p);
+      const double* sr = Sh + (size_t)sp * nd;
+      const double* yr = Yh + (size_t)sp * nd;
+      double ag = 0.0, bg = 0.0, sy = 0.0, yy = 0.0;
+      if (np) {
+        for (int e = wl; e < nd; e += 32) {
+          const double sv = sr[e], yv = yr[e], gv = g[e], ynv = yn[e];
+          ag += sv * gv;
+          bg += yv * gv;
+          sy += sv * ynv;
+          yy += yv * ynv;
+        }
+      } else {
+        for (int e = wl; e < nd; e += 32) {
+          const double sv = sr[e], yv = yr[e], gv = g[e];
+          ag += sv * gv;
+          bg += yv * gv;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        ag += __shfl_xor_sync(0xffffffffu, ag, o);
+        bg += __shfl_xor_sync(0xffffffffu, bg, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        yy += __shfl_xor_sync(0xffffffffu, yy, o);
+      }
+      if (wl == 0) {
+        av[p] = ag;
+        bv[p] = bg;
+        if (np) {
+          SYs[(size_t)sp * m + sn] = sy;
+          YYs[(size_t)sp * m + sn] = yy;
+          YYs[(size_t)sn * m + sp] = yy;
+        }
+      }
+    }
+    __threadfence_block();
+    __syncthreads();
+    // packed logical triangles (p <= q)
+    const int ntri = k * (k + 1) / 2;
+    for (int t = threadIdx.x; t < ntri; t += blockDim.x) {
+      int q = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+      while (q * (q + 1) / 2 > t) --q;
+      while ((q + 1) * (q + 2) / 2 <= t) ++q;
+      const int p = t - q * (q + 1) / 2;
+      const int sp = slot(p), sq = slot(q);
+      triSY[t] = SYs[(size_t)sp * m + sq];
+      triYY[t] = YYs[(size_t)sp * m + sq];
+    }
+    __syncthreads();
+  }
+  // ---- gamma (optax scale_by_lbfgs): newest pair, or min(1, 1/|g|) on a fresh pass
+  if (k == 0) {
+    double ss = 0.0;
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) ss += g[e] * g[e];
+    ss = block_sum(ss, sh.red);
+    if (threadIdx.x == 0) L.gamma = fmin(1.0, 1.0 / sqrt(ss));
+  } else if (threadIdx.x == 0) {
+    const int n = k - 1;
+    const double num = triSY[tri(n, n)], den = triYY[tri(n, n)];
+    L.gamma = den > 0.0 ? num / den : 1.0;
+  }
+  // ---- loops 1 and 2 on warp 0 (O(k^2) scalars, fixed order)
+  if (k > 0 && warp == 0) {
+    for (int p = wl; p < k; p += 32) {
+      const double ys = triSY[tri(p, p)];
+      rh[p] = ys == 0.0 ? 0.0 : 1.0 / ys;
+    }
+    __syncwarp();
+    for (int p = k - 1; p >= 0; --p) {
+      double acc = 0.0;
+      for (int q = p + 1 + wl; q < k; q += 32) acc += alp[q] * triSY[tri(p, q)];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (wl == 0) alp[p] = rh[p] * (av[p] - acc);
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (k > 0) {
+    // t_p = b_p - sum_q alpha_q YY[p][q] (independent rows: one warp each)
+    for (int p = warp; p < k; p += nwarps) {
+      double acc = 0.0;
+      for (int q = wl; q < k; q += 32) acc += alp[q] * triYY[p <= q ? tri(p, q) : tri(q, p)];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (wl == 0) bet[p] = bv[p] - acc;  // holds t_p until loop 2 overwrites it
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const double gam = L.gamma;
+      for (int p = 0; p < k; ++p) {
+        double acc = 0.0;
+        for (int q = wl; q < p; q += 32) acc += (alp[q] - bet[q]) * triSY[tri(q, p)];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (wl == 0) bet[p] = rh[p] * (gam * bet[p] + acc);
+        __syncwarp();
+      }
+      for (int q = wl; q < k; q += 32) {
+        cy[q] = gam * alp[q];
+        cs[q] = bet[q] - alp[q];
+      }
+    }
+    __syncthreads();
+  }
+  // ---- pass B: dir = -gamma g + sum cy_q y_q + sum cs_q s_q, first probe, g.dir
+  const double gam = L.gamma, R = L.R;
+  double dp = 0.0;
+  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
+    const double ge = g[e];
+    double acc = 0.0;
+    int q = 0;
+    for (; q + 4 <= k; q += 4) {
+      const size_t r0 = (size_t)slot(q) * nd + e, r1 = (size_t)slot(q + 1) * nd + e;
+      const size_t r2 = (size_t)slot(q + 2) * nd + e, r3 = (size_t)slot(q + 3) * nd + e;
+      const double y0 = Yh[r0], s0 = Sh[r0], y1 = Yh[r1], s1 = Sh[r1];
+      const double y2 = Yh[r2], s2 = Sh[r2], y3 = Yh[r3], s3 = Sh[r3];
+      acc += cy[q] * y0 + cs[q] * s0;
+      acc += cy[q + 1] * y1 + cs[q + 1] * s1;
+      acc += cy[q + 2] * y2 + cs[q + 2] * s2;
+      acc += cy[q + 3] * y3 + cs[q + 3] * s3;
+    }
+    for (; q < k; ++q) {
+      const size_t r = (size_t)slot(q) * nd + e;
+      acc += cy[q] * Yh[r] + cs[q] * Sh[r];
+    }
+    const double de = acc - gam * ge;
+    dir[e] = de;
+    dp += ge * de;
+    ps[e] = (x[e] + 1.0 * de) / R;
+  }
+  dp = block_sum(dp, sh.red);
+  if (threadIdx.x == 0) {
+    L.f0 = L.f;
+    L.dphi0 = dp;
+    L.phase = PH_EXPAND;
+    L.ls_steps = 0;
+    L.alpha = 1.0;
+    L.a_prev = 0.0; L.f_prev = L.f; L.d_prev = dp;
+    L.a_lo = 0.0; L.f_lo = L.f; L.d_lo = dp;
+    L.a_hi = 0.0; L.f_hi = L.f; L.d_hi = dp;
+    L.have_lo = 0;
+    L.newpair = 0;
+  }
+  __syncthreads();
+}
+
+__device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double* tsm) {
+  LbState& L = sh.L;
+  const int nd = A.nd, m = A.m;
+  const size_t off = (size_t)lane * nd;
+  double* x = A.x + off;
+  double* s = A.s + off;
+  double* g = A.g + off;
+  const double* dir = A.dir + off;
+  const double* pg = A.pg + off;
+  const double* glo = A.glo + off;
+  const int outcome = sh.outcome;
+  const bool fail = outcome == LS_FAIL;
+  const double R = L.R;
+  const double f_old = L.f;
+  __syncthreads();
+  if (!fail) {
+    const bool probe = outcome == LS_ACCEPT_PROBE;
+    const double al = probe ? L.alpha : L.a_lo;
+    const int sl = L.hhead;
+    double* Sr = A.Sh + ((size_t)lane * m + sl) * nd;
+    double* Yr = A.Yh + ((size_t)lane * m + sl) * nd;
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
+      const double xo = x[e];
+      const double xn = xo + al * dir[e];
+      const double gn = probe ? pg[e] / R : glo[e];
+      Sr[e] = xn - xo;
+      Yr[e] = gn - g[e];
+      x[e] = xn;
+      s[e] = xn / R;
+      g[e] = gn;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      L.f = L.f_lo;  // accepted energy (an accepted probe is stashed in f_lo)
+      L.hhead = (L.hhead + 1) % m;
+      L.hk = min(L.hk + 1, m);
+      L.newpair = 1;
+      L.last_step = al;
+    }
+  } else if (threadIdx.x == 0) {
+    L.last_step = L.alpha;
+  }
+  __syncthreads();
+  // |g_s| = |g_x| R
+  double ss = 0.0;
+  for (int e = threadIdx.x; e < nd; e += blockDim.x) ss += g[e] * g[e];
+  ss = block_sum(ss, sh.red);
+  if (threadIdx.x == 0) {
+    L.stag = (L.f < f_old) ? 0 : L.stag + 1;
+    const int64_t ev = L.ls_steps > 1 ? L.ls_steps : 1;
+    L.pass_evals += ev;
+    L.n_evals += ev;
+    L.it += 1;
+    const double gnorm = sqrt(ss) * R;
+    int glob = gnorm < A.grad_tol ? CCO_STATUS_GRAD_TOL : CCO_STATUS_RUNNING;
+    if (L.f < A.energy_tol) glob = CCO_STATUS_ENERGY_TOL;
+    int local = L.pass_evals >= A.budget ? CCO_STATUS_BUDGET : CCO_STATUS_RUNNING;
+    if (L.stag >= A.patience) local = CCO_STATUS_STAGNATED;
+    if (fail) local = CCO_STATUS_LINESEARCH_FAIL;
+    const bool last = L.pass_idx >= A.n_pass - 1;
+    const bool pass_end = local != CCO_STATUS_RUNNING && glob == CCO_STATUS_RUNNING;
+    const bool advance = pass_end && !last;
+    int status = glob != CCO_STATUS_RUNNING ? glob : CCO_STATUS_RUNNING;
+    if (pass_end && last) status = local;
+    L.status = status;
+    sh.new_lo = advance;  // reuse as the advance flag
+  }
+  __syncthreads();
+  if (sh.new_lo) {
+    const int nx = min(L.pass_idx + 1, A.n_pass - 1);
+    const double rn = A.rescales[nx];
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
+      x[e] = s[e] * rn;
+      g[e] = g[e] * R / rn;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      L.pass_idx += 1;
+      L.R = rn;
+      L.pass_evals = 0;
+      L.stag = 0;
+      L.hk = 0;
+      L.hhead = 0;
+      L.newpair = 0;
+    }
+  }
+  __syncthreads();
+  lb_record(A, lane, sh, s);
+  if (L.status == CCO_STATUS_RUNNING) lb_begin_iteration(A, lane, sh, tsm);
+}
+
+__global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
+  const int lane = blockIdx.x;
+  const size_t off = (size_t)lane * A.nd;
+  for (int e = threadIdx.x; e < A.nd; e += blockDim.x) A.ps[off + e] = s0[off + e];
+  if (threadIdx.x == 0) {
+    LbState L = {};
+    L.phase = PH_INIT;
+    L.status = CCO_STATUS_RUNNING;
+    L.R = A.rescales[0];
+    A.st[lane] = L;
+    if (A.traj_count) A.traj_count[lane] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
+  extern __shared__ double dsm[];
+  __shared__ LbShared sh;
+  const int lane = blockIdx.x;
+  if (threadIdx.x == 0) sh.L = A.st[lane];
+  __syncthreads();
+  if (sh.L.status != CCO_STATUS_RUNNING) return;
+  LbState& L = sh.L;
+  const int nd = A.nd;
+  const size_t off = (size_t)lane * nd;
+  // packed triangles + 7 scalar arrays: shared memory, or a per-lane global
+  // scratch row when memory is too large for shared memory
+  double* tsm = A.smem_tri
+                    ? dsm
+                    : A.tri_g + (size_t)lane * ((size_t)A.m * (A.m + 1) + 7 * (size_t)A.m);
+  if (L.phase == PH_INIT) {
+    // init_one (lbfgs.py:163-197): x = R0 s0, g_x = g_s / R0, one evaluation
+    const double R0 = L.R;
+    double* x = A.x + off;
+    double* s = A.s + off;
+    double* g = A.g + off;
+    const double* ps = A.ps + off;
+    const double* pg = A.pg + off;
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
+      const double v = ps[e];
+      s[e] = v;
+      x[e] = v * R0;
+      g[e] = pg[e] / R0;
+    }
+    if (threadIdx.x == 0) {
+      L.f = A.pf[lane];
+      L.n_evals = 1;
+      L.status = L.f < A.energy_tol ? CCO_STATUS_ENERGY_TOL : CCO_STATUS_RUNNING;
+      L.last_step = 0.0;
+    }
+    __syncthreads();
+    lb_record(A, lane, sh, s);
+    if (L.status == CCO_STATUS_RUNNING) lb_begin_iteration(A, lane, sh, tsm);
+  } else {
+    // one probe of the line search
+    const double R = L.R;
+    const double* pg = A.pg + off;
+    const double* dir = A.dir + off;
+    double dp = 0.0;
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) dp += (pg[e] / R) * dir[e];
+    dp = block_sum(dp, sh.red);
+    if (threadIdx.x == 0) {
+      L.ls_steps += 1;
+      int nl = 0;
+      const double fp = A.pf[lane];
+      sh.outcome = ls_decide(L, fp, dp, A.max_ls, &nl);
+      sh.new_lo = nl;
+      if (sh.outcome == LS_ACCEPT_PROBE) {
+        // stash the accepted value where end_iteration reads it
+        L.f_lo = fp;
+      }
+    }
+    __syncthreads();
+    if (sh.new_lo) {
+      double* glo = A.glo + off;
+      for (int e = threadIdx.x; e < nd; e += blockDim.x) glo[e] = pg[e] / R;
+    }
+    if (sh.outcome == LS_CONTINUE) {
+      const double al = L.alpha;
+      const double* x = A.x + off;
+      double* ps = A.ps + off;
+      for (int e = threadIdx.x; e < nd; e += blockDim.x) ps[e] = (x[e] + al * dir[e]) / R;
+    } else {
+      __syncthreads();
+      lb_end_iteration(A, lane, sh, tsm);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) A.st[lane] = sh.L;
+}
+
+__global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double* gn_out,
+                                 int64_t* ne_out, int64_t* ni_out, int64_t* st_out) {
+  __shared__ double red[32];
+  const int lane = blockIdx.x;
+  const size_t off = (size_t)lane * A.nd;
+  double ss = 0.0;
+  for (int e = threadIdx.x; e < A.nd; e += blockDim.x) {
+    const double v = A.g[off + e];
+    ss += v * v;
+    s_out[off + e] = wrap01(A.s[off + e]);
+  }
+  ss = block_sum(ss, red);
+  if (threadIdx.x == 0) {
+    const LbState L = A.st[lane];
+    e_out[lane] = L.f;
+    gn_out[lane] = sqrt(ss) * L.R;
+    ne_out[lane] = L.n_evals;
+    ni_out[lane] = L.it;
+    st_out[lane] = L.status;
+  }
+}
+
+__global__ void k_count_running(const int64_t* status, size_t stride, int B, int* out) {
+  __shared__ double red[32];
+  double c = 0.0;
+  for (int i = threadIdx.x; i < B; i += blockDim.x)
+    c += (status[(size_t)i * stride] == CCO_STATUS_RUNNING) ? 1.0 : 0.0;
+  c = block_sum(c, red);
+  if (threadIdx.x == 0) *out = (int)c;
+}
+
+}  // namespace
+
+cudaError_t descent_init(const DescentArgs& a, const double* s0, cudaStream_t st) {
+  k_descent_init<<<a.B, kUpdThreads, 0, st>>>(a, s0);
+  return cudaGetLastError();
+}
+cudaError_t descent_update(const DescentArgs& a, cudaStream_t st) {
+  k_descent_update<<<a.B, kUpdThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t descent_finalize(const DescentArgs& a, double* s_out, double* e_out, double* gn_out,
+                             int64_t* ne_out, int64_t* ni_out, int64_t* st_out,
+                             cudaStream_t st) {
+  k_descent_finalize<<<a.B, kUpdThreads, 0, st>>>(a, s_out, e_out, gn_out, ne_out, ni_out,
+                                                  st_out);
+  return cudaGetLastError();
+}
+
+size_t lbfgs_update_smem(int m) {
+  return ((size_t)m * (m + 1) + 7 * (size_t)m) * sizeof(double);
+}
+cudaError_t lbfgs_configure(size_t smem) {
+  return cudaFuncSetAttribute(k_lbfgs_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem);
+}
+cudaError_t lbfgs_init(const LbArgs& a, const double* s0, cudaStream_t st) {
+  k_lbfgs_init<<<a.B, kUpdThreads, 0, st>>>(a, s0);
+  return cudaGetLastError();
+}
+cudaError_t lbfgs_update(const LbArgs& a, cudaStream_t st) {
+  k_lbfgs_update<<<a.B, kUpdThreads, a.smem_tri, st>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double* gn_out,
+                           int64_t* ne_out, int64_t* ni_out, int64_t* st_out,
+                           cudaStream_t st) {
+  k_lbfgs_finalize<<<a.B, kUpdThreads, 0, st>>>(a, s_out, e_out, gn_out, ne_out, ni_out, st_out);
+  return cudaGetLastError();
+}
+cudaError_t count_running(const int64_t* status, size_t stride, int B, int* out,
+                          cudaStream_t st) {
+  k_count_running<<<1, 256, 0, st>>>(status, stride, B, out);
+  return cudaGetLastError();
+}
+
+}  // namespace cco

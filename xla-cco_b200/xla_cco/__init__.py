@@ -1,0 +1,52 @@
+"""xla_cco (B200 build): collective-coordinate hot path on sm_100a.
+
+Drop-in for the relaxation path of the reference package ``xla_cco``
+(``src/xla_cco/__init__.py:54-100``): the same names for the k-set, box,
+energy and minimizer API. Everything is float64; computation runs in the
+hand-written CUDA kernels of ``libcco.so`` (no CPU fallback).
+"""
+
+from xla_cco._types import require_float64
+from xla_cco.box import Box, cubic_box, wrap_fractional
+from xla_cco.energy import (
+    AbstractEnergy,
+    StealthyEnergy,
+    collective_density,
+    make_stealthy_energy,
+)
+from xla_cco.kvectors import (
+    KSet,
+    chi_from_count,
+    enumerate_kvectors,
+    k_outer_from_ka,
+    ka_from_chi,
+    unit_ball_volume,
+)
+from xla_cco.minimize import relax
+from xla_cco.minimize.descent import DescentSettings, adaptive_descent
+from xla_cco.minimize.lbfgs import LBFGSSettings, lbfgs
+from xla_cco.minimize.result import RelaxResult, Trajectory
+
+__all__ = [
+    "AbstractEnergy",
+    "Box",
+    "DescentSettings",
+    "KSet",
+    "LBFGSSettings",
+    "RelaxResult",
+    "StealthyEnergy",
+    "Trajectory",
+    "adaptive_descent",
+    "chi_from_count",
+    "collective_density",
+    "cubic_box",
+    "enumerate_kvectors",
+    "k_outer_from_ka",
+    "ka_from_chi",
+    "lbfgs",
+    "make_stealthy_energy",
+    "relax",
+    "require_float64",
+    "unit_ball_volume",
+    "wrap_fractional",
+]

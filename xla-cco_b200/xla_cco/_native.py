@@ -1,0 +1,162 @@
+"""ctypes binding of libcco.so (the C ABI declared in include/cco.h).
+
+The library is the only compute path: there is no CPU fallback. Loading
+fails loudly if the shared object is missing, and every compute entry point
+raises ``RuntimeError`` when no CUDA device is visible (the reference's
+fail-fast GPU guard, ``xla_cco/_device.py:137-142``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libcco.so"
+
+CCO_OK = 0
+CCO_ERR_ARG = 1
+CCO_ERR_OOM = 2
+CCO_ERR_ADMISSION = 3
+CCO_ERR_DEVICE = 4
+CCO_ERR_TIMEOUT = 5
+CCO_ERR_ROUNDS = 6
+CCO_ERR_NODEVICE = 7
+MAX_RESCALES = 8
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_vp = ctypes.c_void_p
+
+
+class DescentSettingsC(ctypes.Structure):
+    _fields_ = [
+        ("step_init", ctypes.c_double),
+        ("step_min", ctypes.c_double),
+        ("shrink", ctypes.c_double),
+        ("grow", ctypes.c_double),
+        ("rel_tol", ctypes.c_double),
+        ("max_evals", ctypes.c_int64),
+        ("energy_tol", ctypes.c_double),
+        ("record_every", ctypes.c_int64),
+        ("max_records", ctypes.c_int64),
+    ]
+
+
+class LBFGSSettingsC(ctypes.Structure):
+    _fields_ = [
+        ("memory", ctypes.c_int64),
+        ("n_rescales", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+        ("rescales", ctypes.c_double * MAX_RESCALES),
+        ("max_evals_per_pass", ctypes.c_int64),
+        ("energy_tol", ctypes.c_double),
+        ("grad_tol", ctypes.c_double),
+        ("stagnation_patience", ctypes.c_int64),
+        ("max_linesearch_steps", ctypes.c_int64),
+        ("record_every", ctypes.c_int64),
+        ("max_records", ctypes.c_int64),
+    ]
+
+
+class RelaxOutC(ctypes.Structure):
+    _fields_ = [
+        ("s", _vp),
+        ("energy", _vp),
+        ("grad_norm", _vp),
+        ("n_evals", _vp),
+        ("n_iters", _vp),
+        ("status", _vp),
+        ("traj_s", _vp),
+        ("traj_energy", _vp),
+        ("traj_step", _vp),
+        ("traj_iteration", _vp),
+        ("traj_count", _vp),
+        ("ticks", ctypes.c_int64),
+    ]
+
+
+# (name, restype, argtypes) for every symbol include/cco.h declares
+SIGNATURES = {
+    "cco_abi_version": (ctypes.c_int, []),
+    "cco_error_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "cco_last_error": (ctypes.c_char_p, []),
+    "cco_device_count": (ctypes.c_int, [_c_int_p]),
+    "cco_problem_create": (
+        ctypes.c_int,
+        [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_double,
+         ctypes.POINTER(_vp)],
+    ),  # fmt: skip
+    "cco_problem_destroy": (ctypes.c_int, [_vp]),
+    "cco_problem_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p]),
+    "cco_energy_grad": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "cco_relax_descent": (
+        ctypes.c_int,
+        [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(DescentSettingsC), ctypes.c_int,
+         ctypes.POINTER(RelaxOutC)],
+    ),  # fmt: skip
+    "cco_relax_lbfgs": (
+        ctypes.c_int,
+        [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(LBFGSSettingsC), ctypes.c_int,
+         ctypes.POINTER(RelaxOutC)],
+    ),  # fmt: skip
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libcco.so once (``RuntimeError`` if it was never built)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = Path(os.environ.get("CCO_LIB", LIB_PATH))
+        if not path.exists():
+            raise RuntimeError(
+                f"libcco.so not found at {path}; build it with `python xla-cco_b200/build.py` "
+                "(there is no CPU fallback)"
+            )
+        lib = ctypes.CDLL(str(path))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+class CcoError(RuntimeError):
+    """A libcco call failed; ``code`` is the CCO_ERR_* value."""
+
+    def __init__(self, code: int, msg: str) -> None:
+        super().__init__(msg)
+        self.code = code
+
+
+def check(code: int, what: str) -> None:
+    """Map a CCO return code to the reference's Python exception types."""
+    if code == CCO_OK:
+        return
+    lib = load()
+    detail = (lib.cco_last_error() or b"").decode(errors="replace")
+    msg = f"{what}: {lib.cco_error_string(code).decode()}" + (f" ({detail})" if detail else "")
+    if code == CCO_ERR_ARG:
+        raise ValueError(msg)
+    raise CcoError(code, msg)
+
+
+def device_count() -> int:
+    """Number of visible CUDA devices (0 when none)."""
+    n = ctypes.c_int(0)
+    code = load().cco_device_count(ctypes.byref(n))
+    return int(n.value) if code == CCO_OK else 0
+
+
+def require_gpu() -> None:
+    """``RuntimeError`` unless a CUDA device is visible (no silent CPU fallback)."""
+    if device_count() == 0:
+        raise RuntimeError(
+            "xla_cco (B200 build) needs a CUDA device: no GPU is visible and there is no CPU path"
+        )

@@ -1,0 +1,144 @@
+"""Batched relaxation on the device (drop-in for ``xla_cco.minimize.relax``).
+
+``relax(energy, s0, settings, chunk_iters=2000)`` relaxes a (B, N, d) batch
+and returns a ``RelaxResult`` with a leading lane axis, in input order
+(``minimize/__init__.py:102-151``). Each lane is a device state machine
+(``csrc/cco_opt.cu``); a finished lane is frozen bit-exactly and skipped by
+every later launch, which is the reference's per-lane freeze plus host-side
+compaction done on the device. ``chunk_iters`` is validated and accepted; the
+result does not depend on it (the reference guarantees the same).
+"""
+
+from __future__ import annotations
+
+from typing import Any, Union
+
+import numpy as np
+
+from xla_cco import _native
+from xla_cco._types import require_float64
+from xla_cco.minimize.descent import DescentSettings
+from xla_cco.minimize.lbfgs import LBFGSSettings
+from xla_cco.minimize.result import RelaxResult, Trajectory
+
+__all__ = ["relax", "relax_device", "DescentSettings", "LBFGSSettings"]
+
+
+def _descent_c(st: DescentSettings) -> _native.DescentSettingsC:
+    return _native.DescentSettingsC(
+        float(st.step_init), float(st.step_min), float(st.shrink), float(st.grow),
+        float(st.rel_tol), int(st.max_evals), float(st.energy_tol), int(st.record_every),
+        int(st.max_records),
+    )  # fmt: skip
+
+
+def _lbfgs_c(st: LBFGSSettings) -> _native.LBFGSSettingsC:
+    if not 1 <= len(st.rescales) <= _native.MAX_RESCALES:
+        raise ValueError(f"need 1..{_native.MAX_RESCALES} rescale passes")
+    c = _native.LBFGSSettingsC()
+    c.memory = int(st.memory)
+    c.n_rescales = len(st.rescales)
+    for i, r in enumerate(st.rescales):
+        c.rescales[i] = float(r)
+    c.max_evals_per_pass = int(st.max_evals_per_pass)
+    c.energy_tol = float(st.energy_tol)
+    c.grad_tol = float(st.grad_tol)
+    c.stagnation_patience = int(st.stagnation_patience)
+    c.max_linesearch_steps = int(st.max_linesearch_steps)
+    c.record_every = int(st.record_every)
+    c.max_records = int(st.max_records)
+    return c
+
+
+def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
+                 chunk_iters: int = 2_000) -> dict:  # fmt: skip
+    """Run the device relaxation on a CUDA tensor ``s0`` (B, N, d); results stay on the device.
+
+    Returns a dict of CUDA tensors (``s``, ``energy``, ``grad_norm``,
+    ``n_evals``, ``n_iters``, ``status``, trajectory fields) plus ``ticks``.
+    """
+    import torch
+
+    from xla_cco.energy import StealthyEnergy
+
+    if not isinstance(energy, StealthyEnergy):
+        raise TypeError("the B200 relax path evaluates a StealthyEnergy on the device")
+    if isinstance(settings, DescentSettings):
+        cset, fn = _descent_c(settings), "cco_relax_descent"
+    elif isinstance(settings, LBFGSSettings):
+        cset, fn = _lbfgs_c(settings), "cco_relax_lbfgs"
+    else:
+        raise TypeError(f"unsupported settings type {type(settings).__name__}")
+    if energy._zero_weight != 0.0:
+        raise ValueError("zero k rows with nonzero weight are not supported by relax")
+    b, n, d = s0.shape
+    assert d == energy.dim, "dimension mismatch"
+    dev = s0.device
+    h = energy.problem_handle(dev.index if dev.index is not None else torch.cuda.current_device(), n)
+    f64, i64 = torch.float64, torch.int64
+    out = {
+        "s": torch.empty_like(s0),
+        "energy": torch.empty(b, dtype=f64, device=dev),
+        "grad_norm": torch.empty(b, dtype=f64, device=dev),
+        "n_evals": torch.empty(b, dtype=i64, device=dev),
+        "n_iters": torch.empty(b, dtype=i64, device=dev),
+        "status": torch.empty(b, dtype=i64, device=dev),
+    }
+    rec = settings.record_every > 0 and settings.max_records > 0
+    cap = int(settings.max_records)
+    if rec:
+        out["traj_s"] = torch.zeros((b, cap, n, d), dtype=f64, device=dev)
+        out["traj_energy"] = torch.zeros((b, cap), dtype=f64, device=dev)
+        out["traj_step"] = torch.zeros((b, cap), dtype=f64, device=dev)
+        out["traj_iteration"] = torch.zeros((b, cap), dtype=i64, device=dev)
+        out["traj_count"] = torch.zeros(b, dtype=i64, device=dev)
+    co = _native.RelaxOutC()
+    for key in ("s", "energy", "grad_norm", "n_evals", "n_iters", "status"):
+        setattr(co, key, out[key].data_ptr())
+    if rec:
+        for key in ("traj_s", "traj_energy", "traj_step", "traj_iteration", "traj_count"):
+            setattr(co, key, out[key].data_ptr())
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        code = getattr(_native.load(), fn)(
+            h, stream, b, s0.data_ptr(), _native.ctypes.byref(cset), int(chunk_iters),
+            _native.ctypes.byref(co),
+        )  # fmt: skip
+    if code == _native.CCO_ERR_ROUNDS:
+        raise RuntimeError("relax did not finish within the round bound")
+    _native.check(code, fn)
+    out["ticks"] = int(co.ticks)
+    return out
+
+
+def relax(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
+          chunk_iters: int = 2_000) -> RelaxResult:  # fmt: skip
+    """Relax a batch of configurations; result leaves carry a leading batch axis.
+
+    ``TypeError`` if ``s0`` is not float64 or ``settings`` is of another type;
+    ``RuntimeError`` if the round bound is exceeded or no GPU is visible.
+    """
+    import torch
+
+    require_float64(s0, "s0")
+    assert s0.ndim == 3, "s0 must have shape (b, n, d)"
+    assert chunk_iters >= 1, "chunk_iters must be positive"
+    assert s0.shape[0] >= 1, "need at least one configuration"
+    if not isinstance(settings, (DescentSettings, LBFGSSettings)):
+        raise TypeError(f"unsupported settings type {type(settings).__name__}")
+    _native.require_gpu()
+    host = not (isinstance(s0, torch.Tensor) and s0.is_cuda)
+    s_dev = torch.from_numpy(np.ascontiguousarray(np.asarray(s0))).cuda() if host else s0.contiguous()
+    out = relax_device(energy, s_dev, settings, chunk_iters)
+    conv = (lambda t: t.cpu().numpy()) if host else (lambda t: t)
+    traj = None
+    if "traj_s" in out:
+        traj = Trajectory(
+            s=conv(out["traj_s"]), energy=conv(out["traj_energy"]), step=conv(out["traj_step"]),
+            iteration=conv(out["traj_iteration"]), count=conv(out["traj_count"]),
+        )  # fmt: skip
+    return RelaxResult(
+        s=conv(out["s"]), energy=conv(out["energy"]), grad_norm=conv(out["grad_norm"]),
+        n_evals=conv(out["n_evals"]), n_iters=conv(out["n_iters"]), status=conv(out["status"]),
+        trajectory=traj,
+    )  # fmt: skip
