@@ -1,0 +1,350 @@
+#!/usr/bin/env python3
+"""Benchmark: batched L-BFGS relaxation to Phi < 1e-20 on B200.
+
+Workload (one "step"): relax 256 seeded uniform configurations, d = 2,
+N = 1000, chi = 0.40 (half-space k-set M = 802), cubic unit-density box,
+LBFGSSettings(energy_tol = 1e-20) with the default three-pass schedule and
+memory 100, all float64. Metric: relaxations/s to Phi < 1e-20 (lanes that
+reach the tolerance, per second of device time), with p50/p99 lane latency.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU runs (torchrun, one process per GPU) are independent replicas:
+lanes are independent relaxations, so each rank relaxes its own seeded batch
+with no data-path collective; NCCL carries only the barrier and the max over
+ranks of the timed region.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT / "xla-cco_b200", ROOT / "oracle"):
+    sys.path.insert(0, str(_p))
+
+METRIC = "relaxations/s to Phi<1e-20 (batched L-BFGS, plain FP64)"
+UNIT = "relaxations/s"
+N_PART, DIM, CHI, PHI_PACK, BATCH, SEED = 1000, 2, 0.40, 0.05, 256, 0
+TOL = 1e-20
+F_PAIR = {1: 7, 2: 21, 3: 35}  # algorithmic FP64 flops per (k, particle) pair and evaluation
+# Mean energy+force evaluations per relaxation of this workload (reference
+# counting: line-search probes + 1), measured by the device arm on seeds
+# 0..255 with the same algorithm; converts the CPU arm's evals/s into
+# relaxations/s. Refreshed from the device arm's "evals_per_relax".
+EVALS_PER_RELAX = None
+
+
+def workload():
+    from xla_cco import cubic_box, enumerate_kvectors, k_outer_from_ka, ka_from_chi, make_stealthy_energy
+
+    box = cubic_box(N_PART, DIM)
+    ks = enumerate_kvectors(box.basis, 0.0, k_outer_from_ka(ka_from_chi(CHI, PHI_PACK, DIM), PHI_PACK, DIM))
+    return box, ks, make_stealthy_energy(box, ks)
+
+
+def config_dict(ks, extra=None):
+    c = {
+        "workload": f"lbfgs_relax_d{DIM}_n{N_PART}_chi{CHI}_m{ks.n.shape[0]}_b{BATCH}",
+        "d": DIM, "n_particles": N_PART, "chi": CHI, "m_kvectors": int(ks.n.shape[0]),
+        "batch": BATCH, "energy_tol": TOL, "minimizer": "L-BFGS m=100, rescales 1e4/1/1e-2",
+        "seeds": "default_rng(seed + rank).uniform((B, N, d))",
+        "l2": "inputs larger than L2: history 2*100*N*d*8 B per lane = 0.8 GB per step",
+    }  # fmt: skip
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")  # fmt: skip
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )  # fmt: skip
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self) -> None:
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+# ------------------------------------------------------------------ CPU arm
+def cpu_sample(s0: np.ndarray, ks, box, evals_per_relax: float | None, budget: int = 200):
+    """Time the oracle L-BFGS on all host threads; returns the cpu_baseline dict."""
+    import oracle
+    from xla_cco import LBFGSSettings
+
+    threads = oracle.max_threads()
+    lanes = min(threads, s0.shape[0])
+    cfg = LBFGSSettings(energy_tol=TOL, rescales=(1e4,), max_evals_per_pass=budget)
+    t0 = time.perf_counter()
+    out = oracle.relax_batch("lbfgs", s0[:lanes], ks.n, ks.weights, box.volume, cfg, threads=threads)
+    dt = time.perf_counter() - t0
+    evals = int(out["n_evals"].sum())
+    eps = evals / dt
+    value = eps / evals_per_relax if evals_per_relax else None
+    return {
+        "value": value, "unit": UNIT, "cores": threads, "kind": "port",
+        "evals_per_s": eps,
+        "sample": (f"C oracle L-BFGS (OpenMP, {threads} threads) on {lanes} of the seeded "
+                   f"configurations, {budget}-evaluation budget each ({evals} energy+force "
+                   f"evaluations in {dt:.1f} s); relaxations/s = evals/s / "
+                   f"{evals_per_relax} evaluations per relaxation of this workload"),
+    }  # fmt: skip
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle  # noqa: F401
+
+    box, ks, _ = workload()
+    s0 = np.random.default_rng(SEED).uniform(size=(BATCH, N_PART, DIM))
+    for _ in range(args.warmup):
+        cpu_sample(s0, ks, box, EVALS_PER_RELAX, budget=args.ref_budget)
+    vals, cb = [], None
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cb = cpu_sample(s0, ks, box, EVALS_PER_RELAX, budget=args.ref_budget)
+        vals.append(cb["value"] if cb["value"] is not None else float("nan"))
+    wall = time.perf_counter() - t0
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_dict(ks),
+        "cpu_baseline": cb,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ device arm
+def fp64_peak_tflops() -> float | None:
+    import ctypes
+
+    lib_path = ROOT / "xla-cco_b200" / "xla_cco" / "_lib" / "libcco_peaks.so"
+    if not lib_path.exists():
+        return None
+    lib = ctypes.CDLL(str(lib_path))
+    out = ctypes.c_double(0.0)
+    best = 0.0
+    for _ in range(3):
+        if lib.cco_peak_fma(1, 148 * 8, 256, 2000, ctypes.byref(out)) == 0:
+            best = max(best, out.value)
+    return best or None
+
+
+def run_device(args) -> None:
+    import torch
+
+    from xla_cco import LBFGSSettings, relax
+    from xla_cco.minimize import relax_device
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    box, ks, energy = workload()
+    settings = LBFGSSettings(energy_tol=TOL)
+    s0 = np.random.default_rng(SEED + rank).uniform(size=(args.batch, N_PART, DIM))
+    s_dev = torch.from_numpy(s0).cuda()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        relax_device(energy, s_dev, settings)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    outs = []
+    for _ in range(args.steps):
+        outs.append(relax_device(energy, s_dev, settings))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    succ = sum(int((o["energy"] < TOL).sum().item()) for o in outs)
+    evals = np.concatenate([o["n_evals"].cpu().numpy() for o in outs])
+    lat = np.concatenate([o["latency_ns"].cpu().numpy() for o in outs]) / 1e6
+    launches = sum(o["launches"] for o in outs)
+    ticks = sum(o["ticks"] for o in outs)
+    t_max = ms
+    if dist is not None:
+        tt = torch.tensor([ms, float(succ)], dtype=torch.float64, device="cuda")
+        mx = tt.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt, op=dist.ReduceOp.SUM)
+        t_max, succ = float(mx[0]), int(tt[1])
+    value = succ / (t_max / 1e3)
+
+    # roofline of the evaluation kernels (pass 1 + reduce + pass 2) on this batch
+    ev_n = 20
+    for _ in range(3):
+        energy.evaluate(s_dev)
+    torch.cuda.synchronize()
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record(stream)
+    for _ in range(ev_n):
+        energy.evaluate(s_dev)
+    r1.record(stream)
+    torch.cuda.synchronize()
+    eval_ms = r0.elapsed_time(r1) / ev_n
+    m = int(ks.n.shape[0])
+    flop = float(args.batch) * N_PART * m * F_PAIR[DIM]
+    achieved = flop / (eval_ms * 1e-3) / 1e12
+    peak = fp64_peak_tflops()
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get("eval_bytes_per_launch")
+
+    # end to end through the public API: pinned host in, host out, every step
+    pinned = torch.from_numpy(s0).pin_memory()
+    h2d = pinned.numel() * 8
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_succ = 0
+    for _ in range(args.steps):
+        res = relax(energy, pinned, settings)
+        e2e_succ += int((res.energy < TOL).sum())
+    e2e_s = time.perf_counter() - t0
+    d2h = args.batch * (N_PART * DIM * 8 + 8 * 5)
+    e2e = {"value": e2e_succ / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "timing": "host wall clock around relax(numpy->numpy)"}  # fmt: skip
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    epr = float(evals.mean())
+    cb = None
+    if not args.no_cpu_baseline:
+        cb = cpu_sample(s0, ks, box, epr)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(ks, {
+            "parallelism": f"replicas x{world}",
+            "success": f"{succ}/{args.batch * args.steps * world}",
+            "p50_latency_ms": float(np.percentile(lat, 50)),
+            "p99_latency_ms": float(np.percentile(lat, 99)),
+            "evals_per_relax": epr, "ticks": ticks,
+            "evals_per_s": float(evals.sum()) / (ms / 1e3),
+            "pair_evals_per_s": float(evals.sum()) * N_PART * m / (ms / 1e3),
+        }),
+        "roofline": {
+            "kernel": "energy+force evaluation (pass1 + reduce + pass2), batch 256",
+            "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if peak else None, "traffic": traffic,
+            "eval_ms": eval_ms,
+            "peak_source": "measured FP64 FMA probe (libcco_peaks.so), this run",
+            "algorithmic": f"{F_PAIR[DIM]} flop per (k, particle) pair x N M x batch",
+        },
+        "cpu_baseline": cb,
+        "e2e": e2e,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cco", "reference"], default="cco")
+    ap.add_argument("--batch", type=int, default=BATCH)
+    ap.add_argument("--ref-budget", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_device(args)
+
+
+if __name__ == "__main__":
+    main()

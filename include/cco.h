@@ -131,7 +131,10 @@ typedef struct {
   double* traj_step;    /* [B][max_records] */
   int64_t* traj_iteration; /* [B][max_records] */
   int64_t* traj_count;  /* [B] */
+  int64_t* latency_ns;  /* [B] optional: device time from the start of the call to the
+                           lane's completion (%globaltimer), NULL to skip */
   int64_t ticks;        /* out: device ticks (one energy evaluation per running lane each) */
+  int64_t launches;     /* out: kernel launches issued by the call */
 } cco_relax_out;
 
 /*

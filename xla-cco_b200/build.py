@@ -47,8 +47,26 @@ def _stale() -> bool:
     return any(p.stat().st_mtime > t for p in deps)
 
 
+PEAKS_LIB = OUT_DIR / "libcco_peaks.so"
+
+
+def build_peaks(force: bool = False) -> Path:
+    """Compile the FMA throughput probe (measurement utility used by bench.py)."""
+    src = CSRC / "peaks.cu"
+    if not force and PEAKS_LIB.exists() and PEAKS_LIB.stat().st_mtime > src.stat().st_mtime:
+        return PEAKS_LIB
+    OUT_DIR.mkdir(parents=True, exist_ok=True)
+    cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-o", str(PEAKS_LIB), str(src)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed building libcco_peaks.so")
+    return PEAKS_LIB
+
+
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
     """Compile the library if any source is newer than it; return its path."""
+    build_peaks(force)
     if not force and not _stale():
         return LIB
     OUT_DIR.mkdir(parents=True, exist_ok=True)

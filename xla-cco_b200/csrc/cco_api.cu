@@ -544,11 +544,11 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
   a.rec_cap = rec ? cfg->max_records : 0;
   double* vec = nullptr;   // s, g, ps, pg
   double* sc = nullptr;    // f, step, norm, pf
-  int64_t* ic = nullptr;   // it, n_evals, status
+  int64_t* ic = nullptr;   // it, n_evals, status, t0, t1
   int* ph = nullptr;       // phase, nonzero
   CCO_CUDA(cudaMallocAsync(&vec, sizeof(double) * nd * B * 4, st));
   CCO_CUDA(cudaMallocAsync(&sc, sizeof(double) * B * 4, st));
-  CCO_CUDA(cudaMallocAsync(&ic, sizeof(int64_t) * B * 3, st));
+  CCO_CUDA(cudaMallocAsync(&ic, sizeof(int64_t) * B * 5, st));
   CCO_CUDA(cudaMallocAsync(&ph, sizeof(int) * B * 2, st));
   a.s = vec;
   a.g = vec + nd * B;
@@ -563,6 +563,8 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
   a.it = ic;
   a.n_evals = ic + B;
   a.status = ic + 2 * B;
+  a.t0 = ic + 3 * B;
+  a.t1 = ic + 4 * B;
   a.phase = ph;
   a.nonzero = ph + B;
   if (rec) {
@@ -586,10 +588,11 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
   int rc = run_ticks(st, tick, a.status, 1, B, max_ticks, &ticks);
   if (rc == CCO_OK) {
     cudaError_t e = descent_finalize(a, out->s, out->energy, out->grad_norm, out->n_evals,
-                                     out->n_iters, out->status, st);
+                                     out->n_iters, out->status, out->latency_ns, st);
     if (e != cudaSuccess) rc = cuda_fail(e, "descent_finalize");
   }
   out->ticks = ticks;
+  out->launches = ticks * 4 + ticks / kGraphTicks + 3;
   ws.release(st);
   cudaFreeAsync(vec, st);
   cudaFreeAsync(sc, st);
@@ -698,10 +701,11 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   int rc = run_ticks(st, tick, status0, st_stride, B, max_ticks, &ticks);
   if (rc == CCO_OK) {
     cudaError_t e = lbfgs_finalize(A, out->s, out->energy, out->grad_norm, out->n_evals,
-                                   out->n_iters, out->status, st);
+                                   out->n_iters, out->status, out->latency_ns, st);
     if (e != cudaSuccess) rc = cuda_fail(e, "lbfgs_finalize");
   }
   out->ticks = ticks;
+  out->launches = ticks * 4 + ticks / kGraphTicks + 3;
   ws.release(st);
   cudaFreeAsync(stv, st);
   cudaFreeAsync(vec, st);

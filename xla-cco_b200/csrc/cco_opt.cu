@@ -30,6 +30,12 @@ namespace {
 
 constexpr int kUpdThreads = 256;
 
+__device__ __forceinline__ int64_t gtimer() {
+  uint64_t v;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+  return (int64_t)v;
+}
+
 __device__ __forceinline__ double wrap01(double v) {
   const double w = v - floor(v);
   const double below_one = 0x1.fffffffffffffp-1;
@@ -82,6 +88,8 @@ __global__ void k_descent_init(DescentArgs a, const double* __restrict__ s0) {
     a.it[lane] = 0;
     a.n_evals[lane] = 0;
     a.step[lane] = a.step_init;
+    a.t0[lane] = gtimer();
+    a.t1[lane] = 0;
     if (a.traj_count) a.traj_count[lane] = 0;
   }
 }
@@ -124,6 +132,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_descent_update(DescentArgs a) {
       a.phase[lane] = PH_ITER;
       s_status = descent_status(a.f[lane], a.nonzero[lane] != 0, a.step[lane], 0, a);
       a.status[lane] = s_status;
+      if (s_status != CCO_STATUS_RUNNING) a.t1[lane] = gtimer();
     }
     __syncthreads();
     descent_record(a, lane, 0, s, a.f[lane], a.step[lane]);
@@ -153,6 +162,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_descent_update(DescentArgs a) {
     if (threadIdx.x == 0) {
       s_status = descent_status(a.f[lane], a.nonzero[lane] != 0, a.step[lane], a.it[lane], a);
       a.status[lane] = s_status;
+      if (s_status != CCO_STATUS_RUNNING) a.t1[lane] = gtimer();
     }
     __syncthreads();
     descent_record(a, lane, a.it[lane], s, a.f[lane], a.step[lane]);
@@ -169,7 +179,8 @@ __global__ void __launch_bounds__(kUpdThreads) k_descent_update(DescentArgs a) {
 }
 
 __global__ void k_descent_finalize(DescentArgs a, double* s_out, double* e_out, double* gn_out,
-                                   int64_t* ne_out, int64_t* ni_out, int64_t* st_out) {
+                                   int64_t* ne_out, int64_t* ni_out, int64_t* st_out,
+                                   int64_t* lat_out) {
   __shared__ double red[32];
   const int lane = blockIdx.x;
   const size_t off = (size_t)lane * a.nd;
@@ -186,6 +197,7 @@ __global__ void k_descent_finalize(DescentArgs a, double* s_out, double* e_out, 
     ne_out[lane] = a.n_evals[lane];
     ni_out[lane] = a.it[lane];
     st_out[lane] = a.status[lane];
+    if (lat_out) lat_out[lane] = a.t1[lane] - a.t0[lane];
   }
 }
 
@@ -541,6 +553,7 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double
     int status = glob != CCO_STATUS_RUNNING ? glob : CCO_STATUS_RUNNING;
     if (pass_end && last) status = local;
     L.status = status;
+    if (status != CCO_STATUS_RUNNING) L.t1 = gtimer();
     sh.new_lo = advance;  // reuse as the advance flag
   }
   __syncthreads();
@@ -576,6 +589,7 @@ __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
     L.phase = PH_INIT;
     L.status = CCO_STATUS_RUNNING;
     L.R = A.rescales[0];
+    L.t0 = gtimer();
     A.st[lane] = L;
     if (A.traj_count) A.traj_count[lane] = 0;
   }
@@ -615,6 +629,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
       L.n_evals = 1;
       L.status = L.f < A.energy_tol ? CCO_STATUS_ENERGY_TOL : CCO_STATUS_RUNNING;
       L.last_step = 0.0;
+      if (L.status != CCO_STATUS_RUNNING) L.t1 = gtimer();
     }
     __syncthreads();
     lb_record(A, lane, sh, s);
@@ -658,7 +673,8 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
 }
 
 __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double* gn_out,
-                                 int64_t* ne_out, int64_t* ni_out, int64_t* st_out) {
+                                 int64_t* ne_out, int64_t* ni_out, int64_t* st_out,
+                                 int64_t* lat_out) {
   __shared__ double red[32];
   const int lane = blockIdx.x;
   const size_t off = (size_t)lane * A.nd;
@@ -676,6 +692,7 @@ __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double*
     ne_out[lane] = L.n_evals;
     ni_out[lane] = L.it;
     st_out[lane] = L.status;
+    if (lat_out) lat_out[lane] = L.t1 - L.t0;
   }
 }
 
@@ -699,10 +716,10 @@ cudaError_t descent_update(const DescentArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 cudaError_t descent_finalize(const DescentArgs& a, double* s_out, double* e_out, double* gn_out,
-                             int64_t* ne_out, int64_t* ni_out, int64_t* st_out,
+                             int64_t* ne_out, int64_t* ni_out, int64_t* st_out, int64_t* lat_out,
                              cudaStream_t st) {
   k_descent_finalize<<<a.B, kUpdThreads, 0, st>>>(a, s_out, e_out, gn_out, ne_out, ni_out,
-                                                  st_out);
+                                                  st_out, lat_out);
   return cudaGetLastError();
 }
 
@@ -722,9 +739,10 @@ cudaError_t lbfgs_update(const LbArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double* gn_out,
-                           int64_t* ne_out, int64_t* ni_out, int64_t* st_out,
+                           int64_t* ne_out, int64_t* ni_out, int64_t* st_out, int64_t* lat_out,
                            cudaStream_t st) {
-  k_lbfgs_finalize<<<a.B, kUpdThreads, 0, st>>>(a, s_out, e_out, gn_out, ne_out, ni_out, st_out);
+  k_lbfgs_finalize<<<a.B, kUpdThreads, 0, st>>>(a, s_out, e_out, gn_out, ne_out, ni_out, st_out,
+                                                lat_out);
   return cudaGetLastError();
 }
 cudaError_t count_running(const int64_t* status, size_t stride, int B, int* out,

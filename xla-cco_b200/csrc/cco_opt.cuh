@@ -22,6 +22,7 @@ struct DescentArgs {
   int64_t *it, *n_evals, *status;
   int* phase;
   int* nonzero;           // [B] any(g != 0)
+  int64_t *t0, *t1;       // [B] %globaltimer at start / completion
   // trajectory (null when off)
   double *traj_s, *traj_e, *traj_step;
   int64_t *traj_it, *traj_count;
@@ -36,6 +37,7 @@ struct LbState {
   double a_hi, f_hi, d_hi;
   double gamma, last_step;
   int64_t it, n_evals, pass_evals, stag, status;
+  int64_t t0, t1;         // %globaltimer at start / completion
   int32_t phase, ls_steps, pass_idx, hk, hhead, have_lo, newpair, pad_;
 };
 
@@ -62,14 +64,14 @@ cudaError_t descent_init(const DescentArgs& a, const double* s0, cudaStream_t st
 cudaError_t descent_update(const DescentArgs& a, cudaStream_t st);
 cudaError_t descent_finalize(const DescentArgs& a, double* s_out, double* e_out,
                              double* gn_out, int64_t* ne_out, int64_t* ni_out,
-                             int64_t* st_out, cudaStream_t st);
+                             int64_t* st_out, int64_t* lat_out, cudaStream_t st);
 
 size_t lbfgs_update_smem(int m);
 cudaError_t lbfgs_configure(size_t smem);
 cudaError_t lbfgs_init(const LbArgs& a, const double* s0, cudaStream_t st);
 cudaError_t lbfgs_update(const LbArgs& a, cudaStream_t st);
 cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double* gn_out,
-                           int64_t* ne_out, int64_t* ni_out, int64_t* st_out,
+                           int64_t* ne_out, int64_t* ni_out, int64_t* st_out, int64_t* lat_out,
                            cudaStream_t st);
 
 // Count lanes whose status is RUNNING (status stride in int64 units).

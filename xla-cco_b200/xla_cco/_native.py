@@ -72,7 +72,9 @@ class RelaxOutC(ctypes.Structure):
         ("traj_step", _vp),
         ("traj_iteration", _vp),
         ("traj_count", _vp),
+        ("latency_ns", _vp),
         ("ticks", ctypes.c_int64),
+        ("launches", ctypes.c_int64),
     ]
 
 

@@ -83,6 +83,7 @@ def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSet
         "n_evals": torch.empty(b, dtype=i64, device=dev),
         "n_iters": torch.empty(b, dtype=i64, device=dev),
         "status": torch.empty(b, dtype=i64, device=dev),
+        "latency_ns": torch.empty(b, dtype=i64, device=dev),
     }
     rec = settings.record_every > 0 and settings.max_records > 0
     cap = int(settings.max_records)
@@ -93,7 +94,7 @@ def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSet
         out["traj_iteration"] = torch.zeros((b, cap), dtype=i64, device=dev)
         out["traj_count"] = torch.zeros(b, dtype=i64, device=dev)
     co = _native.RelaxOutC()
-    for key in ("s", "energy", "grad_norm", "n_evals", "n_iters", "status"):
+    for key in ("s", "energy", "grad_norm", "n_evals", "n_iters", "status", "latency_ns"):
         setattr(co, key, out[key].data_ptr())
     if rec:
         for key in ("traj_s", "traj_energy", "traj_step", "traj_iteration", "traj_count"):
@@ -108,6 +109,7 @@ def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSet
         raise RuntimeError("relax did not finish within the round bound")
     _native.check(code, fn)
     out["ticks"] = int(co.ticks)
+    out["launches"] = int(co.launches)
     return out
 
 
@@ -127,8 +129,13 @@ def relax(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
     if not isinstance(settings, (DescentSettings, LBFGSSettings)):
         raise TypeError(f"unsupported settings type {type(settings).__name__}")
     _native.require_gpu()
-    host = not (isinstance(s0, torch.Tensor) and s0.is_cuda)
-    s_dev = torch.from_numpy(np.ascontiguousarray(np.asarray(s0))).cuda() if host else s0.contiguous()
+    if isinstance(s0, torch.Tensor):
+        host = not s0.is_cuda
+        # a pinned host tensor is copied asynchronously on the current stream
+        s_dev = s0.cuda(non_blocking=True) if host else s0.contiguous()
+    else:
+        host = True
+        s_dev = torch.from_numpy(np.ascontiguousarray(np.asarray(s0))).cuda()
     out = relax_device(energy, s_dev, settings, chunk_iters)
     conv = (lambda t: t.cpu().numpy()) if host else (lambda t: t)
     traj = None
