@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -68,47 +69,77 @@ struct cco_problem {
 namespace {
 
 // ----------------------------------------------------------- problem build
-struct Digits {
-  int nlev, base;
-  int nent[kMaxLevels];
-};
-
-// Digit tables for |n| <= R on one axis: 1 level (z^0..z^R) for small R,
-// otherwise 2 or 3 levels of base b with b^levels > R. Level 0 always holds
-// z^0..z^(b-1); the run axis needs z^1 there, so its base is >= 2.
-Digits choose_digits(int R, bool run_axis) {
-  Digits g{};
+// Digit layout of one axis for |n| <= R with `nlev` levels: base b with
+// b^nlev > R; level 0 holds z^0..z^(b-1) (the run axis needs z^1, so b >= 2
+// there), the top level holds R / b^(nlev-1) + 1 entries.
+void set_axis(TabLayout& T, int a, int R, int nlev, bool run_axis) {
   const int nv = R + 1;
-  if (nv <= 16) {
-    g.nlev = 1;
-    g.base = std::max(nv, run_axis ? 2 : 1);
-    g.nent[0] = g.base;
-    return g;
+  int b = 1;
+  if (nlev == 1) {
+    b = std::max(nv, run_axis ? 2 : 1);
+  } else {
+    b = std::max(2, (int)std::floor(std::pow((double)nv, 1.0 / nlev)));
+    auto pw = [&](int x) { long long r = 1; for (int l = 0; l < nlev; ++l) r *= x; return r; };
+    while (pw(b) < nv) ++b;
   }
-  g.nlev = nv <= 1024 ? 2 : 3;
-  g.base = (int)std::ceil(std::pow((double)nv, 1.0 / g.nlev));
-  while ((g.nlev == 2 ? g.base * g.base : g.base * g.base * g.base) < nv) ++g.base;
-  int scale = 1;
-  for (int l = 0; l < g.nlev - 1; ++l) {
-    g.nent[l] = g.base;
-    scale *= g.base;
+  T.nlev[a] = nlev;
+  T.base[a] = b;
+  long long scale = 1;
+  for (int l = 0; l < kMaxLevels; ++l) {
+    if (l >= nlev) T.nent[a][l] = 0;
+    else if (l == nlev - 1) T.nent[a][l] = (int)(R / scale) + 1;
+    else T.nent[a][l] = b;
+    if (l == 0 && nlev == 1) T.nent[a][0] = b;
+    scale *= b;
   }
-  g.nent[g.nlev - 1] = R / scale + 1;
-  return g;
 }
 
-int pack_digits(int v, const Digits& g) {
-  const int neg = v < 0;
-  int a = v < 0 ? -v : v;
-  int out = 0;
-  for (int l = 0; l < g.nlev; ++l) {
-    int dl;
-    if (l == g.nlev - 1) dl = a;
-    else {
-      dl = a % g.base;
-      a /= g.base;
+void assign_rows(TabLayout& T, int d) {
+  int row = 0;
+  for (int a = 0; a < 3; ++a)
+    for (int l = 0; l < kMaxLevels; ++l) {
+      T.row[a][l] = row;
+      if (a < d && l < T.nlev[a]) row += T.nent[a][l];
     }
-    out |= (dl & 255) << (8 * l);
+  T.nrows = row;
+  T.zrow = T.row[d - 1][0] + 1;
+}
+
+// Fewest table lookups whose rows fit `max_rows`: start with one level per
+// axis (one load per lookup) and add a level to the axis with the most rows
+// until the table fits (or every axis has kMaxLevels levels).
+TabLayout make_layout(const int* R, int d, int max_rows) {
+  TabLayout T{};
+  int lev[3] = {1, 1, 1};
+  for (;;) {
+    for (int a = 0; a < d; ++a) set_axis(T, a, R[a], lev[a], a == d - 1);
+    assign_rows(T, d);
+    if (T.nrows <= max_rows) break;
+    int best = -1, most = 0;
+    for (int a = 0; a < d; ++a) {
+      int rows = 0;
+      for (int l = 0; l < lev[a]; ++l) rows += T.nent[a][l];
+      if (lev[a] < kMaxLevels && rows > most) { most = rows; best = a; }
+    }
+    if (best < 0) break;
+    ++lev[best];
+  }
+  return T;
+}
+
+// Absolute table rows of the digits of v on axis a (+ sign bit 24).
+int pack_rows(int v, const TabLayout& T, int a) {
+  const int neg = v < 0;
+  int x = v < 0 ? -v : v;
+  int out = 0;
+  for (int l = 0; l < T.nlev[a]; ++l) {
+    int dl;
+    if (l == T.nlev[a] - 1) dl = x;
+    else {
+      dl = x % T.base[a];
+      x /= T.base[a];
+    }
+    out |= ((T.row[a][l] + dl) & 255) << (8 * l);
   }
   return out | (neg << 24);
 }
@@ -191,47 +222,33 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
       same &= n_vectors[(size_t)order[k] * d + a] == n_vectors[(size_t)order[k - 1] * d + a];
     if (same) return fail(CCO_ERR_ARG, "duplicate k row (rows %d and %d)", order[k - 1], order[k]);
   }
-  Digits dg[3];
-  for (int a = 0; a < d; ++a) dg[a] = choose_digits(R[a], a == d - 1);
-
   ProbDev P{};
   P.d = d;
   P.N = n_particles;
   P.M = m;
-  int row = 0;
-  for (int a = 0; a < 3; ++a) {
-    if (a < d) {
-      P.nlev[a] = dg[a].nlev;
-      P.base[a] = dg[a].base;
-      for (int l = 0; l < kMaxLevels; ++l) {
-        P.nent[a][l] = l < dg[a].nlev ? dg[a].nent[l] : 0;
-        P.row[a][l] = row;
-        if (l < dg[a].nlev) row += dg[a].nent[l];
-      }
-    } else {
-      P.nlev[a] = 1;
-      P.base[a] = 1;
-    }
+  {
+    const int Rv[3] = {R[0], R[1], R[2]};
+    P.t1 = make_layout(Rv, d, (int)(kPass1TableBudget / (kPass1Stride * sizeof(double2))));
+    P.t2 = make_layout(Rv, d, (int)(kPass2TableBudget / (kPass2Tile * sizeof(double2))));
   }
-  P.nrows = row;
+  if (P.t1.nrows > 255 || P.t2.nrows > 255)
+    return fail(CCO_ERR_ARG, "k-set phase tables too large (%d / %d rows)", P.t1.nrows, P.t2.nrows);
   P.ntile1 = (n_particles + kPass1Tile - 1) / kPass1Tile;
   P.ntile2 = (n_particles + kPass2Tile - 1) / kPass2Tile;
   P.vol = volume;
   P.gpref = (2.0 * (2.0 * M_PI)) / volume;
 
-  // runs -> segments
+  // runs -> segments (headers carry each pass's absolute table rows)
   std::vector<SegHdr> s1, s2;
-  auto emit = [&](std::vector<SegHdr>& dst, int kstart, int len, int maxlen) {
+  auto emit = [&](std::vector<SegHdr>& dst, const TabLayout& T, int kstart, int len, int maxlen) {
     for (int off = 0; off < len; off += maxlen) {
       SegHdr h{};
       h.kstart = kstart + off;
       h.len = std::min(maxlen, len - off);
       const int* nv = n_vectors + (size_t)order[h.kstart] * d;
-      for (int a = 0; a < 3; ++a) {
-        if (a < d) {
-          h.n[a] = nv[a];
-          h.dig[a] = pack_digits(nv[a], dg[a]);
-        }
+      for (int a = 0; a < d; ++a) {
+        h.n[a] = nv[a];
+        h.dig[a] = pack_rows(nv[a], T, a);
       }
       dst.push_back(h);
     }
@@ -246,19 +263,23 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
       brk |= c[d - 1] != p[d - 1] + 1;
     }
     if (brk) {
-      emit(s1, start, k - start, kSeg1Len);
-      emit(s2, start, k - start, kSeg2Len);
+      emit(s1, P.t1, start, k - start, kSeg1Len);
+      emit(s2, P.t2, start, k - start, kSeg2Len);
       start = k;
     }
   }
-  // longest pass-1 segments first: a warp's threads then share a trip count
-  std::stable_sort(s1.begin(), s1.end(), [](const SegHdr& x, const SegHdr& y) { return x.len > y.len; });
+  // longest segments first: pass-1 warps share trip counts, pass 2 pairs
+  // segments of similar length
+  auto by_len = [](const SegHdr& x, const SegHdr& y) { return x.len > y.len; };
+  std::stable_sort(s1.begin(), s1.end(), by_len);
+  std::stable_sort(s2.begin(), s2.end(), by_len);
   P.nseg1 = (int)s1.size();
   P.nseg2 = (int)s2.size();
 
   const size_t smem1 = eval_smem1(P), smem2 = eval_smem2(P);
   if (smem1 > 220 * 1024 || smem2 > 220 * 1024)
-    return fail(CCO_ERR_ARG, "k-set digit tables too large for shared memory (%d rows)", P.nrows);
+    return fail(CCO_ERR_ARG, "k-set phase tables too large for shared memory (%d / %d rows)",
+                P.t1.nrows, P.t2.nrows);
 
   DeviceGuard guard(device);
   static std::once_flag once;
@@ -323,7 +344,7 @@ int cco_problem_info(const cco_problem* p, int* d, int* n_particles, int* m, int
   if (m) *m = p->M;
   if (n_seg1) *n_seg1 = p->host.nseg1;
   if (n_seg2) *n_seg2 = p->host.nseg2;
-  if (table_rows) *table_rows = p->host.nrows;
+  if (table_rows) *table_rows = p->host.t1.nrows * 256 + p->host.t2.nrows;
   return CCO_OK;
 }
 
@@ -439,12 +460,23 @@ namespace {
 
 // Runs ticks (one evaluation + one update per running lane) in captured CUDA
 // graphs of kGraphTicks ticks until no lane is RUNNING or the tick bound is
-// reached. Completion is checked one graph behind so the device never idles
-// on the host.
+// reached. The lanes are split into `nbr` independent branches of the graph:
+// a branch's FP64-bound evaluation overlaps another branch's HBM-bound
+// minimizer update on the device. Completion is checked one graph behind so
+// the device never idles on the host.
 constexpr int kGraphTicks = 16;
+constexpr int kMaxBranches = 4;
+
+int branch_count(int B) {
+  int nbr = 2;
+  if (const char* env = getenv("CCO_BRANCHES")) nbr = atoi(env);
+  nbr = std::max(1, std::min(nbr, kMaxBranches));
+  while (nbr > 1 && B / nbr < 32) --nbr;
+  return nbr;
+}
 
 template <class TickFn>
-int run_ticks(cudaStream_t st, TickFn tick, const int64_t* status, size_t stride, int B,
+int run_ticks(cudaStream_t st, int nbr, TickFn tick, const int64_t* status, size_t stride, int B,
               int64_t max_ticks, int64_t* ticks_out) {
   int* d_count = nullptr;
   int* h_count = nullptr;
@@ -456,13 +488,24 @@ int run_ticks(cudaStream_t st, TickFn tick, const int64_t* status, size_t stride
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int rc = CCO_OK;
-  // capture kGraphTicks ticks on a side stream ordered after `st`
-  cudaStream_t cap;
-  CCO_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-  cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  // capture kGraphTicks ticks of every branch; branches fork from and join
+  // back into the first capture stream
+  cudaStream_t cap[kMaxBranches];
+  cudaEvent_t fork, join[kMaxBranches];
+  for (int b = 0; b < nbr; ++b) CCO_CUDA(cudaStreamCreateWithFlags(&cap[b], cudaStreamNonBlocking));
+  CCO_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  for (int b = 0; b < nbr; ++b) CCO_CUDA(cudaEventCreateWithFlags(&join[b], cudaEventDisableTiming));
+  cudaError_t e = cudaStreamBeginCapture(cap[0], cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    for (int t = 0; t < kGraphTicks && e == cudaSuccess; ++t) e = tick(cap);
-    cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+    e = cudaEventRecord(fork, cap[0]);
+    for (int b = 1; b < nbr && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(cap[b], fork, 0);
+    for (int t = 0; t < kGraphTicks && e == cudaSuccess; ++t)
+      for (int b = 0; b < nbr && e == cudaSuccess; ++b) e = tick(cap[b], b);
+    for (int b = 1; b < nbr && e == cudaSuccess; ++b) {
+      e = cudaEventRecord(join[b], cap[b]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(cap[0], join[b], 0);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(cap[0], &graph);
     if (e == cudaSuccess) e = e2;
   }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
@@ -497,7 +540,11 @@ int run_ticks(cudaStream_t st, TickFn tick, const int64_t* status, size_t stride
   else if (!done) rc = fail(CCO_ERR_ROUNDS, "relax did not finish within the round bound (%lld ticks)", (long long)max_ticks);
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
-  cudaStreamDestroy(cap);
+  for (int b = 0; b < nbr; ++b) {
+    cudaStreamDestroy(cap[b]);
+    cudaEventDestroy(join[b]);
+  }
+  cudaEventDestroy(fork);
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
   cudaFreeAsync(d_count, st);
@@ -505,6 +552,45 @@ int run_ticks(cudaStream_t st, TickFn tick, const int64_t* status, size_t stride
   cudaFreeHost(h_count);
   if (ticks_out) *ticks_out = ticks;
   return rc;
+}
+
+// Argument blocks of lanes [lo, lo + nb): every lane array is lane-major.
+DescentArgs descent_shift(const DescentArgs& a, int lo, int nb) {
+  DescentArgs r = a;
+  const size_t v = (size_t)lo * a.nd;
+  r.B = nb;
+  r.s += v; r.g += v; r.ps += v; r.pg += v;
+  r.pf += lo; r.f += lo; r.step += lo; r.norm += lo;
+  r.it += lo; r.n_evals += lo; r.status += lo; r.phase += lo; r.nonzero += lo;
+  r.t0 += lo; r.t1 += lo;
+  if (a.traj_count) {
+    r.traj_s += (size_t)lo * a.rec_cap * a.nd;
+    r.traj_e += (size_t)lo * a.rec_cap;
+    r.traj_step += (size_t)lo * a.rec_cap;
+    r.traj_it += (size_t)lo * a.rec_cap;
+    r.traj_count += lo;
+  }
+  return r;
+}
+
+LbArgs lbfgs_shift(const LbArgs& A, int lo, int nb) {
+  LbArgs r = A;
+  const size_t v = (size_t)lo * A.ld;
+  r.B = nb;
+  r.st += lo;
+  r.x += v; r.s += v; r.g += v; r.dir += v; r.glo += v; r.ps += v; r.pg += v;
+  r.pf += lo;
+  r.Sh += v * A.m; r.Yh += v * A.m;
+  r.SYs += (size_t)lo * A.m * A.m; r.YYs += (size_t)lo * A.m * A.m;
+  if (r.tri_g) r.tri_g += (size_t)lo * ((size_t)A.m * (A.m + 1) + 7 * (size_t)A.m);
+  if (A.traj_count) {
+    r.traj_s += (size_t)lo * A.rec_cap * A.nd;
+    r.traj_e += (size_t)lo * A.rec_cap;
+    r.traj_step += (size_t)lo * A.rec_cap;
+    r.traj_it += (size_t)lo * A.rec_cap;
+    r.traj_count += lo;
+  }
+  return r;
 }
 
 bool out_ok(const cco_relax_out* o) {
@@ -574,26 +660,33 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
     a.traj_it = out->traj_iteration;
     a.traj_count = out->traj_count;
   }
-  EvalWS ws;
-  CCO_CUDA(ws.alloc(p, B, st));
-  CCO_CUDA(ws.build(p, B, a.ps, nd, pf, 1, pg, nd, a.status, 1, st));
+  const int nbr = branch_count(B);
+  EvalWS ws[kMaxBranches];
+  DescentArgs ab[kMaxBranches];
+  for (int b = 0; b < nbr; ++b) {
+    const int lo = b * B / nbr, nb = (b + 1) * B / nbr - lo;
+    ab[b] = descent_shift(a, lo, nb);
+    CCO_CUDA(ws[b].alloc(p, nb, st));
+    CCO_CUDA(ws[b].build(p, nb, ab[b].ps, nd, pf + lo, 1, pg + (size_t)lo * nd, nd,
+                         a.status + lo, 1, st));
+  }
   CCO_CUDA(descent_init(a, s0, st));
-  auto tick = [&](cudaStream_t s) -> cudaError_t {
-    cudaError_t e = eval_launch(ws.plan, s);
-    if (e == cudaSuccess) e = descent_update(a, s);
+  auto tick = [&](cudaStream_t s, int b) -> cudaError_t {
+    cudaError_t e = eval_launch(ws[b].plan, s);
+    if (e == cudaSuccess) e = descent_update(ab[b], s);
     return e;
   };
   const int64_t max_ticks = 1 + a.max_iters + kGraphTicks;
   int64_t ticks = 0;
-  int rc = run_ticks(st, tick, a.status, 1, B, max_ticks, &ticks);
+  int rc = run_ticks(st, nbr, tick, a.status, 1, B, max_ticks, &ticks);
   if (rc == CCO_OK) {
     cudaError_t e = descent_finalize(a, out->s, out->energy, out->grad_norm, out->n_evals,
                                      out->n_iters, out->status, out->latency_ns, st);
     if (e != cudaSuccess) rc = cuda_fail(e, "descent_finalize");
   }
   out->ticks = ticks;
-  out->launches = ticks * 4 + ticks / kGraphTicks + 3;
-  ws.release(st);
+  out->launches = ticks * 4 * nbr + ticks / kGraphTicks + 2 + nbr;
+  for (int b = 0; b < nbr; ++b) ws[b].release(st);
   cudaFreeAsync(vec, st);
   cudaFreeAsync(sc, st);
   cudaFreeAsync(ic, st);
@@ -621,12 +714,14 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   cudaStream_t st = (cudaStream_t)stream;
   const int B = batch;
   const size_t nd = (size_t)p->N * p->d;
+  const size_t ld = (nd + 3) & ~(size_t)3;  // 32-byte rows, zero padding
   const int m = (int)cfg->memory;
   LbArgs A{};
   A.B = B;
   A.N = p->N;
   A.d = p->d;
   A.nd = (int)nd;
+  A.ld = (int)ld;
   A.m = m;
   A.n_pass = cfg->n_rescales;
   for (int i = 0; i < CCO_MAX_RESCALES; ++i) A.rescales[i] = i < cfg->n_rescales ? cfg->rescales[i] : 1.0;
@@ -656,23 +751,24 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   double* pf = nullptr;
   double* trig = nullptr;
   CCO_CUDA(cudaMallocAsync(&stv, sizeof(LbState) * B, st));
-  CCO_CUDA(cudaMallocAsync(&vec, sizeof(double) * nd * B * 7, st));
-  CCO_CUDA(cudaMallocAsync(&hist, sizeof(double) * nd * B * m * 2, st));
+  CCO_CUDA(cudaMallocAsync(&vec, sizeof(double) * ld * B * 7, st));
+  CCO_CUDA(cudaMemsetAsync(vec, 0, sizeof(double) * ld * B * 7, st));
+  CCO_CUDA(cudaMallocAsync(&hist, sizeof(double) * ld * B * m * 2, st));
   CCO_CUDA(cudaMallocAsync(&dots, sizeof(double) * (size_t)B * m * m * 2, st));
   CCO_CUDA(cudaMallocAsync(&pf, sizeof(double) * B, st));
   if (!in_smem) CCO_CUDA(cudaMallocAsync(&trig, tri_bytes * B, st));
   A.st = stv;
   A.x = vec;
-  A.s = vec + nd * B;
-  A.g = vec + 2 * nd * B;
-  A.dir = vec + 3 * nd * B;
-  A.glo = vec + 4 * nd * B;
-  A.ps = vec + 5 * nd * B;
-  double* pg = vec + 6 * nd * B;
+  A.s = vec + ld * B;
+  A.g = vec + 2 * ld * B;
+  A.dir = vec + 3 * ld * B;
+  A.glo = vec + 4 * ld * B;
+  A.ps = vec + 5 * ld * B;
+  double* pg = vec + 6 * ld * B;
   A.pg = pg;
   A.pf = pf;
   A.Sh = hist;
-  A.Yh = hist + nd * B * m;
+  A.Yh = hist + ld * B * m;
   A.SYs = dots;
   A.YYs = dots + (size_t)B * m * m;
   A.tri_g = trig;
@@ -685,28 +781,35 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   }
   const size_t st_stride = sizeof(LbState) / sizeof(int64_t);
   const int64_t* status0 = &stv->status;
-  EvalWS ws;
-  CCO_CUDA(ws.alloc(p, B, st));
-  CCO_CUDA(ws.build(p, B, A.ps, nd, pf, 1, pg, nd, status0, st_stride, st));
+  const int nbr = branch_count(B);
+  EvalWS ws[kMaxBranches];
+  LbArgs Ab[kMaxBranches];
+  for (int b = 0; b < nbr; ++b) {
+    const int lo = b * B / nbr, nb = (b + 1) * B / nbr - lo;
+    Ab[b] = lbfgs_shift(A, lo, nb);
+    CCO_CUDA(ws[b].alloc(p, nb, st));
+    CCO_CUDA(ws[b].build(p, nb, Ab[b].ps, ld, pf + lo, 1, pg + (size_t)lo * ld, ld,
+                         status0 + (size_t)lo * st_stride, st_stride, st));
+  }
   CCO_CUDA(lbfgs_init(A, s0, st));
-  auto tick = [&](cudaStream_t s) -> cudaError_t {
-    cudaError_t e = eval_launch(ws.plan, s);
-    if (e == cudaSuccess) e = lbfgs_update(A, s);
+  auto tick = [&](cudaStream_t s, int b) -> cudaError_t {
+    cudaError_t e = eval_launch(ws[b].plan, s);
+    if (e == cudaSuccess) e = lbfgs_update(Ab[b], s);
     return e;
   };
   const int64_t max_ticks =
       1 + (int64_t)cfg->n_rescales * (cfg->max_evals_per_pass + cfg->max_linesearch_steps + 1) +
       kGraphTicks;
   int64_t ticks = 0;
-  int rc = run_ticks(st, tick, status0, st_stride, B, max_ticks, &ticks);
+  int rc = run_ticks(st, nbr, tick, status0, st_stride, B, max_ticks, &ticks);
   if (rc == CCO_OK) {
     cudaError_t e = lbfgs_finalize(A, out->s, out->energy, out->grad_norm, out->n_evals,
                                    out->n_iters, out->status, out->latency_ns, st);
     if (e != cudaSuccess) rc = cuda_fail(e, "lbfgs_finalize");
   }
   out->ticks = ticks;
-  out->launches = ticks * 4 + ticks / kGraphTicks + 3;
-  ws.release(st);
+  out->launches = ticks * 4 * nbr + ticks / kGraphTicks + 2 + nbr;
+  for (int b = 0; b < nbr; ++b) ws[b].release(st);
   cudaFreeAsync(stv, st);
   cudaFreeAsync(vec, st);
   cudaFreeAsync(hist, st);

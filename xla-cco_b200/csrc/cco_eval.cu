@@ -7,27 +7,29 @@
 //
 // B200 formulation. The k-set is stored as runs of consecutive last-axis n
 // with a fixed prefix (n_0..n_{d-2}); along a run the phase advances by one
-// complex multiply, exp(i th_{k+1,j}) = exp(i th_kj) z_j with
-// z_j = exp(2 pi i s_{j,d-1}). A run start takes its phase from per-particle
-// digit tables in shared memory: z_a^|n| = prod_l T_a,l[digit_l(|n|)], level 0
-// built by products of z (<= base factors) and higher levels from FP64 sincospi
-// of the exact exponent, so a phase carries O((base + run length) eps) error,
-// well inside the reference's eps |theta| trig error. No theta matrix ever
-// reaches HBM; HBM traffic per evaluation is s in, g out and the M-row
-// density, so the kernels are FP64-pipe bound (SURVEY roofline).
+// complex multiply, exp(i th_{k+1,j}) = exp(i th_kj) z_j, z_j = exp(2 pi i
+// s_{j,d-1}). A segment start takes its phase from per-particle tables in
+// shared memory: z_a^|n| = prod_l T_a,l[digit_l(|n|)]. Table entries come
+// from FP64 sincospi of the exact integer exponent, re-seeded every 8 entries
+// with products in between, so a phase carries O(10 eps) error on top of the
+// <= segment-length products along a run - inside the reference's eps |theta|
+// trig error. No theta matrix ever reaches HBM: traffic per evaluation is s
+// in, g out and the M-row density, so both passes are FP64-pipe bound.
 //
-//   pass 1 (k_pass1): CTA = (configuration, 128-particle tile). A thread owns
-//     a segment of <= 8 rows and streams the tile's particles, accumulating
-//     8 complex sums in registers (no cross-thread reduction). Small k-sets
-//     split the particles into slices reduced in a fixed order. Output: one
-//     partial density row per tile.
+//   pass 1 (k_pass1): CTA = (configuration, 64-particle tile), 128 threads.
+//     A thread owns a segment of <= 8 rows and streams the tile's particles
+//     four at a time (four independent phase chains), accumulating 8 complex
+//     sums in registers: no cross-thread reduction. Small k-sets split the
+//     particles into slices summed in a fixed order. Output: one partial
+//     density row per tile.
 //   reduce  (k_reduce): sums the tile rows in tile order (deterministic),
 //     forms rho, w rho and Phi (fixed-order block sum).
-//   pass 2 (k_pass2): CTA = (configuration, 128-particle tile); a thread owns
-//     2 particles and walks every segment (uniform across the CTA, density
-//     reads are broadcasts): per row one complex multiply, the coefficient
-//     w(Im rho cos - Re rho sin), and two FMA-class accumulations; prefix axes
-//     are weighted once per segment.
+//   pass 2 (k_pass2): CTA = (configuration, 128-particle tile), one particle
+//     per thread; the CTA walks the segments two at a time (two independent
+//     chains per thread; density reads are warp-uniform broadcasts, fetched
+//     two rows ahead). Per row: one complex multiply, the coefficient
+//     w(Im rho cos - Re rho sin) and two accumulations; prefix axes are
+//     weighted once per segment.
 #include <cstdio>
 
 #include "cco_internal.cuh"
@@ -36,90 +38,133 @@ namespace cco {
 
 namespace {
 
-struct Rows {
-  int r[3][kMaxLevels];
-  int nlev[3];
+template <int D>
+struct Levels {
+  int n[D];
 };
 
 template <int D>
-__device__ __forceinline__ Rows load_rows(const ProbDev& P) {
-  Rows R;
+__device__ __forceinline__ Levels<D> levels(const TabLayout& T) {
+  Levels<D> L;
 #pragma unroll
-  for (int a = 0; a < D; ++a) {
-    R.nlev[a] = P.nlev[a];
-#pragma unroll
-    for (int l = 0; l < kMaxLevels; ++l) R.r[a][l] = P.row[a][l];
-  }
-  return R;
+  for (int a = 0; a < D; ++a) L.n[a] = T.nlev[a];
+  return L;
 }
 
-// Digit tables of the tile's particles: row r holds one power of z_a for all
-// tj particles (stride >= tj). Particles past nj get s = 0 and are never read
-// back into a result.
+// Table entries (a, l, e) = z_a^(e base_a^l) of the tile's particles; units of
+// up to 8 entries, each seeded by FP64 sincospi of the exact exponent. Level 0
+// continues by products with z (error <= 8 eps), higher levels use one
+// sincospi per entry. Particles past nj get s = 0 and are never read back.
 template <int D>
-__device__ void build_tables(const ProbDev& P, const double* __restrict__ s,
-                             int j0, int nj, int tj, int stride, double2* tab) {
-  for (int u = threadIdx.x; u < D * tj; u += blockDim.x) {
-    const int a = u / tj, j = u - a * tj;
+__device__ void build_tables(const TabLayout& T, const double* __restrict__ s, int j0, int nj,
+                             int tj, int stride, double2* tab) {
+  int units = 0;
+#pragma unroll
+  for (int a = 0; a < D; ++a)
+    for (int l = 0; l < T.nlev[a]; ++l) units += (T.nent[a][l] + 7) >> 3;
+  for (int u = threadIdx.x; u < units * tj; u += blockDim.x) {
+    const int j = u % tj;
+    int q = u / tj, a = 0, l = 0, scale = 1;
+    for (;;) {
+      const int c = (T.nent[a][l] + 7) >> 3;
+      if (q < c) break;
+      q -= c;
+      scale *= T.base[a];
+      if (++l >= T.nlev[a]) { l = 0; scale = 1; ++a; }
+    }
     const double sv = (j < nj) ? s[(size_t)(j0 + j) * D + a] : 0.0;
+    const int e0 = q * 8, e1 = min(e0 + 8, T.nent[a][l]);
     double sn, cs;
-    sincospi(2.0 * sv, &sn, &cs);
-    const double2 z = make_double2(cs, sn);
-    double2 p = make_double2(1.0, 0.0);
-    const int r0 = P.row[a][0];
-    const int n0 = P.nent[a][0];
-    for (int e = 0; e < n0; ++e) {
-      tab[(r0 + e) * stride + j] = p;
-      p = cmul(p, z);
-    }
-    int scale = P.base[a];
-    for (int l = 1; l < P.nlev[a]; ++l) {
-      const int rl = P.row[a][l];
-      const int nl = P.nent[a][l];
-      for (int e = 0; e < nl; ++e) {
-        const double t = (double)(e * scale) * sv;
-        sincospi(2.0 * t, &sn, &cs);
-        tab[(rl + e) * stride + j] = make_double2(cs, sn);
+    double2* out = tab + (size_t)T.row[a][l] * stride + j;
+    if (l == 0) {
+      sincospi(2.0 * sv, &sn, &cs);
+      const double2 z = make_double2(cs, sn);
+      sincospi(2.0 * ((double)e0 * sv), &sn, &cs);
+      double2 p = make_double2(cs, sn);
+      for (int e = e0; e < e1; ++e) {
+        out[(size_t)e * stride] = p;
+        p = cmul(p, z);
       }
-      scale *= P.base[a];
+    } else {
+      for (int e = e0; e < e1; ++e) {
+        sincospi(2.0 * ((double)(e * scale) * sv), &sn, &cs);
+        out[(size_t)e * stride] = make_double2(cs, sn);
+      }
     }
   }
 }
 
-// exp(2 pi i n . s_j) at a segment start, from the digit tables.
+// exp(2 pi i n . s_j) at a segment start, from the tables.
 template <int D>
-__device__ __forceinline__ double2 start_phase(const Rows& R, const SegHdr& h,
+__device__ __forceinline__ double2 start_phase(const Levels<D>& L, const SegHdr& h,
                                                const double2* tab, int stride, int j) {
   double2 ph = make_double2(1.0, 0.0);
 #pragma unroll
   for (int a = 0; a < D; ++a) {
     const int dg = h.dig[a];
-    double2 f = tab[(R.r[a][0] + (dg & 255)) * stride + j];
-#pragma unroll
-    for (int l = 1; l < kMaxLevels; ++l) {
-      if (l < R.nlev[a]) f = cmul(f, tab[(R.r[a][l] + ((dg >> (8 * l)) & 255)) * stride + j]);
-    }
+    double2 f = tab[(dg & 255) * stride + j];
+    if (L.n[a] > 1) f = cmul(f, tab[((dg >> 8) & 255) * stride + j]);
+    if (L.n[a] > 2) f = cmul(f, tab[((dg >> 16) & 255) * stride + j]);
     if (dg >> 24) f.y = -f.y;
     ph = (a == 0) ? f : cmul(ph, f);
   }
   return ph;
 }
 
+// Pass-1 accumulation of one segment over the particles j = j, j + ns, ...
+// FULL: the segment has exactly kSeg1Len rows (no per-row predicate).
+template <int D, bool FULL>
+__device__ __forceinline__ void seg_sum(const Levels<D>& L, const SegHdr& h, const double2* tab,
+                                        int zrow, int j, int ns, int nj, double2 (&acc)[kSeg1Len]) {
+  constexpr int S = kPass1Stride;
+  const int len = h.len;
+  for (; j + 3 * ns < nj; j += 4 * ns) {
+    double2 p0 = start_phase<D>(L, h, tab, S, j);
+    double2 p1 = start_phase<D>(L, h, tab, S, j + ns);
+    double2 p2 = start_phase<D>(L, h, tab, S, j + 2 * ns);
+    double2 p3 = start_phase<D>(L, h, tab, S, j + 3 * ns);
+    const double2 z0 = tab[zrow * S + j], z1 = tab[zrow * S + j + ns];
+    const double2 z2 = tab[zrow * S + j + 2 * ns], z3 = tab[zrow * S + j + 3 * ns];
+#pragma unroll
+    for (int i = 0; i < kSeg1Len; ++i) {
+      if (FULL || i < len) {
+        acc[i].x += (p0.x + p1.x) + (p2.x + p3.x);
+        acc[i].y += (p0.y + p1.y) + (p2.y + p3.y);
+        p0 = cmul(p0, z0);
+        p1 = cmul(p1, z1);
+        p2 = cmul(p2, z2);
+        p3 = cmul(p3, z3);
+      }
+    }
+  }
+  for (; j < nj; j += ns) {
+    double2 p0 = start_phase<D>(L, h, tab, S, j);
+    const double2 z0 = tab[zrow * S + j];
+#pragma unroll
+    for (int i = 0; i < kSeg1Len; ++i) {
+      if (FULL || i < len) {
+        acc[i].x += p0.x;
+        acc[i].y += p0.y;
+        p0 = cmul(p0, z0);
+      }
+    }
+  }
+}
+
 template <int D>
-__device__ void pass1_body(const ProbDev& P, const EvalLane& ln, int tile, double2* smem) {
-  const int tj = kPass1Tile, stride = kPass1Tile + 1;
-  const int j0 = tile * tj;
-  const int nj = min(tj, P.N - j0);
-  double2* tab = smem;
-  build_tables<D>(P, ln.s, j0, nj, tj, stride, tab);
-  const Rows R = load_rows<D>(P);
+__device__ void pass1_body(const ProbDev& P, const EvalLane& ln, int tile, double2* tab) {
+  const TabLayout& T = P.t1;
+  const int j0 = tile * kPass1Tile;
+  const int nj = min(kPass1Tile, P.N - j0);
+  build_tables<D>(T, ln.s, j0, nj, kPass1Tile, kPass1Stride, tab);
+  const Levels<D> L = levels<D>(T);
+  const int zrow = T.zrow;
   __syncthreads();
   const int nseg = P.nseg1;
-  int nslice = 1;
-  while (2 * nslice * nseg <= (int)blockDim.x && 2 * nslice <= nj) nslice *= 2;
-  const int units = nseg * nslice;
-  double2* red = tab + (size_t)P.nrows * stride;
-  const int zrow = R.r[D - 1][0] + 1;
+  int ns = 1;
+  while (2 * ns * nseg <= (int)blockDim.x && 2 * ns <= nj) ns *= 2;
+  const int units = nseg * ns;
+  double2* red = tab + (size_t)T.nrows * kPass1Stride;
   double2* out = ln.part + (size_t)tile * P.M;
   for (int u = threadIdx.x; u < units; u += blockDim.x) {
     const int sg = u % nseg, slice = u / nseg;
@@ -127,38 +172,11 @@ __device__ void pass1_body(const ProbDev& P, const EvalLane& ln, int tile, doubl
     double2 acc[kSeg1Len];
 #pragma unroll
     for (int i = 0; i < kSeg1Len; ++i) acc[i] = make_double2(0.0, 0.0);
-    int j = slice;
-    for (; j + nslice < nj; j += 2 * nslice) {
-      const int jb = j + nslice;
-      double2 pa = start_phase<D>(R, h, tab, stride, j);
-      double2 pb = start_phase<D>(R, h, tab, stride, jb);
-      const double2 za = tab[zrow * stride + j];
-      const double2 zb = tab[zrow * stride + jb];
-#pragma unroll
-      for (int i = 0; i < kSeg1Len; ++i) {
-        if (i < h.len) {
-          acc[i].x += pa.x;
-          acc[i].y += pa.y;
-          acc[i].x += pb.x;
-          acc[i].y += pb.y;
-          pa = cmul(pa, za);
-          pb = cmul(pb, zb);
-        }
-      }
-    }
-    if (j < nj) {
-      double2 pa = start_phase<D>(R, h, tab, stride, j);
-      const double2 za = tab[zrow * stride + j];
-#pragma unroll
-      for (int i = 0; i < kSeg1Len; ++i) {
-        if (i < h.len) {
-          acc[i].x += pa.x;
-          acc[i].y += pa.y;
-          pa = cmul(pa, za);
-        }
-      }
-    }
-    if (nslice == 1) {
+    if (h.len == kSeg1Len)
+      seg_sum<D, true>(L, h, tab, zrow, slice, ns, nj, acc);
+    else
+      seg_sum<D, false>(L, h, tab, zrow, slice, ns, nj, acc);
+    if (ns == 1) {
 #pragma unroll
       for (int i = 0; i < kSeg1Len; ++i)
         if (i < h.len) out[h.kstart + i] = acc[i];
@@ -167,14 +185,14 @@ __device__ void pass1_body(const ProbDev& P, const EvalLane& ln, int tile, doubl
       for (int i = 0; i < kSeg1Len; ++i) red[((size_t)slice * nseg + sg) * kSeg1Len + i] = acc[i];
     }
   }
-  if (nslice > 1) {
+  if (ns > 1) {
     __syncthreads();
     for (int v = threadIdx.x; v < nseg * kSeg1Len; v += blockDim.x) {
       const int sg = v / kSeg1Len, i = v - sg * kSeg1Len;
       const SegHdr h = P.seg1[sg];
       if (i < h.len) {
         double2 t = red[v];
-        for (int q = 1; q < nslice; ++q) {
+        for (int q = 1; q < ns; ++q) {
           const double2 o = red[(size_t)q * nseg * kSeg1Len + v];
           t.x += o.x;
           t.y += o.y;
@@ -185,68 +203,85 @@ __device__ void pass1_body(const ProbDev& P, const EvalLane& ln, int tile, doubl
   }
 }
 
-template <int D>
+// One row of the back-projection for one chain.
+__device__ __forceinline__ void bp_step(double2 r, double2& ph, double2 z, double di, double& S,
+                                        double& Tn) {
+  const double c = r.y * ph.x - r.x * ph.y;
+  S += c;
+  Tn += c * di;
+  ph = cmul(ph, z);
+}
+
+// STAGED: the lane's weighted density (M rows) is copied once into shared
+// memory after the tables and every row read is a shared-memory broadcast;
+// otherwise rows are read through L1 from global memory.
+template <int D, bool STAGED>
 __device__ void pass2_body(const ProbDev& P, const EvalLane& ln, int tile, double2* tab) {
-  constexpr int JB = kPass2PerThread;
-  const int tj = kPass2Tile, stride = kPass2Tile;
-  const int j0 = tile * tj;
-  const int nj = min(tj, P.N - j0);
-  build_tables<D>(P, ln.s, j0, nj, tj, stride, tab);
-  const Rows R = load_rows<D>(P);
-  __syncthreads();
-  const int zrow = R.r[D - 1][0] + 1;
-  int jl[JB];
-  double2 z[JB];
-  double G[JB][D];
-#pragma unroll
-  for (int b = 0; b < JB; ++b) {
-    jl[b] = threadIdx.x + b * blockDim.x;
-    z[b] = tab[zrow * stride + jl[b]];
-#pragma unroll
-    for (int a = 0; a < D; ++a) G[b][a] = 0.0;
-  }
+  const TabLayout& T = P.t2;
+  constexpr int S = kPass2Tile;
+  const int j0 = tile * kPass2Tile;
+  const int nj = min(kPass2Tile, P.N - j0);
   const double2* __restrict__ rw = ln.rhow;
-  for (int sg = 0; sg < P.nseg2; ++sg) {
-    const SegHdr h = P.seg2[sg];
-    double2 ph[JB];
-    double S[JB], T[JB];
-#pragma unroll
-    for (int b = 0; b < JB; ++b) {
-      ph[b] = start_phase<D>(R, h, tab, stride, jl[b]);
-      S[b] = 0.0;
-      T[b] = 0.0;
-    }
-    double nn = (double)h.n[D - 1];
-    const double2* rk = rw + h.kstart;
-    for (int i = 0; i < h.len; ++i) {
-      const double2 r = __ldg(rk + i);
-#pragma unroll
-      for (int b = 0; b < JB; ++b) {
-        const double c = r.y * ph[b].x - r.x * ph[b].y;
-        S[b] += c;
-        T[b] += c * nn;
-        ph[b] = cmul(ph[b], z[b]);
-      }
-      nn += 1.0;
-    }
-#pragma unroll
-    for (int b = 0; b < JB; ++b) {
-#pragma unroll
-      for (int a = 0; a < D - 1; ++a) G[b][a] += (double)h.n[a] * S[b];
-      G[b][D - 1] += T[b];
-    }
+  if (STAGED) {
+    double2* st = tab + (size_t)T.nrows * S;
+    for (int k = threadIdx.x; k < P.M; k += blockDim.x) st[k] = rw[k];
+    rw = st;
   }
+  build_tables<D>(T, ln.s, j0, nj, kPass2Tile, S, tab);
+  const Levels<D> L = levels<D>(T);
+  __syncthreads();
+  const int j = threadIdx.x;
+  const double2 z = tab[T.zrow * S + j];
+  double G[D];
 #pragma unroll
-  for (int b = 0; b < JB; ++b) {
-    if (jl[b] < nj) {
-      double* gj = ln.g + (size_t)(j0 + jl[b]) * D;
-#pragma unroll
-      for (int a = 0; a < D; ++a) gj[a] = P.gpref * G[b][a];
+  for (int a = 0; a < D; ++a) G[a] = 0.0;
+  const int nseg = P.nseg2;
+  for (int sg = 0; sg < nseg; sg += 2) {
+    const SegHdr hA = P.seg2[sg];
+    const SegHdr hB = P.seg2[min(sg + 1, nseg - 1)];
+    double2 pA = start_phase<D>(L, hA, tab, S, j);
+    double2 pB = start_phase<D>(L, hB, tab, S, j);
+    double SA = 0.0, TA = 0.0, SB = 0.0, TB = 0.0;
+    const double2* rA = rw + hA.kstart;
+    const double2* rB = rw + hB.kstart;
+    // la >= lb (segments sorted by length); an odd last segment pairs with nothing
+    const int la = hA.len, lb = (sg + 1 < nseg) ? hB.len : 0;
+    int i = 0;
+    double di = 0.0;
+    for (; i + 2 <= lb; i += 2) {
+      const double2 a0 = rA[i], a1 = rA[i + 1];
+      const double2 b0 = rB[i], b1 = rB[i + 1];
+      bp_step(a0, pA, z, di, SA, TA);
+      bp_step(b0, pB, z, di, SB, TB);
+      bp_step(a1, pA, z, di + 1.0, SA, TA);
+      bp_step(b1, pB, z, di + 1.0, SB, TB);
+      di += 2.0;
     }
+    if (i < lb) {
+      bp_step(rA[i], pA, z, di, SA, TA);
+      bp_step(rB[i], pB, z, di, SB, TB);
+      ++i;
+      di += 1.0;
+    }
+    for (; i + 2 <= la; i += 2) {
+      const double2 a0 = rA[i], a1 = rA[i + 1];
+      bp_step(a0, pA, z, di, SA, TA);
+      bp_step(a1, pA, z, di + 1.0, SA, TA);
+      di += 2.0;
+    }
+    if (i < la) bp_step(rA[i], pA, z, di, SA, TA);
+#pragma unroll
+    for (int a = 0; a < D - 1; ++a) G[a] += (double)hA.n[a] * SA + (double)hB.n[a] * SB;
+    G[D - 1] += ((double)hA.n[D - 1] * SA + TA) + ((double)hB.n[D - 1] * SB + TB);
+  }
+  if (j < nj) {
+    double* gj = ln.g + (size_t)(j0 + j) * D;
+#pragma unroll
+    for (int a = 0; a < D; ++a) gj[a] = P.gpref * G[a];
   }
 }
 
-__global__ void __launch_bounds__(kPass1Threads) k_pass1(EvalPlan plan) {
+__global__ void __launch_bounds__(kPass1Threads, 4) k_pass1(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
   const EvalItem it = plan.items1[blockIdx.x];
@@ -285,7 +320,7 @@ __global__ void __launch_bounds__(256) k_reduce(EvalPlan plan) {
   if (threadIdx.x == 0) *ln.f = e / P.vol;
 }
 
-__global__ void __launch_bounds__(kPass2Threads) k_pass2(EvalPlan plan) {
+__global__ void __launch_bounds__(kPass2Threads, 4) k_pass2(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
   const EvalItem it = plan.items2[blockIdx.x];
@@ -293,10 +328,19 @@ __global__ void __launch_bounds__(kPass2Threads) k_pass2(EvalPlan plan) {
   if (!lane_active(ln.status) || ln.g == nullptr) return;
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
-  switch (sp.d) {
-    case 1: pass2_body<1>(sp, ln, it.tile, smem); break;
-    case 2: pass2_body<2>(sp, ln, it.tile, smem); break;
-    default: pass2_body<3>(sp, ln, it.tile, smem); break;
+  const bool staged = (size_t)sp.M * sizeof(double2) <= kPass2RhoStage;
+  if (staged) {
+    switch (sp.d) {
+      case 1: pass2_body<1, true>(sp, ln, it.tile, smem); break;
+      case 2: pass2_body<2, true>(sp, ln, it.tile, smem); break;
+      default: pass2_body<3, true>(sp, ln, it.tile, smem); break;
+    }
+  } else {
+    switch (sp.d) {
+      case 1: pass2_body<1, false>(sp, ln, it.tile, smem); break;
+      case 2: pass2_body<2, false>(sp, ln, it.tile, smem); break;
+      default: pass2_body<3, false>(sp, ln, it.tile, smem); break;
+    }
   }
 }
 
@@ -315,14 +359,22 @@ __global__ void k_rho_scatter(const double2* __restrict__ rho, const int* __rest
 
 }  // namespace
 
-size_t eval_smem1(const ProbDev& p) {
-  int nslice = 1;
-  while (2 * nslice * p.nseg1 <= kPass1Threads && 2 * nslice <= kPass1Tile) nslice *= 2;
-  size_t red = nslice > 1 ? (size_t)nslice * p.nseg1 * kSeg1Len : 0;
-  return ((size_t)p.nrows * (kPass1Tile + 1) + red) * sizeof(double2);
+int pass1_slices(int nseg, int nj) {
+  int ns = 1;
+  while (2 * ns * nseg <= kPass1Threads && 2 * ns <= nj) ns *= 2;
+  return ns;
 }
 
-size_t eval_smem2(const ProbDev& p) { return (size_t)p.nrows * kPass2Tile * sizeof(double2); }
+size_t eval_smem1(const ProbDev& p) {
+  const int ns = pass1_slices(p.nseg1, kPass1Tile);
+  const size_t red = ns > 1 ? (size_t)ns * p.nseg1 * kSeg1Len : 0;
+  return ((size_t)p.t1.nrows * kPass1Stride + red) * sizeof(double2);
+}
+
+size_t eval_smem2(const ProbDev& p) {
+  const size_t rho = (size_t)p.M * sizeof(double2);
+  return (size_t)p.t2.nrows * kPass2Tile * sizeof(double2) + (rho <= kPass2RhoStage ? rho : 0);
+}
 
 cudaError_t eval_configure() {
   cudaError_t e = cudaFuncSetAttribute(k_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -333,8 +385,7 @@ cudaError_t eval_configure() {
 }
 
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream) {
-  if (plan.n_items1 > 0)
-    k_pass1<<<plan.n_items1, kPass1Threads, plan.smem1, stream>>>(plan);
+  if (plan.n_items1 > 0) k_pass1<<<plan.n_items1, kPass1Threads, plan.smem1, stream>>>(plan);
   if (plan.n_lanes > 0) k_reduce<<<plan.n_lanes, 256, 0, stream>>>(plan);
   if (plan.want_grad && plan.n_items2 > 0)
     k_pass2<<<plan.n_items2, kPass2Threads, plan.smem2, stream>>>(plan);

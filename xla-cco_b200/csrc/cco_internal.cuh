@@ -19,17 +19,21 @@ namespace cco {
 
 constexpr int kSeg1Len = 8;     // pass-1 segment length (register accumulators)
 constexpr int kSeg2Len = 256;   // pass-2 segment length (phase re-seed interval)
-constexpr int kPass1Threads = 256;
-constexpr int kPass1Tile = 128; // particles per pass-1 CTA
-constexpr int kPass2Threads = 64;
-constexpr int kPass2PerThread = 2;
-constexpr int kPass2Tile = kPass2Threads * kPass2PerThread;
+constexpr int kPass1Threads = 128;
+constexpr int kPass1Tile = 64;  // particles per pass-1 CTA
+constexpr int kPass1Stride = kPass1Tile + 1;  // padded table row (bank spread)
+constexpr int kPass2Threads = 128;
+constexpr int kPass2Tile = kPass2Threads;     // one particle per pass-2 thread
 constexpr int kMaxLevels = 3;
+constexpr size_t kPass1TableBudget = 56 * 1024;   // bytes of pass-1 tables per CTA
+constexpr size_t kPass2TableBudget = 44 * 1024;   // bytes of pass-2 tables per CTA
+constexpr size_t kPass2RhoStage = 24 * 1024;      // density staged in pass-2 smem up to this
 
 // One segment: rows kstart .. kstart+len-1 (run order) share the prefix
 // n_0..n_{d-2}; the last axis runs n_{d-1} = n[d-1] + i.
-// dig[a] packs the digit-table indices of |n_a| (start value for the last
-// axis): level l in bits 8l..8l+7, sign (n_a < 0) in bit 24.
+// dig[a] packs the absolute table rows of the digits of |n_a| (start value
+// for the last axis) in that pass's table layout: level l in bits 8l..8l+7,
+// sign (n_a < 0) in bit 24.
 struct SegHdr {
   int dig[3];
   int kstart;
@@ -38,19 +42,26 @@ struct SegHdr {
 };
 static_assert(sizeof(SegHdr) == 32, "segment header is two 16-byte loads");
 
+// Per-particle phase tables of one pass: row r holds z_a^(e * base^l) for one
+// (axis a, level l, entry e); level 0 always holds z^0 .. z^(base-1).
+struct TabLayout {
+  int nlev[3];
+  int base[3];
+  int nent[3][kMaxLevels];
+  int row[3][kMaxLevels];
+  int nrows;
+  int zrow;   // row of z^1 of the last axis
+};
+
 // Device-resident problem descriptor.
 struct ProbDev {
   int d, N, M, nseg1, nseg2;
-  int nlev[3];          // digit levels per axis
-  int base[3];          // digit base per axis
-  int nent[3][kMaxLevels];   // entries per level
-  int row[3][kMaxLevels];    // first table row of (axis, level)
-  int nrows;                 // table rows per particle
+  TabLayout t1, t2;          // pass-1 / pass-2 table layouts
   int ntile1, ntile2;        // particle tiles of pass 1 / pass 2
   double vol;                // V
   double gpref;              // 2 (2 pi) / V
   const SegHdr* seg1;
-  const SegHdr* seg2;
+  const SegHdr* seg2;        // sorted by length (pairs processed together)
   const double* w_run;
   const int* run2ref;
 };

@@ -280,8 +280,18 @@ __device__ __forceinline__ int tri(int p, int q) { return q * (q + 1) / 2 + p; }
 struct LbShared {
   LbState L;
   double red[32];
-  int outcome, new_lo;
+  int outcome, new_lo, advance;
 };
+
+// Lane vectors and history rows have a padded length ld (a multiple of 4
+// doubles, 16-byte aligned rows); padding entries stay zero, so every vector
+// loop runs over ld/2 double2 words without a tail.
+__device__ __forceinline__ double2 ld2(const double* p, int i) {
+  return reinterpret_cast<const double2*>(p)[i];
+}
+__device__ __forceinline__ void st2(double* p, int i, double2 v) {
+  reinterpret_cast<double2*>(p)[i] = v;
+}
 
 __device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double* s) {
   if (A.traj_count == nullptr) return;
@@ -308,18 +318,17 @@ __device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double*
 // Direction for the current (x, g) and the first probe at alpha = 1.
 __device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, double* tsm) {
   LbState& L = sh.L;
-  const int nd = A.nd, m = A.m;
-  const size_t off = (size_t)lane * nd;
+  const int ld = A.ld, h2 = A.ld >> 1, m = A.m;
+  const size_t off = (size_t)lane * ld;
   const double* g = A.g + off;
   const double* x = A.x + off;
   double* dir = A.dir + off;
   double* ps = A.ps + off;
-  const double* Sh = A.Sh + (size_t)lane * m * nd;
-  const double* Yh = A.Yh + (size_t)lane * m * nd;
+  const double* Sh = A.Sh + (size_t)lane * m * ld;
+  const double* Yh = A.Yh + (size_t)lane * m * ld;
   double* SYs = A.SYs + (size_t)lane * m * m;
   double* YYs = A.YYs + (size_t)lane * m * m;
   const int k = L.hk;
-  // scalar arrays live after the triangles
   double* triSY = tsm;
   double* triYY = tsm + (size_t)m * (m + 1) / 2;
   double* av = tsm + (size_t)m * (m + 1);
@@ -331,32 +340,51 @@ __device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, doub
   double* cs = cy + m;
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-  auto slot = [&](int p) { return (L.hhead - k + p + m) % m; };
+  const int head = L.hhead;
+  auto slot = [&](int p) { return (head - k + p + m) % m; };
 
-  // ---- pass A: a_p = s_p.g, b_p = y_p.g, and the new pair's column
+  // ---- pass A: a_p = s_p.g, b_p = y_p.g and the newest pair's column
+  //      (one warp per pair, four double2 words per lane in flight)
   if (k > 0) {
-    const int n = k - 1;
-    const int sn = slot(n);
-    const double* yn = Yh + (size_t)sn * nd;
+    const int sn = slot(k - 1);
+    const double* yn = Yh + (size_t)sn * ld;
     const bool np = L.newpair != 0;
     for (int p = warp; p < k; p += nwarps) {
       const int sp = slot(p);
-      const double* sr = Sh + (size_t)sp * nd;
-      const double* yr = Yh + (size_t)sp * nd;
+      const double* sr = Sh + (size_t)sp * ld;
+      const double* yr = Yh + (size_t)sp * ld;
       double ag = 0.0, bg = 0.0, sy = 0.0, yy = 0.0;
-      if (np) {
-        for (int e = wl; e < nd; e += 32) {
-          const double sv = sr[e], yv = yr[e], gv = g[e], ynv = yn[e];
-          ag += sv * gv;
-          bg += yv * gv;
-          sy += sv * ynv;
-          yy += yv * ynv;
+      int e = wl;
+      for (; e + 96 < h2; e += 128) {
+        double2 sv[4], yv[4], gv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          sv[u] = ld2(sr, e + 32 * u);
+          yv[u] = ld2(yr, e + 32 * u);
+          gv[u] = ld2(g, e + 32 * u);
         }
-      } else {
-        for (int e = wl; e < nd; e += 32) {
-          const double sv = sr[e], yv = yr[e], gv = g[e];
-          ag += sv * gv;
-          bg += yv * gv;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          ag += sv[u].x * gv[u].x + sv[u].y * gv[u].y;
+          bg += yv[u].x * gv[u].x + yv[u].y * gv[u].y;
+        }
+        if (np) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const double2 w = ld2(yn, e + 32 * u);
+            sy += sv[u].x * w.x + sv[u].y * w.y;
+            yy += yv[u].x * w.x + yv[u].y * w.y;
+          }
+        }
+      }
+      for (; e < h2; e += 32) {
+        const double2 sv = ld2(sr, e), yv = ld2(yr, e), gv = ld2(g, e);
+        ag += sv.x * gv.x + sv.y * gv.y;
+        bg += yv.x * gv.x + yv.y * gv.y;
+        if (np) {
+          const double2 w = ld2(yn, e);
+          sy += sv.x * w.x + sv.y * w.y;
+          yy += yv.x * w.x + yv.y * w.y;
         }
       }
 #pragma unroll
@@ -394,7 +422,10 @@ __device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, doub
   // ---- gamma (optax scale_by_lbfgs): newest pair, or min(1, 1/|g|) on a fresh pass
   if (k == 0) {
     double ss = 0.0;
-    for (int e = threadIdx.x; e < nd; e += blockDim.x) ss += g[e] * g[e];
+    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+      const double2 v = ld2(g, e);
+      ss += v.x * v.x + v.y * v.y;
+    }
     ss = block_sum(ss, sh.red);
     if (threadIdx.x == 0) L.gamma = fmin(1.0, 1.0 / sqrt(ss));
   } else if (threadIdx.x == 0) {
@@ -402,20 +433,43 @@ __device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, doub
     const double num = triSY[tri(n, n)], den = triYY[tri(n, n)];
     L.gamma = den > 0.0 ? num / den : 1.0;
   }
-  // ---- loops 1 and 2 on warp 0 (O(k^2) scalars, fixed order)
+  // ---- loops 1 and 2 on warp 0 (O(k^2) scalars, fixed order). Column-
+  //      oriented triangular solves: lane l keeps the running sums of pairs
+  //      p = l, l+32, ...; each solved alpha_q is broadcast once and folded
+  //      into every older row, so a step costs one shuffle, not a reduction.
+  constexpr int kRegRows = 8;  // k <= 256 in registers
   if (k > 0 && warp == 0) {
     for (int p = wl; p < k; p += 32) {
       const double ys = triSY[tri(p, p)];
       rh[p] = ys == 0.0 ? 0.0 : 1.0 / ys;
     }
     __syncwarp();
-    for (int p = k - 1; p >= 0; --p) {
-      double acc = 0.0;
-      for (int q = p + 1 + wl; q < k; q += 32) acc += alp[q] * triSY[tri(p, q)];
+    if (k <= 32 * kRegRows) {
+      double t[kRegRows];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (wl == 0) alp[p] = rh[p] * (av[p] - acc);
-      __syncwarp();
+      for (int i = 0; i < kRegRows; ++i) t[i] = (32 * i + wl < k) ? av[32 * i + wl] : 0.0;
+      for (int q = k - 1; q >= 0; --q) {
+        const int own = q & 31, oi = q >> 5;
+        double tq = 0.0;
+#pragma unroll
+        for (int i = 0; i < kRegRows; ++i) tq = (i == oi) ? t[i] : tq;
+        const double aq = __shfl_sync(0xffffffffu, rh[q] * tq, own);
+        if (wl == 0) alp[q] = aq;
+#pragma unroll
+        for (int i = 0; i < kRegRows; ++i) {
+          const int p = 32 * i + wl;
+          if (p < q) t[i] -= aq * triSY[tri(p, q)];
+        }
+      }
+    } else {
+      for (int p = k - 1; p >= 0; --p) {
+        double acc = 0.0;
+        for (int q = p + 1 + wl; q < k; q += 32) acc += alp[q] * triSY[tri(p, q)];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (wl == 0) alp[p] = rh[p] * (av[p] - acc);
+        __syncwarp();
+      }
     }
   }
   __syncthreads();
@@ -431,13 +485,39 @@ __device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, doub
     __syncthreads();
     if (warp == 0) {
       const double gam = L.gamma;
-      for (int p = 0; p < k; ++p) {
-        double acc = 0.0;
-        for (int q = wl; q < p; q += 32) acc += (alp[q] - bet[q]) * triSY[tri(q, p)];
+      if (k <= 32 * kRegRows) {
+        // u_p = sum_{q<p} (alpha_q - beta_q) SY[q][p], accumulated column-wise
+        double u[kRegRows];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (wl == 0) bet[p] = rh[p] * (gam * bet[p] + acc);
+        for (int i = 0; i < kRegRows; ++i) u[i] = 0.0;
+        for (int p = 0; p < k; ++p) {
+          const int own = p & 31, oi = p >> 5;
+          double up = 0.0;
+#pragma unroll
+          for (int i = 0; i < kRegRows; ++i) up = (i == oi) ? u[i] : up;
+          double dq = 0.0;
+          if (wl == own) {
+            const double bp = rh[p] * (gam * bet[p] + up);
+            bet[p] = bp;
+            dq = alp[p] - bp;
+          }
+          dq = __shfl_sync(0xffffffffu, dq, own);
+#pragma unroll
+          for (int i = 0; i < kRegRows; ++i) {
+            const int q = 32 * i + wl;
+            if (q > p && q < k) u[i] += dq * triSY[tri(p, q)];
+          }
+        }
         __syncwarp();
+      } else {
+        for (int p = 0; p < k; ++p) {
+          double acc = 0.0;
+          for (int q = wl; q < p; q += 32) acc += (alp[q] - bet[q]) * triSY[tri(q, p)];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+          if (wl == 0) bet[p] = rh[p] * (gam * bet[p] + acc);
+          __syncwarp();
+        }
       }
       for (int q = wl; q < k; q += 32) {
         cy[q] = gam * alp[q];
@@ -447,30 +527,37 @@ __device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, doub
     __syncthreads();
   }
   // ---- pass B: dir = -gamma g + sum cy_q y_q + sum cs_q s_q, first probe, g.dir
+  //      (one double2 word per thread, eight pairs = 16 loads in flight)
   const double gam = L.gamma, R = L.R;
   double dp = 0.0;
-  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-    const double ge = g[e];
-    double acc = 0.0;
+  for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+    double ax = 0.0, ay = 0.0;
     int q = 0;
-    for (; q + 4 <= k; q += 4) {
-      const size_t r0 = (size_t)slot(q) * nd + e, r1 = (size_t)slot(q + 1) * nd + e;
-      const size_t r2 = (size_t)slot(q + 2) * nd + e, r3 = (size_t)slot(q + 3) * nd + e;
-      const double y0 = Yh[r0], s0 = Sh[r0], y1 = Yh[r1], s1 = Sh[r1];
-      const double y2 = Yh[r2], s2 = Sh[r2], y3 = Yh[r3], s3 = Sh[r3];
-      acc += cy[q] * y0 + cs[q] * s0;
-      acc += cy[q + 1] * y1 + cs[q + 1] * s1;
-      acc += cy[q + 2] * y2 + cs[q + 2] * s2;
-      acc += cy[q + 3] * y3 + cs[q + 3] * s3;
+    for (; q + 8 <= k; q += 8) {
+      double2 yv[8], sv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const size_t r = (size_t)slot(q + u) * ld;
+        yv[u] = ld2(Yh + r, e);
+        sv[u] = ld2(Sh + r, e);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        ax += cy[q + u] * yv[u].x + cs[q + u] * sv[u].x;
+        ay += cy[q + u] * yv[u].y + cs[q + u] * sv[u].y;
+      }
     }
     for (; q < k; ++q) {
-      const size_t r = (size_t)slot(q) * nd + e;
-      acc += cy[q] * Yh[r] + cs[q] * Sh[r];
+      const size_t r = (size_t)slot(q) * ld;
+      const double2 yv = ld2(Yh + r, e), sv = ld2(Sh + r, e);
+      ax += cy[q] * yv.x + cs[q] * sv.x;
+      ay += cy[q] * yv.y + cs[q] * sv.y;
     }
-    const double de = acc - gam * ge;
-    dir[e] = de;
-    dp += ge * de;
-    ps[e] = (x[e] + 1.0 * de) / R;
+    const double2 gv = ld2(g, e), xv = ld2(x, e);
+    const double2 de = make_double2(ax - gam * gv.x, ay - gam * gv.y);
+    st2(dir, e, de);
+    dp += gv.x * de.x + gv.y * de.y;
+    st2(ps, e, make_double2((xv.x + 1.0 * de.x) / R, (xv.y + 1.0 * de.y) / R));
   }
   dp = block_sum(dp, sh.red);
   if (threadIdx.x == 0) {
@@ -490,8 +577,8 @@ __device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, doub
 
 __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double* tsm) {
   LbState& L = sh.L;
-  const int nd = A.nd, m = A.m;
-  const size_t off = (size_t)lane * nd;
+  const int ld = A.ld, h2 = A.ld >> 1, m = A.m;
+  const size_t off = (size_t)lane * ld;
   double* x = A.x + off;
   double* s = A.s + off;
   double* g = A.g + off;
@@ -507,17 +594,23 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double
     const bool probe = outcome == LS_ACCEPT_PROBE;
     const double al = probe ? L.alpha : L.a_lo;
     const int sl = L.hhead;
-    double* Sr = A.Sh + ((size_t)lane * m + sl) * nd;
-    double* Yr = A.Yh + ((size_t)lane * m + sl) * nd;
-    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-      const double xo = x[e];
-      const double xn = xo + al * dir[e];
-      const double gn = probe ? pg[e] / R : glo[e];
-      Sr[e] = xn - xo;
-      Yr[e] = gn - g[e];
-      x[e] = xn;
-      s[e] = xn / R;
-      g[e] = gn;
+    double* Sr = A.Sh + ((size_t)lane * m + sl) * ld;
+    double* Yr = A.Yh + ((size_t)lane * m + sl) * ld;
+    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+      const double2 xo = ld2(x, e), dv = ld2(dir, e), go = ld2(g, e);
+      const double2 xn = make_double2(xo.x + al * dv.x, xo.y + al * dv.y);
+      double2 gn;
+      if (probe) {
+        const double2 pv = ld2(pg, e);
+        gn = make_double2(pv.x / R, pv.y / R);
+      } else {
+        gn = ld2(glo, e);
+      }
+      st2(Sr, e, make_double2(xn.x - xo.x, xn.y - xo.y));
+      st2(Yr, e, make_double2(gn.x - go.x, gn.y - go.y));
+      st2(x, e, xn);
+      st2(s, e, make_double2(xn.x / R, xn.y / R));
+      st2(g, e, gn);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -533,7 +626,10 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double
   __syncthreads();
   // |g_s| = |g_x| R
   double ss = 0.0;
-  for (int e = threadIdx.x; e < nd; e += blockDim.x) ss += g[e] * g[e];
+  for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+    const double2 v = ld2(g, e);
+    ss += v.x * v.x + v.y * v.y;
+  }
   ss = block_sum(ss, sh.red);
   if (threadIdx.x == 0) {
     L.stag = (L.f < f_old) ? 0 : L.stag + 1;
@@ -554,15 +650,16 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double
     if (pass_end && last) status = local;
     L.status = status;
     if (status != CCO_STATUS_RUNNING) L.t1 = gtimer();
-    sh.new_lo = advance;  // reuse as the advance flag
+    sh.advance = advance;
   }
   __syncthreads();
-  if (sh.new_lo) {
+  if (sh.advance) {
     const int nx = min(L.pass_idx + 1, A.n_pass - 1);
     const double rn = A.rescales[nx];
-    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-      x[e] = s[e] * rn;
-      g[e] = g[e] * R / rn;
+    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+      const double2 sv = ld2(s, e), gv = ld2(g, e);
+      st2(x, e, make_double2(sv.x * rn, sv.y * rn));
+      st2(g, e, make_double2(gv.x * R / rn, gv.y * R / rn));
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -582,8 +679,8 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double
 
 __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
   const int lane = blockIdx.x;
-  const size_t off = (size_t)lane * A.nd;
-  for (int e = threadIdx.x; e < A.nd; e += blockDim.x) A.ps[off + e] = s0[off + e];
+  for (int e = threadIdx.x; e < A.nd; e += blockDim.x)
+    A.ps[(size_t)lane * A.ld + e] = s0[(size_t)lane * A.nd + e];
   if (threadIdx.x == 0) {
     LbState L = {};
     L.phase = PH_INIT;
@@ -603,8 +700,8 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
   __syncthreads();
   if (sh.L.status != CCO_STATUS_RUNNING) return;
   LbState& L = sh.L;
-  const int nd = A.nd;
-  const size_t off = (size_t)lane * nd;
+  const int h2 = A.ld >> 1;
+  const size_t off = (size_t)lane * A.ld;
   // packed triangles + 7 scalar arrays: shared memory, or a per-lane global
   // scratch row when memory is too large for shared memory
   double* tsm = A.smem_tri
@@ -618,11 +715,11 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
     double* g = A.g + off;
     const double* ps = A.ps + off;
     const double* pg = A.pg + off;
-    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-      const double v = ps[e];
-      s[e] = v;
-      x[e] = v * R0;
-      g[e] = pg[e] / R0;
+    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+      const double2 v = ld2(ps, e), gv = ld2(pg, e);
+      st2(s, e, v);
+      st2(x, e, make_double2(v.x * R0, v.y * R0));
+      st2(g, e, make_double2(gv.x / R0, gv.y / R0));
     }
     if (threadIdx.x == 0) {
       L.f = A.pf[lane];
@@ -640,7 +737,10 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
     const double* pg = A.pg + off;
     const double* dir = A.dir + off;
     double dp = 0.0;
-    for (int e = threadIdx.x; e < nd; e += blockDim.x) dp += (pg[e] / R) * dir[e];
+    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+      const double2 pv = ld2(pg, e), dv = ld2(dir, e);
+      dp += (pv.x / R) * dv.x + (pv.y / R) * dv.y;
+    }
     dp = block_sum(dp, sh.red);
     if (threadIdx.x == 0) {
       L.ls_steps += 1;
@@ -648,21 +748,24 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
       const double fp = A.pf[lane];
       sh.outcome = ls_decide(L, fp, dp, A.max_ls, &nl);
       sh.new_lo = nl;
-      if (sh.outcome == LS_ACCEPT_PROBE) {
-        // stash the accepted value where end_iteration reads it
-        L.f_lo = fp;
-      }
+      if (sh.outcome == LS_ACCEPT_PROBE) L.f_lo = fp;  // read by end_iteration
     }
     __syncthreads();
     if (sh.new_lo) {
       double* glo = A.glo + off;
-      for (int e = threadIdx.x; e < nd; e += blockDim.x) glo[e] = pg[e] / R;
+      for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+        const double2 pv = ld2(pg, e);
+        st2(glo, e, make_double2(pv.x / R, pv.y / R));
+      }
     }
     if (sh.outcome == LS_CONTINUE) {
       const double al = L.alpha;
       const double* x = A.x + off;
       double* ps = A.ps + off;
-      for (int e = threadIdx.x; e < nd; e += blockDim.x) ps[e] = (x[e] + al * dir[e]) / R;
+      for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+        const double2 xv = ld2(x, e), dv = ld2(dir, e);
+        st2(ps, e, make_double2((xv.x + al * dv.x) / R, (xv.y + al * dv.y) / R));
+      }
     } else {
       __syncthreads();
       lb_end_iteration(A, lane, sh, tsm);
@@ -677,12 +780,12 @@ __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double*
                                  int64_t* lat_out) {
   __shared__ double red[32];
   const int lane = blockIdx.x;
-  const size_t off = (size_t)lane * A.nd;
+  const size_t off = (size_t)lane * A.ld;
   double ss = 0.0;
   for (int e = threadIdx.x; e < A.nd; e += blockDim.x) {
     const double v = A.g[off + e];
     ss += v * v;
-    s_out[off + e] = wrap01(A.s[off + e]);
+    s_out[(size_t)lane * A.nd + e] = wrap01(A.s[off + e]);
   }
   ss = block_sum(ss, red);
   if (threadIdx.x == 0) {

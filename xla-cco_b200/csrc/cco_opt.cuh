@@ -43,6 +43,7 @@ struct LbState {
 
 struct LbArgs {
   int B, N, d, nd, m, n_pass;
+  int ld;                 // padded vector length (multiple of 4 doubles)
   double rescales[CCO_MAX_RESCALES];
   double energy_tol, grad_tol;
   int64_t budget, patience, max_ls;
