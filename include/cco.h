@@ -89,6 +89,35 @@ int cco_problem_info(const cco_problem* p, int* d, int* n_particles, int* m,
 int cco_energy_grad(cco_problem* p, void* stream, int batch, const double* s,
                     double* phi, double* grad, double* rho_re, double* rho_im);
 
+/*
+ * cco_energy_grad without any allocation (no counterpart in the reference).
+ *
+ * For callers that must not allocate device memory during a call: code that
+ * runs while a CUDA stream is being captured into a graph (cudaMalloc is
+ * illegal there), code running under a custom or pre-reserved memory pool
+ * that forbids outside allocations, and hard real-time loops that cannot
+ * afford an allocator round trip. cco_energy_grad obtains its scratch (the
+ * per-tile partial densities and the launch plan) from cudaMallocAsync on
+ * every call; this variant carves it instead out of one fixed device array of
+ * CCO_NOALLOC_SCRATCH_BYTES compiled into the library. Every GPU that loads
+ * the library holds that array until the process exits.
+ *
+ * Same arguments and results as cco_energy_grad with rho_re = rho_im = NULL.
+ * The problem itself is created beforehand (cco_problem_create allocates).
+ * Limit: the scratch of one call, about batch * M * 16 * (2 + ceil(N / 64))
+ * bytes plus the plan, must fit CCO_NOALLOC_SCRATCH_BYTES; a larger batch is
+ * rejected with CCO_ERR_ARG and nothing is launched - split it into smaller
+ * calls. The first call on each device resolves the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. All calls share the one array and nothing in it
+ * needs to start at zero (every call writes all the scratch it reads), but
+ * two calls that overlap on the GPU (different streams, or graph branches
+ * without an ordering edge) race on it: order them.
+ */
+#define CCO_NOALLOC_SCRATCH_BYTES (16u << 20)
+int cco_energy_grad_noalloc(cco_problem* p, void* stream, int batch, const double* s,
+                            double* phi, double* grad);
+
 /* Minimizer settings: same fields and meaning as the reference's settings. */
 typedef struct {
   double step_init;    /* 1e-3  */

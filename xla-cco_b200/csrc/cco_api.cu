@@ -455,6 +455,75 @@ extern "C" int cco_energy_grad(cco_problem* p, void* stream, int batch, const do
   return CCO_OK;
 }
 
+// ------------------------------------------------- evaluation without allocation
+namespace {
+
+// Scratch of cco_energy_grad_noalloc: one fixed device array in the library,
+// resident on every GPU that loads it until the process exits. Host code must
+// never pass this name to a kernel: on the host it is only a stand-in for the
+// symbol; the device address is resolved per device below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CCO_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch on `device`, resolved on the first call with
+// that device current (the caller holds a DeviceGuard for it).
+int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kNoallocMaxDevices)
+    return fail(CCO_ERR_ARG, "device %d out of range for the fixed scratch", device);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_addr[device] == nullptr) {
+    void* addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(fixed scratch)");
+    g_noalloc_addr[device] = addr;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
+  return CCO_OK;
+}
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int cco_energy_grad_noalloc(cco_problem* p, void* stream, int batch, const double* s,
+                                       double* phi, double* grad) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (batch < 0) return fail(CCO_ERR_ARG, "batch must be >= 0");
+  if (batch == 0) return CCO_OK;
+  if (!s || !phi) return fail(CCO_ERR_ARG, "null s or phi");
+  const size_t B = (size_t)batch, M = (size_t)p->M;
+  const size_t nt1 = (size_t)p->host.ntile1, nt2 = (size_t)p->host.ntile2;
+  const size_t b_lanes = round256(sizeof(EvalLane) * B);
+  const size_t b_it1 = round256(sizeof(EvalItem) * B * nt1);
+  const size_t b_it2 = round256(sizeof(EvalItem) * B * nt2);
+  const size_t b_rho = round256(sizeof(double2) * B * M);
+  const size_t b_part = round256(sizeof(double2) * B * nt1 * M);
+  const size_t need = b_lanes + b_it1 + b_it2 + 2 * b_rho + b_part;
+  if (need > CCO_NOALLOC_SCRATCH_BYTES)
+    return fail(CCO_ERR_ARG,
+                "batch %d needs %zu bytes of fixed scratch, the limit is %zu: split the batch",
+                batch, need, (size_t)CCO_NOALLOC_SCRATCH_BYTES);
+  DeviceGuard guard(p->device);
+  unsigned char* base = nullptr;
+  const int rc = noalloc_scratch(p->device, &base);
+  if (rc != CCO_OK) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  EvalWS ws;  // carved from the fixed scratch; never released
+  ws.lanes = reinterpret_cast<EvalLane*>(base);
+  ws.it1 = reinterpret_cast<EvalItem*>(base + b_lanes);
+  ws.it2 = reinterpret_cast<EvalItem*>(base + b_lanes + b_it1);
+  ws.rho = reinterpret_cast<double2*>(base + b_lanes + b_it1 + b_it2);
+  ws.rhow = reinterpret_cast<double2*>(base + b_lanes + b_it1 + b_it2 + b_rho);
+  ws.part = reinterpret_cast<double2*>(base + b_lanes + b_it1 + b_it2 + 2 * b_rho);
+  const size_t nd = (size_t)p->N * p->d;
+  CCO_CUDA(ws.build(p, batch, s, nd, phi, 1, grad, nd, nullptr, 0, st));
+  CCO_CUDA(eval_launch(ws.plan, st));
+  return CCO_OK;
+}
+
 // ------------------------------------------------------------ relax drivers
 namespace {
 

@@ -92,6 +92,7 @@ SIGNATURES = {
     "cco_problem_destroy": (ctypes.c_int, [_vp]),
     "cco_problem_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p]),
     "cco_energy_grad": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "cco_energy_grad_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
     "cco_relax_descent": (
         ctypes.c_int,
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(DescentSettingsC), ctypes.c_int,
