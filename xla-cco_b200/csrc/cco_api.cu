@@ -39,6 +39,46 @@ int cuda_fail(cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
   } while (0)
 
+// Stream-ordered allocations come from one memory pool per device that keeps
+// its memory (release threshold = max): a relaxation's ~GB of lane state is
+// reused by the next call instead of being unmapped at every synchronize, as
+// the default pool (threshold 0) would do.
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxPoolDevices] = {};
+
+cudaError_t device_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxPoolDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+    g_pool[dev] = pool;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+template <class T>
+cudaError_t pool_alloc(T** ptr, size_t bytes, cudaStream_t st) {
+  cudaMemPool_t pool;
+  const cudaError_t e = device_pool(&pool);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(reinterpret_cast<void**>(ptr), bytes, pool, st);
+}
+
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {
@@ -392,12 +432,12 @@ struct EvalWS {
 
   cudaError_t alloc(const cco_problem* p, int B, cudaStream_t st) {
     const int M = p->M, nt1 = p->host.ntile1, nt2 = p->host.ntile2;
-    cudaError_t e = cudaMallocAsync(&lanes, sizeof(EvalLane) * B, st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&it1, sizeof(EvalItem) * (size_t)B * nt1, st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&it2, sizeof(EvalItem) * (size_t)B * nt2, st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&rho, sizeof(double2) * (size_t)B * M, st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&rhow, sizeof(double2) * (size_t)B * M, st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&part, sizeof(double2) * (size_t)B * nt1 * M, st);
+    cudaError_t e = pool_alloc(&lanes, sizeof(EvalLane) * B, st);
+    if (e == cudaSuccess) e = pool_alloc(&it1, sizeof(EvalItem) * (size_t)B * nt1, st);
+    if (e == cudaSuccess) e = pool_alloc(&it2, sizeof(EvalItem) * (size_t)B * nt2, st);
+    if (e == cudaSuccess) e = pool_alloc(&rho, sizeof(double2) * (size_t)B * M, st);
+    if (e == cudaSuccess) e = pool_alloc(&rhow, sizeof(double2) * (size_t)B * M, st);
+    if (e == cudaSuccess) e = pool_alloc(&part, sizeof(double2) * (size_t)B * nt1 * M, st);
     return e;
   }
   cudaError_t build(const cco_problem* p, int B, const double* s, size_t s_stride, double* f,
@@ -531,9 +571,12 @@ namespace {
 // graphs of kGraphTicks ticks until no lane is RUNNING or the tick bound is
 // reached. The lanes are split into `nbr` independent branches of the graph:
 // a branch's FP64-bound evaluation overlaps another branch's HBM-bound
-// minimizer update on the device. Completion is checked one graph behind so
-// the device never idles on the host.
+// minimizer update on the device. Completion is checked kInflight graphs
+// behind, so host or driver hiccups (a clock sampler, a busy CPU) do not
+// leave the device idle; lanes already finished make the surplus graphs
+// near-empty launches.
 constexpr int kGraphTicks = 16;
+constexpr int kInflight = 3;
 constexpr int kMaxBranches = 4;
 
 int branch_count(int B) {
@@ -547,13 +590,15 @@ int branch_count(int B) {
 template <class TickFn>
 int run_ticks(cudaStream_t st, int nbr, TickFn tick, const int64_t* status, size_t stride, int B,
               int64_t max_ticks, int64_t* ticks_out) {
+  constexpr int kSlots = kInflight + 1;
   int* d_count = nullptr;
-  int* h_count = nullptr;
-  CCO_CUDA(cudaMallocAsync(&d_count, 2 * sizeof(int), st));
-  CCO_CUDA(cudaMallocHost(&h_count, 2 * sizeof(int)));
-  cudaEvent_t ev[2];
-  CCO_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
-  CCO_CUDA(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+  // pinned completion counters: allocated once per host thread (cudaMallocHost
+  // is slow and may synchronize, so it stays out of every call)
+  static thread_local int* h_count = nullptr;
+  CCO_CUDA(pool_alloc(&d_count, kSlots * sizeof(int), st));
+  if (h_count == nullptr) CCO_CUDA(cudaMallocHost(&h_count, kSlots * sizeof(int)));
+  cudaEvent_t ev[kSlots];
+  for (int i = 0; i < kSlots; ++i) CCO_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int rc = CCO_OK;
@@ -579,31 +624,31 @@ int run_ticks(cudaStream_t st, int nbr, TickFn tick, const int64_t* status, size
   }
   if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
   int64_t ticks = 0;
-  int launched = 0;
+  int launched = 0, checked = 0;
   bool done = false;
   while (e == cudaSuccess && !done) {
     if (ticks >= max_ticks) break;
     e = cudaGraphLaunch(exec, st);
     if (e != cudaSuccess) break;
     ticks += kGraphTicks;
-    const int slot = launched & 1;
+    const int slot = launched % kSlots;
     e = count_running(status, stride, B, d_count + slot, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_count + slot, d_count + slot, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaEventRecord(ev[slot], st);
     ++launched;
-    if (e == cudaSuccess && launched >= 2) {
-      const int prev = (launched - 2) & 1;
-      e = cudaEventSynchronize(ev[prev]);
-      if (e == cudaSuccess && h_count[prev] == 0) done = true;
+    if (e == cudaSuccess && launched - checked > kInflight) {
+      const int old = checked % kSlots;
+      e = cudaEventSynchronize(ev[old]);
+      ++checked;
+      if (e == cudaSuccess && h_count[old] == 0) done = true;
     }
   }
-  if (e == cudaSuccess && !done) {
-    // drain: the last launch's count
-    if (launched >= 1) {
-      const int last = (launched - 1) & 1;
-      e = cudaEventSynchronize(ev[last]);
-      if (e == cudaSuccess && h_count[last] == 0) done = true;
-    }
+  // drain the launches still in flight, oldest first
+  while (e == cudaSuccess && !done && checked < launched) {
+    const int old = checked % kSlots;
+    e = cudaEventSynchronize(ev[old]);
+    ++checked;
+    if (e == cudaSuccess && h_count[old] == 0) done = true;
   }
   if (e != cudaSuccess) rc = cuda_fail(e, "relax ticks");
   else if (!done) rc = fail(CCO_ERR_ROUNDS, "relax did not finish within the round bound (%lld ticks)", (long long)max_ticks);
@@ -614,11 +659,9 @@ int run_ticks(cudaStream_t st, int nbr, TickFn tick, const int64_t* status, size
     cudaEventDestroy(join[b]);
   }
   cudaEventDestroy(fork);
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
+  for (int i = 0; i < kSlots; ++i) cudaEventDestroy(ev[i]);
   cudaFreeAsync(d_count, st);
   cudaStreamSynchronize(st);
-  cudaFreeHost(h_count);
   if (ticks_out) *ticks_out = ticks;
   return rc;
 }
@@ -651,7 +694,8 @@ LbArgs lbfgs_shift(const LbArgs& A, int lo, int nb) {
   r.pf += lo;
   r.Sh += v * A.m; r.Yh += v * A.m;
   r.SYs += (size_t)lo * A.m * A.m; r.YYs += (size_t)lo * A.m * A.m;
-  if (r.tri_g) r.tri_g += (size_t)lo * ((size_t)A.m * (A.m + 1) + 7 * (size_t)A.m);
+  if (r.tri_g) r.tri_g += (size_t)lo * ((size_t)A.m * (A.m + 1));
+  r.scal += (size_t)lo * A.scal_stride;
   if (A.traj_count) {
     r.traj_s += (size_t)lo * A.rec_cap * A.nd;
     r.traj_e += (size_t)lo * A.rec_cap;
@@ -701,10 +745,10 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
   double* sc = nullptr;    // f, step, norm, pf
   int64_t* ic = nullptr;   // it, n_evals, status, t0, t1
   int* ph = nullptr;       // phase, nonzero
-  CCO_CUDA(cudaMallocAsync(&vec, sizeof(double) * nd * B * 4, st));
-  CCO_CUDA(cudaMallocAsync(&sc, sizeof(double) * B * 4, st));
-  CCO_CUDA(cudaMallocAsync(&ic, sizeof(int64_t) * B * 5, st));
-  CCO_CUDA(cudaMallocAsync(&ph, sizeof(int) * B * 2, st));
+  CCO_CUDA(pool_alloc(&vec, sizeof(double) * nd * B * 4, st));
+  CCO_CUDA(pool_alloc(&sc, sizeof(double) * B * 4, st));
+  CCO_CUDA(pool_alloc(&ic, sizeof(int64_t) * B * 5, st));
+  CCO_CUDA(pool_alloc(&ph, sizeof(int) * B * 2, st));
   a.s = vec;
   a.g = vec + nd * B;
   a.ps = vec + 2 * nd * B;
@@ -745,7 +789,7 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
     if (e == cudaSuccess) e = descent_update(ab[b], s);
     return e;
   };
-  const int64_t max_ticks = 1 + a.max_iters + kGraphTicks;
+  const int64_t max_ticks = 1 + a.max_iters + (kInflight + 1) * kGraphTicks;
   int64_t ticks = 0;
   int rc = run_ticks(st, nbr, tick, a.status, 1, B, max_ticks, &ticks);
   if (rc == CCO_OK) {
@@ -775,6 +819,7 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   if (cfg->n_rescales < 1 || cfg->n_rescales > CCO_MAX_RESCALES)
     return fail(CCO_ERR_ARG, "need 1..%d rescale passes", CCO_MAX_RESCALES);
   if (cfg->memory < 1) return fail(CCO_ERR_ARG, "memory must be >= 1");
+  if (cfg->memory > 256) return fail(CCO_ERR_ARG, "memory must be <= 256 on this build");
   if (cfg->max_linesearch_steps < 1) return fail(CCO_ERR_ARG, "max_linesearch_steps must be >= 1");
   const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
   if (rec && (!out->traj_s || !out->traj_energy || !out->traj_step || !out->traj_iteration || !out->traj_count))
@@ -819,13 +864,18 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   double* dots = nullptr;  // SY, YY
   double* pf = nullptr;
   double* trig = nullptr;
-  CCO_CUDA(cudaMallocAsync(&stv, sizeof(LbState) * B, st));
-  CCO_CUDA(cudaMallocAsync(&vec, sizeof(double) * ld * B * 7, st));
+  CCO_CUDA(pool_alloc(&stv, sizeof(LbState) * B, st));
+  CCO_CUDA(pool_alloc(&vec, sizeof(double) * ld * B * 7, st));
   CCO_CUDA(cudaMemsetAsync(vec, 0, sizeof(double) * ld * B * 7, st));
-  CCO_CUDA(cudaMallocAsync(&hist, sizeof(double) * ld * B * m * 2, st));
-  CCO_CUDA(cudaMallocAsync(&dots, sizeof(double) * (size_t)B * m * m * 2, st));
-  CCO_CUDA(cudaMallocAsync(&pf, sizeof(double) * B, st));
-  if (!in_smem) CCO_CUDA(cudaMallocAsync(&trig, tri_bytes * B, st));
+  CCO_CUDA(pool_alloc(&hist, sizeof(double) * ld * B * m * 2, st));
+  CCO_CUDA(pool_alloc(&dots, sizeof(double) * (size_t)B * m * m * 2, st));
+  CCO_CUDA(pool_alloc(&pf, sizeof(double) * B, st));
+  if (!in_smem) CCO_CUDA(pool_alloc(&trig, tri_bytes * B, st));
+  A.nblkB = (int)((ld / 2 + 255) / 256);
+  A.scal_stride = (4 * m + 1 + A.nblkB + 1) & ~1;
+  double* scal = nullptr;
+  CCO_CUDA(pool_alloc(&scal, sizeof(double) * (size_t)A.scal_stride * B, st));
+  A.scal = scal;
   A.st = stv;
   A.x = vec;
   A.s = vec + ld * B;
@@ -868,7 +918,7 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   };
   const int64_t max_ticks =
       1 + (int64_t)cfg->n_rescales * (cfg->max_evals_per_pass + cfg->max_linesearch_steps + 1) +
-      kGraphTicks;
+      (kInflight + 1) * kGraphTicks;
   int64_t ticks = 0;
   int rc = run_ticks(st, nbr, tick, status0, st_stride, B, max_ticks, &ticks);
   if (rc == CCO_OK) {
@@ -877,7 +927,7 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
     if (e != cudaSuccess) rc = cuda_fail(e, "lbfgs_finalize");
   }
   out->ticks = ticks;
-  out->launches = ticks * 4 * nbr + ticks / kGraphTicks + 2 + nbr;
+  out->launches = ticks * 7 * nbr + ticks / kGraphTicks + 2 + nbr;
   for (int b = 0; b < nbr; ++b) ws[b].release(st);
   cudaFreeAsync(stv, st);
   cudaFreeAsync(vec, st);
@@ -885,6 +935,7 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   cudaFreeAsync(dots, st);
   cudaFreeAsync(pf, st);
   if (trig) cudaFreeAsync(trig, st);
+  cudaFreeAsync(scal, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "relax lbfgs");
   return rc;

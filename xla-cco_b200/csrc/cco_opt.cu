@@ -29,6 +29,8 @@ namespace cco {
 namespace {
 
 constexpr int kUpdThreads = 256;
+constexpr int kPassBMaxPairs = 512;  // direction coefficients staged in smem up to this
+constexpr int kScalarMaxPairs = 256; // L-BFGS memory supported by the scalar kernel
 
 __device__ __forceinline__ int64_t gtimer() {
   uint64_t v;
@@ -293,6 +295,12 @@ __device__ __forceinline__ void st2(double* p, int i, double2 v) {
   reinterpret_cast<double2*>(p)[i] = v;
 }
 
+// Per-lane scalar rows in A.scal: a_p, b_p (m each), gamma + cy (1 + m),
+// cs (m), then the pass-B partials of g.dir (nblkB).
+__device__ __forceinline__ double* scal_row(const LbArgs& A, int lane) {
+  return A.scal + (size_t)lane * A.scal_stride;
+}
+
 __device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double* s) {
   if (A.traj_count == nullptr) return;
   __shared__ int64_t row;
@@ -315,267 +323,11 @@ __device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double*
   __syncthreads();
 }
 
-// Direction for the current (x, g) and the first probe at alpha = 1.
-__device__ void lb_begin_iteration(const LbArgs& A, int lane, LbShared& sh, double* tsm) {
-  LbState& L = sh.L;
-  const int ld = A.ld, h2 = A.ld >> 1, m = A.m;
-  const size_t off = (size_t)lane * ld;
-  const double* g = A.g + off;
-  const double* x = A.x + off;
-  double* dir = A.dir + off;
-  double* ps = A.ps + off;
-  const double* Sh = A.Sh + (size_t)lane * m * ld;
-  const double* Yh = A.Yh + (size_t)lane * m * ld;
-  double* SYs = A.SYs + (size_t)lane * m * m;
-  double* YYs = A.YYs + (size_t)lane * m * m;
-  const int k = L.hk;
-  double* triSY = tsm;
-  double* triYY = tsm + (size_t)m * (m + 1) / 2;
-  double* av = tsm + (size_t)m * (m + 1);
-  double* bv = av + m;
-  double* alp = bv + m;
-  double* bet = alp + m;
-  double* rh = bet + m;
-  double* cy = rh + m;
-  double* cs = cy + m;
-  const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
-  const int head = L.hhead;
-  auto slot = [&](int p) { return (head - k + p + m) % m; };
-
-  // ---- pass A: a_p = s_p.g, b_p = y_p.g and the newest pair's column
-  //      (one warp per pair, four double2 words per lane in flight)
-  if (k > 0) {
-    const int sn = slot(k - 1);
-    const double* yn = Yh + (size_t)sn * ld;
-    const bool np = L.newpair != 0;
-    for (int p = warp; p < k; p += nwarps) {
-      const int sp = slot(p);
-      const double* sr = Sh + (size_t)sp * ld;
-      const double* yr = Yh + (size_t)sp * ld;
-      double ag = 0.0, bg = 0.0, sy = 0.0, yy = 0.0;
-      int e = wl;
-      for (; e + 96 < h2; e += 128) {
-        double2 sv[4], yv[4], gv[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          sv[u] = ld2(sr, e + 32 * u);
-          yv[u] = ld2(yr, e + 32 * u);
-          gv[u] = ld2(g, e + 32 * u);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          ag += sv[u].x * gv[u].x + sv[u].y * gv[u].y;
-          bg += yv[u].x * gv[u].x + yv[u].y * gv[u].y;
-        }
-        if (np) {
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const double2 w = ld2(yn, e + 32 * u);
-            sy += sv[u].x * w.x + sv[u].y * w.y;
-            yy += yv[u].x * w.x + yv[u].y * w.y;
-          }
-        }
-      }
-      for (; e < h2; e += 32) {
-        const double2 sv = ld2(sr, e), yv = ld2(yr, e), gv = ld2(g, e);
-        ag += sv.x * gv.x + sv.y * gv.y;
-        bg += yv.x * gv.x + yv.y * gv.y;
-        if (np) {
-          const double2 w = ld2(yn, e);
-          sy += sv.x * w.x + sv.y * w.y;
-          yy += yv.x * w.x + yv.y * w.y;
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        ag += __shfl_xor_sync(0xffffffffu, ag, o);
-        bg += __shfl_xor_sync(0xffffffffu, bg, o);
-        sy += __shfl_xor_sync(0xffffffffu, sy, o);
-        yy += __shfl_xor_sync(0xffffffffu, yy, o);
-      }
-      if (wl == 0) {
-        av[p] = ag;
-        bv[p] = bg;
-        if (np) {
-          SYs[(size_t)sp * m + sn] = sy;
-          YYs[(size_t)sp * m + sn] = yy;
-          YYs[(size_t)sn * m + sp] = yy;
-        }
-      }
-    }
-    __threadfence_block();
-    __syncthreads();
-    // packed logical triangles (p <= q)
-    const int ntri = k * (k + 1) / 2;
-    for (int t = threadIdx.x; t < ntri; t += blockDim.x) {
-      int q = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
-      while (q * (q + 1) / 2 > t) --q;
-      while ((q + 1) * (q + 2) / 2 <= t) ++q;
-      const int p = t - q * (q + 1) / 2;
-      const int sp = slot(p), sq = slot(q);
-      triSY[t] = SYs[(size_t)sp * m + sq];
-      triYY[t] = YYs[(size_t)sp * m + sq];
-    }
-    __syncthreads();
-  }
-  // ---- gamma (optax scale_by_lbfgs): newest pair, or min(1, 1/|g|) on a fresh pass
-  if (k == 0) {
-    double ss = 0.0;
-    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-      const double2 v = ld2(g, e);
-      ss += v.x * v.x + v.y * v.y;
-    }
-    ss = block_sum(ss, sh.red);
-    if (threadIdx.x == 0) L.gamma = fmin(1.0, 1.0 / sqrt(ss));
-  } else if (threadIdx.x == 0) {
-    const int n = k - 1;
-    const double num = triSY[tri(n, n)], den = triYY[tri(n, n)];
-    L.gamma = den > 0.0 ? num / den : 1.0;
-  }
-  // ---- loops 1 and 2 on warp 0 (O(k^2) scalars, fixed order). Column-
-  //      oriented triangular solves: lane l keeps the running sums of pairs
-  //      p = l, l+32, ...; each solved alpha_q is broadcast once and folded
-  //      into every older row, so a step costs one shuffle, not a reduction.
-  constexpr int kRegRows = 8;  // k <= 256 in registers
-  if (k > 0 && warp == 0) {
-    for (int p = wl; p < k; p += 32) {
-      const double ys = triSY[tri(p, p)];
-      rh[p] = ys == 0.0 ? 0.0 : 1.0 / ys;
-    }
-    __syncwarp();
-    if (k <= 32 * kRegRows) {
-      double t[kRegRows];
-#pragma unroll
-      for (int i = 0; i < kRegRows; ++i) t[i] = (32 * i + wl < k) ? av[32 * i + wl] : 0.0;
-      for (int q = k - 1; q >= 0; --q) {
-        const int own = q & 31, oi = q >> 5;
-        double tq = 0.0;
-#pragma unroll
-        for (int i = 0; i < kRegRows; ++i) tq = (i == oi) ? t[i] : tq;
-        const double aq = __shfl_sync(0xffffffffu, rh[q] * tq, own);
-        if (wl == 0) alp[q] = aq;
-#pragma unroll
-        for (int i = 0; i < kRegRows; ++i) {
-          const int p = 32 * i + wl;
-          if (p < q) t[i] -= aq * triSY[tri(p, q)];
-        }
-      }
-    } else {
-      for (int p = k - 1; p >= 0; --p) {
-        double acc = 0.0;
-        for (int q = p + 1 + wl; q < k; q += 32) acc += alp[q] * triSY[tri(p, q)];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (wl == 0) alp[p] = rh[p] * (av[p] - acc);
-        __syncwarp();
-      }
-    }
-  }
-  __syncthreads();
-  if (k > 0) {
-    // t_p = b_p - sum_q alpha_q YY[p][q] (independent rows: one warp each)
-    for (int p = warp; p < k; p += nwarps) {
-      double acc = 0.0;
-      for (int q = wl; q < k; q += 32) acc += alp[q] * triYY[p <= q ? tri(p, q) : tri(q, p)];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (wl == 0) bet[p] = bv[p] - acc;  // holds t_p until loop 2 overwrites it
-    }
-    __syncthreads();
-    if (warp == 0) {
-      const double gam = L.gamma;
-      if (k <= 32 * kRegRows) {
-        // u_p = sum_{q<p} (alpha_q - beta_q) SY[q][p], accumulated column-wise
-        double u[kRegRows];
-#pragma unroll
-        for (int i = 0; i < kRegRows; ++i) u[i] = 0.0;
-        for (int p = 0; p < k; ++p) {
-          const int own = p & 31, oi = p >> 5;
-          double up = 0.0;
-#pragma unroll
-          for (int i = 0; i < kRegRows; ++i) up = (i == oi) ? u[i] : up;
-          double dq = 0.0;
-          if (wl == own) {
-            const double bp = rh[p] * (gam * bet[p] + up);
-            bet[p] = bp;
-            dq = alp[p] - bp;
-          }
-          dq = __shfl_sync(0xffffffffu, dq, own);
-#pragma unroll
-          for (int i = 0; i < kRegRows; ++i) {
-            const int q = 32 * i + wl;
-            if (q > p && q < k) u[i] += dq * triSY[tri(p, q)];
-          }
-        }
-        __syncwarp();
-      } else {
-        for (int p = 0; p < k; ++p) {
-          double acc = 0.0;
-          for (int q = wl; q < p; q += 32) acc += (alp[q] - bet[q]) * triSY[tri(q, p)];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-          if (wl == 0) bet[p] = rh[p] * (gam * bet[p] + acc);
-          __syncwarp();
-        }
-      }
-      for (int q = wl; q < k; q += 32) {
-        cy[q] = gam * alp[q];
-        cs[q] = bet[q] - alp[q];
-      }
-    }
-    __syncthreads();
-  }
-  // ---- pass B: dir = -gamma g + sum cy_q y_q + sum cs_q s_q, first probe, g.dir
-  //      (one double2 word per thread, eight pairs = 16 loads in flight)
-  const double gam = L.gamma, R = L.R;
-  double dp = 0.0;
-  for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-    double ax = 0.0, ay = 0.0;
-    int q = 0;
-    for (; q + 8 <= k; q += 8) {
-      double2 yv[8], sv[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const size_t r = (size_t)slot(q + u) * ld;
-        yv[u] = ld2(Yh + r, e);
-        sv[u] = ld2(Sh + r, e);
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        ax += cy[q + u] * yv[u].x + cs[q + u] * sv[u].x;
-        ay += cy[q + u] * yv[u].y + cs[q + u] * sv[u].y;
-      }
-    }
-    for (; q < k; ++q) {
-      const size_t r = (size_t)slot(q) * ld;
-      const double2 yv = ld2(Yh + r, e), sv = ld2(Sh + r, e);
-      ax += cy[q] * yv.x + cs[q] * sv.x;
-      ay += cy[q] * yv.y + cs[q] * sv.y;
-    }
-    const double2 gv = ld2(g, e), xv = ld2(x, e);
-    const double2 de = make_double2(ax - gam * gv.x, ay - gam * gv.y);
-    st2(dir, e, de);
-    dp += gv.x * de.x + gv.y * de.y;
-    st2(ps, e, make_double2((xv.x + 1.0 * de.x) / R, (xv.y + 1.0 * de.y) / R));
-  }
-  dp = block_sum(dp, sh.red);
-  if (threadIdx.x == 0) {
-    L.f0 = L.f;
-    L.dphi0 = dp;
-    L.phase = PH_EXPAND;
-    L.ls_steps = 0;
-    L.alpha = 1.0;
-    L.a_prev = 0.0; L.f_prev = L.f; L.d_prev = dp;
-    L.a_lo = 0.0; L.f_lo = L.f; L.d_lo = dp;
-    L.a_hi = 0.0; L.f_hi = L.f; L.d_hi = dp;
-    L.have_lo = 0;
-    L.newpair = 0;
-  }
-  __syncthreads();
-}
-
-__device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double* tsm) {
+// End of an L-BFGS iteration (lbfgs.py:267-313): accept or keep the point,
+// push the new (s, y) pair, update counters and statuses, and advance the
+// rescale pass (history reset) when the pass ends. A lane that keeps running
+// is flagged for a new direction (passes A, scalar, B of this tick).
+__device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
   LbState& L = sh.L;
   const int ld = A.ld, h2 = A.ld >> 1, m = A.m;
   const size_t off = (size_t)lane * ld;
@@ -674,7 +426,7 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh, double
   }
   __syncthreads();
   lb_record(A, lane, sh, s);
-  if (L.status == CCO_STATUS_RUNNING) lb_begin_iteration(A, lane, sh, tsm);
+  if (threadIdx.x == 0 && L.status == CCO_STATUS_RUNNING) L.need_dir = 1;
 }
 
 __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
@@ -692,8 +444,10 @@ __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
   }
 }
 
-__global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
-  extern __shared__ double dsm[];
+// Probe kernel: one CTA per lane. Starts the line search of a direction
+// built by the previous tick's passes, consumes this tick's probe and either
+// places the next probe or ends the iteration.
+__global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
   __shared__ LbShared sh;
   const int lane = blockIdx.x;
   if (threadIdx.x == 0) sh.L = A.st[lane];
@@ -702,11 +456,6 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
   LbState& L = sh.L;
   const int h2 = A.ld >> 1;
   const size_t off = (size_t)lane * A.ld;
-  // packed triangles + 7 scalar arrays: shared memory, or a per-lane global
-  // scratch row when memory is too large for shared memory
-  double* tsm = A.smem_tri
-                    ? dsm
-                    : A.tri_g + (size_t)lane * ((size_t)A.m * (A.m + 1) + 7 * (size_t)A.m);
   if (L.phase == PH_INIT) {
     // init_one (lbfgs.py:163-197): x = R0 s0, g_x = g_s / R0, one evaluation
     const double R0 = L.R;
@@ -726,12 +475,33 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
       L.n_evals = 1;
       L.status = L.f < A.energy_tol ? CCO_STATUS_ENERGY_TOL : CCO_STATUS_RUNNING;
       L.last_step = 0.0;
+      L.phase = PH_EXPAND;
       if (L.status != CCO_STATUS_RUNNING) L.t1 = gtimer();
+      else L.need_dir = 1;
     }
     __syncthreads();
     lb_record(A, lane, sh, s);
-    if (L.status == CCO_STATUS_RUNNING) lb_begin_iteration(A, lane, sh, tsm);
   } else {
+    if (L.need_dir) {
+      // the direction and the first probe (alpha = 1) were written by pass B
+      if (threadIdx.x == 0) {
+        const double* dpart = scal_row(A, lane) + 4 * A.m + 1;
+        double dp = 0.0;
+        for (int b = 0; b < A.nblkB; ++b) dp += dpart[b];
+        L.f0 = L.f;
+        L.dphi0 = dp;
+        L.phase = PH_EXPAND;
+        L.ls_steps = 0;
+        L.alpha = 1.0;
+        L.a_prev = 0.0; L.f_prev = L.f; L.d_prev = dp;
+        L.a_lo = 0.0; L.f_lo = L.f; L.d_lo = dp;
+        L.a_hi = 0.0; L.f_hi = L.f; L.d_hi = dp;
+        L.have_lo = 0;
+        L.newpair = 0;
+        L.need_dir = 0;
+      }
+      __syncthreads();
+    }
     // one probe of the line search
     const double R = L.R;
     const double* pg = A.pg + off;
@@ -768,11 +538,285 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_update(LbArgs A) {
       }
     } else {
       __syncthreads();
-      lb_end_iteration(A, lane, sh, tsm);
+      lb_end_iteration(A, lane, sh);
     }
   }
   __syncthreads();
   if (threadIdx.x == 0) A.st[lane] = sh.L;
+}
+
+// Pass A (grid: pair blocks x lanes): a_p = s_p.g, b_p = y_p.g for every
+// stored pair and, after a push, the newest pair's column s_p.y_n, y_p.y_n.
+// One warp per pair with four double2 words per lane in flight.
+__global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
+  const int lane = blockIdx.y;
+  const LbState* Lp = A.st + lane;
+  const int k = Lp->hk;
+  if (Lp->status != CCO_STATUS_RUNNING || !Lp->need_dir || k == 0) return;
+  const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
+  const int p = blockIdx.x * (kUpdThreads / 32) + warp;
+  if (p >= k) return;
+  const int ld = A.ld, h2 = A.ld >> 1, m = A.m;
+  const int head = Lp->hhead;
+  const bool np = Lp->newpair != 0;
+  const int sp = (head - k + p + m) % m, sn = (head - 1 + m) % m;
+  const double* g = A.g + (size_t)lane * ld;
+  const double* sr = A.Sh + ((size_t)lane * m + sp) * ld;
+  const double* yr = A.Yh + ((size_t)lane * m + sp) * ld;
+  const double* yn = A.Yh + ((size_t)lane * m + sn) * ld;
+  double ag = 0.0, bg = 0.0, sy = 0.0, yy = 0.0;
+  int e = wl;
+  for (; e + 96 < h2; e += 128) {
+    double2 sv[4], yv[4], gv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      sv[u] = ld2(sr, e + 32 * u);
+      yv[u] = ld2(yr, e + 32 * u);
+      gv[u] = ld2(g, e + 32 * u);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      ag += sv[u].x * gv[u].x + sv[u].y * gv[u].y;
+      bg += yv[u].x * gv[u].x + yv[u].y * gv[u].y;
+    }
+    if (np) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double2 w = ld2(yn, e + 32 * u);
+        sy += sv[u].x * w.x + sv[u].y * w.y;
+        yy += yv[u].x * w.x + yv[u].y * w.y;
+      }
+    }
+  }
+  for (; e < h2; e += 32) {
+    const double2 sv = ld2(sr, e), yv = ld2(yr, e), gv = ld2(g, e);
+    ag += sv.x * gv.x + sv.y * gv.y;
+    bg += yv.x * gv.x + yv.y * gv.y;
+    if (np) {
+      const double2 w = ld2(yn, e);
+      sy += sv.x * w.x + sv.y * w.y;
+      yy += yv.x * w.x + yv.y * w.y;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ag += __shfl_xor_sync(0xffffffffu, ag, o);
+    bg += __shfl_xor_sync(0xffffffffu, bg, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    yy += __shfl_xor_sync(0xffffffffu, yy, o);
+  }
+  if (wl == 0) {
+    double* sc = scal_row(A, lane);
+    sc[p] = ag;
+    sc[m + p] = bg;
+    if (np) {
+      double* SYt = A.SYs + (size_t)lane * m * m;   // row = newer slot
+      double* YYs = A.YYs + (size_t)lane * m * m;
+      SYt[(size_t)sn * m + sp] = sy;
+      YYs[(size_t)sp * m + sn] = yy;
+      YYs[(size_t)sn * m + sp] = yy;
+    }
+  }
+}
+
+// Scalar kernel (one CTA per lane): gamma and the coefficients of the
+// direction from the inner products. The lower triangles of SY (s_older .
+// y_newer) and YY are copied row by row into shared memory from the slot
+// matrices (rows are contiguous: SYt row = newer slot), then loop 1 runs
+// column-oriented (one shuffle per step) and loop 2 row-oriented (one warp
+// reduction per step); both read contiguous shared-memory rows.
+__global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
+  extern __shared__ double dsm[];
+  __shared__ double av[kScalarMaxPairs], bv[kScalarMaxPairs], alp[kScalarMaxPairs],
+      bet[kScalarMaxPairs], rh[kScalarMaxPairs];
+  __shared__ int sl[kScalarMaxPairs];
+  __shared__ double red[32];
+  __shared__ double gam_s;
+  const int lane = blockIdx.x;
+  const LbState* Lp = A.st + lane;
+  if (Lp->status != CCO_STATUS_RUNNING || !Lp->need_dir) return;
+  const int k = Lp->hk, m = A.m, head = Lp->hhead;
+  double* sc = scal_row(A, lane);
+  const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  // two packings of SY[p][q] = s_p . y_q (p older than q): triSY by newer
+  // rows (tri(p, q) = q (q + 1) / 2 + p) for loop 1, triSO by older rows
+  // (off(p) + q - p, off(p) = p k - p (p - 1) / 2) for loop 2
+  double* triSY = A.smem_tri ? dsm : A.tri_g + (size_t)lane * ((size_t)m * (m + 1));
+  double* triSO = triSY + (size_t)m * (m + 1) / 2;
+  const double* YYs = A.YYs + (size_t)lane * m * m;
+  if (k > 0) {
+    const double* SYt = A.SYs + (size_t)lane * m * m;
+    for (int p = threadIdx.x; p < k; p += blockDim.x) {
+      sl[p] = (head - k + p + m) % m;
+      av[p] = sc[p];
+      bv[p] = sc[m + p];
+    }
+    __syncthreads();
+    for (int q = warp; q < k; q += nwarps) {
+      const double* rs = SYt + (size_t)sl[q] * m;
+      const int base = q * (q + 1) / 2;
+      for (int p = wl; p <= q; p += 32) {
+        const double v = rs[sl[p]];
+        triSY[base + p] = v;
+        triSO[p * k - p * (p - 1) / 2 + (q - p)] = v;
+      }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < k; p += blockDim.x) {
+      const double ys = triSY[tri(p, p)];
+      rh[p] = ys == 0.0 ? 0.0 : 1.0 / ys;
+    }
+    if (threadIdx.x == 0) {
+      const int n = k - 1;
+      const double num = triSY[tri(n, n)], den = YYs[(size_t)sl[n] * m + sl[n]];
+      gam_s = den > 0.0 ? num / den : 1.0;
+    }
+  } else {
+    // gamma (optax scale_by_lbfgs) on a fresh pass: min(1, 1/|g|)
+    const double* g = A.g + (size_t)lane * A.ld;
+    double ss = 0.0;
+    for (int e = threadIdx.x; e < (A.ld >> 1); e += blockDim.x) {
+      const double2 v = ld2(g, e);
+      ss += v.x * v.x + v.y * v.y;
+    }
+    ss = block_sum(ss, red);
+    if (threadIdx.x == 0) gam_s = fmin(1.0, 1.0 / sqrt(ss));
+  }
+  __syncthreads();
+  const double gam = gam_s;
+  if (threadIdx.x == 0) sc[2 * m] = gam;
+  if (k == 0) return;
+  constexpr int R8 = kScalarMaxPairs / 32;
+  if (warp == 0) {
+    // loop 1 (newest first): alpha_q = rho_q t_q, then t_p -= alpha_q SY[p][q], p < q
+    double t[R8];
+#pragma unroll
+    for (int i = 0; i < R8; ++i) t[i] = (32 * i + wl < k) ? av[32 * i + wl] : 0.0;
+    for (int q = k - 1; q >= 0; --q) {
+      const double* row = triSY + q * (q + 1) / 2;
+      const int own = q & 31, oi = q >> 5;
+      double tq = 0.0;
+#pragma unroll
+      for (int i = 0; i < R8; ++i) tq = (i == oi) ? t[i] : tq;
+      const double aq = __shfl_sync(0xffffffffu, rh[q] * tq, own);
+      if (wl == 0) alp[q] = aq;
+#pragma unroll
+      for (int i = 0; i < R8; ++i) {
+        const int p = 32 * i + wl;
+        if (p < q) t[i] -= aq * row[p];
+      }
+    }
+  }
+  __syncthreads();
+  // t2_p = b_p - sum_q alpha_q YY[p][q] (independent rows: one warp each)
+  // (YY rows are read in place: contiguous in slot order, L2-resident)
+  for (int p = warp; p < k; p += nwarps) {
+    const double* row = YYs + (size_t)sl[p] * m;
+    double acc = 0.0;
+    for (int q = wl; q < k; q += 32) acc += alp[q] * row[sl[q]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (wl == 0) bet[p] = bv[p] - acc;  // holds t2_p until loop 2 overwrites it
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // loop 2 (oldest first, column-oriented): beta_p = rho_p (gamma t2_p + u_p),
+    // then u_q += (alpha_p - beta_p) SY[p][q] for every newer q
+    double u[R8];
+#pragma unroll
+    for (int i = 0; i < R8; ++i) u[i] = 0.0;
+    for (int p = 0; p < k; ++p) {
+      const double* row = triSO + (p * k - p * (p - 1) / 2) - p;  // row[q] = SY[p][q]
+      const int own = p & 31, oi = p >> 5;
+      double up = 0.0;
+#pragma unroll
+      for (int i = 0; i < R8; ++i) up = (i == oi) ? u[i] : up;
+      double dq = 0.0;
+      if (wl == own) {
+        const double bp = rh[p] * (gam * bet[p] + up);
+        bet[p] = bp;
+        dq = alp[p] - bp;
+      }
+      dq = __shfl_sync(0xffffffffu, dq, own);
+#pragma unroll
+      for (int i = 0; i < R8; ++i) {
+        const int q = 32 * i + wl;
+        if (q > p && q < k) u[i] += dq * row[q];
+      }
+    }
+    __syncwarp();
+    for (int q = wl; q < k; q += 32) {
+      sc[2 * m + 1 + q] = gam * alp[q];        // cy_q
+      sc[3 * m + 1 + q] = bet[q] - alp[q];     // cs_q
+    }
+  }
+}
+
+// Pass B (grid: element blocks x lanes): dir = -gamma g + sum cy_q y_q +
+// sum cs_q s_q, the first probe s = (x + dir) / R and this block's part of
+// g.dir. One double2 word per thread, eight pairs (16 loads) in flight.
+__global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passB(LbArgs A) {
+  __shared__ double cyv[kPassBMaxPairs], csv[kPassBMaxPairs];
+  __shared__ double red[32];
+  const int lane = blockIdx.y;
+  const LbState* Lp = A.st + lane;
+  if (Lp->status != CCO_STATUS_RUNNING || !Lp->need_dir) return;
+  const int k = Lp->hk, m = A.m, head = Lp->hhead;
+  const int ld = A.ld, h2 = A.ld >> 1;
+  const double R = Lp->R;
+  double* sc = scal_row(A, lane);
+  const double gam = sc[2 * m];
+  const bool in_smem = k <= kPassBMaxPairs;
+  if (in_smem) {
+    for (int q = threadIdx.x; q < k; q += blockDim.x) {
+      cyv[q] = sc[2 * m + 1 + q];
+      csv[q] = sc[3 * m + 1 + q];
+    }
+  }
+  __syncthreads();
+  const double* cy = in_smem ? cyv : sc + 2 * m + 1;
+  const double* cs = in_smem ? csv : sc + 3 * m + 1;
+  const size_t off = (size_t)lane * ld;
+  const double* g = A.g + off;
+  const double* x = A.x + off;
+  double* dir = A.dir + off;
+  double* ps = A.ps + off;
+  const double* Sh = A.Sh + (size_t)lane * m * ld;
+  const double* Yh = A.Yh + (size_t)lane * m * ld;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  double dp = 0.0;
+  if (e < h2) {
+    double ax = 0.0, ay = 0.0;
+    int q = 0;
+    for (; q + 8 <= k; q += 8) {
+      double2 yv[8], sv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const size_t r = (size_t)((head - k + q + u + m) % m) * ld;
+        yv[u] = ld2(Yh + r, e);
+        sv[u] = ld2(Sh + r, e);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        ax += cy[q + u] * yv[u].x + cs[q + u] * sv[u].x;
+        ay += cy[q + u] * yv[u].y + cs[q + u] * sv[u].y;
+      }
+    }
+    for (; q < k; ++q) {
+      const size_t r = (size_t)((head - k + q + m) % m) * ld;
+      const double2 yv = ld2(Yh + r, e), sv = ld2(Sh + r, e);
+      ax += cy[q] * yv.x + cs[q] * sv.x;
+      ay += cy[q] * yv.y + cs[q] * sv.y;
+    }
+    const double2 gv = ld2(g, e), xv = ld2(x, e);
+    const double2 de = make_double2(ax - gam * gv.x, ay - gam * gv.y);
+    st2(dir, e, de);
+    dp = gv.x * de.x + gv.y * de.y;
+    st2(ps, e, make_double2((xv.x + 1.0 * de.x) / R, (xv.y + 1.0 * de.y) / R));
+  }
+  dp = block_sum(dp, red);
+  if (threadIdx.x == 0) sc[4 * m + 1 + blockIdx.x] = dp;
 }
 
 __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double* gn_out,
@@ -826,19 +870,24 @@ cudaError_t descent_finalize(const DescentArgs& a, double* s_out, double* e_out,
   return cudaGetLastError();
 }
 
-size_t lbfgs_update_smem(int m) {
-  return ((size_t)m * (m + 1) + 7 * (size_t)m) * sizeof(double);
-}
+size_t lbfgs_update_smem(int m) { return (size_t)m * (m + 1) * sizeof(double); }
 cudaError_t lbfgs_configure(size_t smem) {
-  return cudaFuncSetAttribute(k_lbfgs_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_lbfgs_scalar, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem);
 }
 cudaError_t lbfgs_init(const LbArgs& a, const double* s0, cudaStream_t st) {
   k_lbfgs_init<<<a.B, kUpdThreads, 0, st>>>(a, s0);
   return cudaGetLastError();
 }
+// One tick of the minimizer: the probe kernel for every lane, then the three
+// direction stages, which exit at once for lanes that are mid line search.
 cudaError_t lbfgs_update(const LbArgs& a, cudaStream_t st) {
-  k_lbfgs_update<<<a.B, kUpdThreads, a.smem_tri, st>>>(a);
+  k_lbfgs_probe<<<a.B, kUpdThreads, 0, st>>>(a);
+  const dim3 ga((a.m + kUpdThreads / 32 - 1) / (kUpdThreads / 32), a.B);
+  k_lbfgs_passA<<<ga, kUpdThreads, 0, st>>>(a);
+  k_lbfgs_scalar<<<a.B, kUpdThreads, a.smem_tri, st>>>(a);
+  const dim3 gb(a.nblkB, a.B);
+  k_lbfgs_passB<<<gb, kUpdThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double* gn_out,

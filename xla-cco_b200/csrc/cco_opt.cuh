@@ -38,7 +38,7 @@ struct LbState {
   double gamma, last_step;
   int64_t it, n_evals, pass_evals, stag, status;
   int64_t t0, t1;         // %globaltimer at start / completion
-  int32_t phase, ls_steps, pass_idx, hk, hhead, have_lo, newpair, pad_;
+  int32_t phase, ls_steps, pass_idx, hk, hhead, have_lo, newpair, need_dir;
 };
 
 struct LbArgs {
@@ -54,8 +54,10 @@ struct LbArgs {
   const double* pg;       // [B][nd] probe dPhi/ds (evaluation output)
   const double* pf;       // [B]
   double *Sh, *Yh;        // [B][m][nd] history rings
-  double *SYs, *YYs;      // [B][m][m] slot inner products
-  double* tri_g;          // [B][m (m+1)] packed triangles when they do not fit in smem
+  double *SYs, *YYs;      // [B][m][m] slot inner products (SYs: row = newer slot)
+  double* tri_g;          // [B][m (m+1) + 7m] packed triangles when they do not fit in smem
+  double* scal;           // [B][scal_stride] a_p, b_p, gamma, cy, cs, pass-B partials
+  int scal_stride, nblkB; // row length of scal; pass-B element blocks per lane
   size_t smem_tri;        // 0: triangles in global memory
   double *traj_s, *traj_e, *traj_step;
   int64_t *traj_it, *traj_count;
