@@ -181,6 +181,26 @@ int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const double* s0,
                     const cco_lbfgs_settings* settings, int chunk_iters,
                     cco_relax_out* out);
 
+/*
+ * Mixed batches: lane i relaxes configuration i of problems[i], so one call
+ * runs instances of different N, d and k-set side by side (the same
+ * evaluation and minimizer launches serve every lane). All problems live on
+ * one device. Positions are packed lane after lane without padding:
+ *   s0, out->s      device, lane i at offset sum_{j<i} N_j d_j, N_i d_i doubles
+ *   out->traj_s     device, lane i at offset max_records * sum_{j<i} N_j d_j
+ * the per-lane scalars (energy, status, traj_energy rows, ...) keep their
+ * [B] / [B][max_records] shapes. Each lane's result is bit-identical to the
+ * same configuration relaxed by cco_relax_descent / cco_relax_lbfgs alone.
+ * No reference counterpart: the reference relaxes one (energy, batch) pair
+ * per call (src/xla_cco/minimize/__init__.py:102-151).
+ */
+int cco_relax_descent_mixed(cco_problem* const* problems, void* stream, int batch,
+                            const double* s0, const cco_descent_settings* settings,
+                            int chunk_iters, cco_relax_out* out);
+int cco_relax_lbfgs_mixed(cco_problem* const* problems, void* stream, int batch,
+                          const double* s0, const cco_lbfgs_settings* settings,
+                          int chunk_iters, cco_relax_out* out);
+
 #ifdef __cplusplus
 }
 #endif

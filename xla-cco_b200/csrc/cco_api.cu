@@ -666,72 +666,191 @@ int run_ticks(cudaStream_t st, int nbr, TickFn tick, const int64_t* status, size
   return rc;
 }
 
-// Argument blocks of lanes [lo, lo + nb): every lane array is lane-major.
-DescentArgs descent_shift(const DescentArgs& a, int lo, int nb) {
-  DescentArgs r = a;
-  const size_t v = (size_t)lo * a.nd;
-  r.B = nb;
-  r.s += v; r.g += v; r.ps += v; r.pg += v;
-  r.pf += lo; r.f += lo; r.step += lo; r.norm += lo;
-  r.it += lo; r.n_evals += lo; r.status += lo; r.phase += lo; r.nonzero += lo;
-  r.t0 += lo; r.t1 += lo;
-  if (a.traj_count) {
-    r.traj_s += (size_t)lo * a.rec_cap * a.nd;
-    r.traj_e += (size_t)lo * a.rec_cap;
-    r.traj_step += (size_t)lo * a.rec_cap;
-    r.traj_it += (size_t)lo * a.rec_cap;
-    r.traj_count += lo;
+// Lanes of one relaxation: each lane has its own problem (mixed N, d and
+// k-set) or all lanes share one. Positions are packed in the caller's
+// buffers (soff, N_i d_i each); the device lane vectors use padded lengths
+// (voff, ld_i).
+struct LaneSet {
+  int B = 0, device = 0;
+  std::vector<const cco_problem*> prob;   // [B]
+  std::vector<int> nd, ld;                 // [B]
+  std::vector<int64_t> soff, voff;         // [B]
+  int64_t s_total = 0, v_total = 0;
+  int max_ld = 0;
+  std::vector<const cco_problem*> uniq;    // distinct problems
+  std::vector<int> pidx;                   // [B] index into uniq
+};
+
+int make_laneset(cco_problem* const* probs, int B, int pad, LaneSet* L) {
+  if (B < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  L->B = B;
+  L->prob.resize(B);
+  L->nd.resize(B);
+  L->ld.resize(B);
+  L->soff.resize(B);
+  L->voff.resize(B);
+  L->pidx.resize(B);
+  for (int i = 0; i < B; ++i) {
+    const cco_problem* p = probs[i];
+    if (!p) return fail(CCO_ERR_ARG, "null problem for lane %d", i);
+    if (i == 0) L->device = p->device;
+    if (p->device != L->device) return fail(CCO_ERR_ARG, "lanes must share one device");
+    const int nd = p->N * p->d;
+    const int ld = (nd + pad - 1) / pad * pad;
+    L->prob[i] = p;
+    L->nd[i] = nd;
+    L->ld[i] = ld;
+    L->soff[i] = L->s_total;
+    L->voff[i] = L->v_total;
+    L->s_total += nd;
+    L->v_total += ld;
+    L->max_ld = std::max(L->max_ld, ld);
+    int u = 0;
+    while (u < (int)L->uniq.size() && L->uniq[u] != p) ++u;
+    if (u == (int)L->uniq.size()) L->uniq.push_back(p);
+    L->pidx[i] = u;
   }
-  return r;
+  return CCO_OK;
 }
 
-LbArgs lbfgs_shift(const LbArgs& A, int lo, int nb) {
-  LbArgs r = A;
-  const size_t v = (size_t)lo * A.ld;
-  r.B = nb;
-  r.st += lo;
-  r.x += v; r.s += v; r.g += v; r.dir += v; r.glo += v; r.ps += v; r.pg += v;
-  r.pf += lo;
-  r.Sh += v * A.m; r.Yh += v * A.m;
-  r.SYs += (size_t)lo * A.m * A.m; r.YYs += (size_t)lo * A.m * A.m;
-  if (r.tri_g) r.tri_g += (size_t)lo * ((size_t)A.m * (A.m + 1));
-  r.scal += (size_t)lo * A.scal_stride;
-  if (A.traj_count) {
-    r.traj_s += (size_t)lo * A.rec_cap * A.nd;
-    r.traj_e += (size_t)lo * A.rec_cap;
-    r.traj_step += (size_t)lo * A.rec_cap;
-    r.traj_it += (size_t)lo * A.rec_cap;
-    r.traj_count += lo;
-  }
-  return r;
+template <class T>
+cudaError_t upload(T** dst, const std::vector<T>& src, cudaStream_t st) {
+  cudaError_t e = pool_alloc(dst, sizeof(T) * std::max<size_t>(src.size(), 1), st);
+  if (e == cudaSuccess && !src.empty())
+    e = cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, st);
+  return e;
 }
+
+// Evaluation plan of lanes [lo, hi) of a lane set, built on the host.
+struct EvalSet {
+  ProbDev* probs = nullptr;
+  EvalLane* lanes = nullptr;
+  EvalItem* it1 = nullptr;
+  EvalItem* it2 = nullptr;
+  double2* dens = nullptr;   // rho, w rho and the pass-1 partials of every lane
+  EvalPlan plan{};
+
+  cudaError_t build(const LaneSet& L, int lo, int hi, double* s_base, double* f_base,
+                    double* g_base, const int64_t* status_base, size_t status_stride,
+                    cudaStream_t st) {
+    std::vector<ProbDev> pv;
+    size_t smem1 = 0, smem2 = 0;
+    int max_d = 1;
+    for (const cco_problem* p : L.uniq) {
+      pv.push_back(p->host);
+      smem1 = std::max(smem1, p->smem1);
+      smem2 = std::max(smem2, p->smem2);
+      max_d = std::max(max_d, p->d);
+    }
+    size_t dn = 0;
+    for (int i = lo; i < hi; ++i) dn += (size_t)L.prob[i]->M * (2 + L.prob[i]->host.ntile1);
+    cudaError_t e = pool_alloc(&dens, sizeof(double2) * std::max<size_t>(dn, 1), st);
+    std::vector<EvalLane> lv;
+    std::vector<EvalItem> i1, i2;
+    size_t o = 0;
+    for (int i = lo; i < hi; ++i) {
+      const cco_problem* p = L.prob[i];
+      const size_t M = p->M;
+      EvalLane ln{};
+      ln.s = s_base + L.voff[i];
+      ln.f = f_base + i;
+      ln.g = g_base ? g_base + L.voff[i] : nullptr;
+      ln.rho = dens + o;
+      ln.rhow = dens + o + M;
+      ln.part = dens + o + 2 * M;
+      o += M * (2 + p->host.ntile1);
+      ln.status = status_base ? status_base + (size_t)i * status_stride : nullptr;
+      ln.prob = L.pidx[i];
+      const int j = i - lo;
+      for (int t = 0; t < p->host.ntile1; ++t) i1.push_back(EvalItem{j, t});
+      for (int t = 0; t < p->host.ntile2; ++t) i2.push_back(EvalItem{j, t});
+      lv.push_back(ln);
+    }
+    if (e == cudaSuccess) e = upload(&probs, pv, st);
+    if (e == cudaSuccess) e = upload(&lanes, lv, st);
+    if (e == cudaSuccess) e = upload(&it1, i1, st);
+    if (e == cudaSuccess) e = upload(&it2, i2, st);
+    plan.probs = probs;
+    plan.lanes = lanes;
+    plan.items1 = it1;
+    plan.items2 = it2;
+    plan.n_lanes = hi - lo;
+    plan.n_items1 = (int)i1.size();
+    plan.n_items2 = (int)i2.size();
+    plan.max_d = max_d;
+    plan.smem1 = smem1;
+    plan.smem2 = smem2;
+    plan.want_grad = g_base != nullptr;
+    return e;
+  }
+  void release(cudaStream_t st) {
+    cudaFreeAsync(probs, st);
+    cudaFreeAsync(lanes, st);
+    cudaFreeAsync(it1, st);
+    cudaFreeAsync(it2, st);
+    cudaFreeAsync(dens, st);
+  }
+};
 
 bool out_ok(const cco_relax_out* o) {
   return o && o->s && o->energy && o->grad_norm && o->n_evals && o->n_iters && o->status;
 }
 
-}  // namespace
+// Device copies of the lane layout arrays (offsets and lengths).
+struct LaneArrays {
+  int64_t *voff = nullptr, *soff = nullptr, *toff = nullptr, *hoff = nullptr;
+  int *lnd = nullptr, *lld = nullptr;
+  cudaError_t build(const LaneSet& L, int64_t cap, int m, cudaStream_t st) {
+    std::vector<int64_t> th(L.B), hh(L.B);
+    int64_t t = 0, h = 0;
+    for (int i = 0; i < L.B; ++i) {
+      th[i] = t;
+      hh[i] = h;
+      t += cap * L.nd[i];
+      h += (int64_t)m * L.ld[i];
+    }
+    cudaError_t e = upload(&voff, L.voff, st);
+    if (e == cudaSuccess) e = upload(&soff, L.soff, st);
+    if (e == cudaSuccess) e = upload(&toff, th, st);
+    if (e == cudaSuccess) e = upload(&hoff, hh, st);
+    if (e == cudaSuccess) e = upload(&lnd, L.nd, st);
+    if (e == cudaSuccess) e = upload(&lld, L.ld, st);
+    return e;
+  }
+  int64_t hist_total(const LaneSet& L, int m) const {
+    int64_t h = 0;
+    for (int i = 0; i < L.B; ++i) h += (int64_t)m * L.ld[i];
+    return h;
+  }
+  void release(cudaStream_t st) {
+    cudaFreeAsync(voff, st);
+    cudaFreeAsync(soff, st);
+    cudaFreeAsync(toff, st);
+    cudaFreeAsync(hoff, st);
+    cudaFreeAsync(lnd, st);
+    cudaFreeAsync(lld, st);
+  }
+};
 
-extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const double* s0,
-                                 const cco_descent_settings* cfg, int chunk_iters,
-                                 cco_relax_out* out) {
-  if (!p || !cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
+int check_traj(const cco_relax_out* out, bool rec) {
+  if (rec && (!out->traj_s || !out->traj_energy || !out->traj_step || !out->traj_iteration ||
+              !out->traj_count))
+    return fail(CCO_ERR_ARG, "trajectory recording needs the traj_* outputs");
+  return CCO_OK;
+}
+
+int relax_descent_set(const LaneSet& L, cudaStream_t st, const double* s0,
+                      const cco_descent_settings* cfg, cco_relax_out* out) {
+  if (!cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
   if (!out_ok(out)) return fail(CCO_ERR_ARG, "incomplete output struct");
-  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
-  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
   if (cfg->max_evals < 0) return fail(CCO_ERR_ARG, "max_evals must be >= 0");
   const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
-  if (rec && (!out->traj_s || !out->traj_energy || !out->traj_step || !out->traj_iteration || !out->traj_count))
-    return fail(CCO_ERR_ARG, "trajectory recording needs the traj_* outputs");
-  DeviceGuard guard(p->device);
-  cudaStream_t st = (cudaStream_t)stream;
-  const int B = batch;
-  const size_t nd = (size_t)p->N * p->d;
+  if (check_traj(out, rec) != CCO_OK) return CCO_ERR_ARG;
+  DeviceGuard guard(L.device);
+  const int B = L.B;
+  const size_t V = L.v_total;
   DescentArgs a{};
   a.B = B;
-  a.N = p->N;
-  a.d = p->d;
-  a.nd = (int)nd;
   a.step_init = cfg->step_init;
   a.step_min = cfg->step_min;
   a.shrink = cfg->shrink;
@@ -741,18 +860,24 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
   a.max_iters = cfg->max_evals / 2;
   a.rec_every = rec ? cfg->record_every : 1;
   a.rec_cap = rec ? cfg->max_records : 0;
+  LaneArrays la;
+  CCO_CUDA(la.build(L, a.rec_cap, 0, st));
+  a.voff = la.voff;
+  a.soff = la.soff;
+  a.toff = la.toff;
+  a.lnd = la.lnd;
   double* vec = nullptr;   // s, g, ps, pg
   double* sc = nullptr;    // f, step, norm, pf
   int64_t* ic = nullptr;   // it, n_evals, status, t0, t1
   int* ph = nullptr;       // phase, nonzero
-  CCO_CUDA(pool_alloc(&vec, sizeof(double) * nd * B * 4, st));
+  CCO_CUDA(pool_alloc(&vec, sizeof(double) * V * 4, st));
   CCO_CUDA(pool_alloc(&sc, sizeof(double) * B * 4, st));
   CCO_CUDA(pool_alloc(&ic, sizeof(int64_t) * B * 5, st));
   CCO_CUDA(pool_alloc(&ph, sizeof(int) * B * 2, st));
   a.s = vec;
-  a.g = vec + nd * B;
-  a.ps = vec + 2 * nd * B;
-  double* pg = vec + 3 * nd * B;
+  a.g = vec + V;
+  a.ps = vec + 2 * V;
+  double* pg = vec + 3 * V;
   a.pg = pg;
   a.f = sc;
   a.step = sc + B;
@@ -774,14 +899,24 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
     a.traj_count = out->traj_count;
   }
   const int nbr = branch_count(B);
-  EvalWS ws[kMaxBranches];
+  EvalSet ws[kMaxBranches];
   DescentArgs ab[kMaxBranches];
   for (int b = 0; b < nbr; ++b) {
-    const int lo = b * B / nbr, nb = (b + 1) * B / nbr - lo;
-    ab[b] = descent_shift(a, lo, nb);
-    CCO_CUDA(ws[b].alloc(p, nb, st));
-    CCO_CUDA(ws[b].build(p, nb, ab[b].ps, nd, pf + lo, 1, pg + (size_t)lo * nd, nd,
-                         a.status + lo, 1, st));
+    const int lo = b * B / nbr, hi = (b + 1) * B / nbr;
+    DescentArgs r = a;
+    r.B = hi - lo;
+    r.voff += lo; r.soff += lo; r.toff += lo; r.lnd += lo;
+    r.pf += lo; r.f += lo; r.step += lo; r.norm += lo;
+    r.it += lo; r.n_evals += lo; r.status += lo; r.phase += lo; r.nonzero += lo;
+    r.t0 += lo; r.t1 += lo;
+    if (rec) {
+      r.traj_e += (size_t)lo * a.rec_cap;
+      r.traj_step += (size_t)lo * a.rec_cap;
+      r.traj_it += (size_t)lo * a.rec_cap;
+      r.traj_count += lo;
+    }
+    ab[b] = r;
+    CCO_CUDA(ws[b].build(L, lo, hi, a.ps, pf, pg, a.status, 1, st));
   }
   CCO_CUDA(descent_init(a, s0, st));
   auto tick = [&](cudaStream_t s, int b) -> cudaError_t {
@@ -798,8 +933,9 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
     if (e != cudaSuccess) rc = cuda_fail(e, "descent_finalize");
   }
   out->ticks = ticks;
-  out->launches = ticks * 4 * nbr + ticks / kGraphTicks + 2 + nbr;
+  out->launches = ticks * 4 * nbr + ticks / kGraphTicks + 2;
   for (int b = 0; b < nbr; ++b) ws[b].release(st);
+  la.release(st);
   cudaFreeAsync(vec, st);
   cudaFreeAsync(sc, st);
   cudaFreeAsync(ic, st);
@@ -809,33 +945,23 @@ extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const 
   return rc;
 }
 
-extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const double* s0,
-                               const cco_lbfgs_settings* cfg, int chunk_iters,
-                               cco_relax_out* out) {
-  if (!p || !cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
+int relax_lbfgs_set(const LaneSet& L, cudaStream_t st, const double* s0,
+                    const cco_lbfgs_settings* cfg, cco_relax_out* out) {
+  if (!cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
   if (!out_ok(out)) return fail(CCO_ERR_ARG, "incomplete output struct");
-  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
-  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
   if (cfg->n_rescales < 1 || cfg->n_rescales > CCO_MAX_RESCALES)
     return fail(CCO_ERR_ARG, "need 1..%d rescale passes", CCO_MAX_RESCALES);
   if (cfg->memory < 1) return fail(CCO_ERR_ARG, "memory must be >= 1");
   if (cfg->memory > 256) return fail(CCO_ERR_ARG, "memory must be <= 256 on this build");
   if (cfg->max_linesearch_steps < 1) return fail(CCO_ERR_ARG, "max_linesearch_steps must be >= 1");
   const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
-  if (rec && (!out->traj_s || !out->traj_energy || !out->traj_step || !out->traj_iteration || !out->traj_count))
-    return fail(CCO_ERR_ARG, "trajectory recording needs the traj_* outputs");
-  DeviceGuard guard(p->device);
-  cudaStream_t st = (cudaStream_t)stream;
-  const int B = batch;
-  const size_t nd = (size_t)p->N * p->d;
-  const size_t ld = (nd + 3) & ~(size_t)3;  // 32-byte rows, zero padding
+  if (check_traj(out, rec) != CCO_OK) return CCO_ERR_ARG;
+  DeviceGuard guard(L.device);
+  const int B = L.B;
+  const size_t V = L.v_total;
   const int m = (int)cfg->memory;
   LbArgs A{};
   A.B = B;
-  A.N = p->N;
-  A.d = p->d;
-  A.nd = (int)nd;
-  A.ld = (int)ld;
   A.m = m;
   A.n_pass = cfg->n_rescales;
   for (int i = 0; i < CCO_MAX_RESCALES; ++i) A.rescales[i] = i < cfg->n_rescales ? cfg->rescales[i] : 1.0;
@@ -858,36 +984,45 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
       configured = 200 * 1024;
     }
   }
+  LaneArrays la;
+  CCO_CUDA(la.build(L, A.rec_cap, m, st));
+  A.voff = la.voff;
+  A.soff = la.soff;
+  A.toff = la.toff;
+  A.hoff = la.hoff;
+  A.lnd = la.lnd;
+  A.lld = la.lld;
+  const size_t H = la.hist_total(L, m);
   LbState* stv = nullptr;
   double* vec = nullptr;   // x, s, g, dir, glo, ps, pg
   double* hist = nullptr;  // S, Y
   double* dots = nullptr;  // SY, YY
   double* pf = nullptr;
   double* trig = nullptr;
+  double* scal = nullptr;
   CCO_CUDA(pool_alloc(&stv, sizeof(LbState) * B, st));
-  CCO_CUDA(pool_alloc(&vec, sizeof(double) * ld * B * 7, st));
-  CCO_CUDA(cudaMemsetAsync(vec, 0, sizeof(double) * ld * B * 7, st));
-  CCO_CUDA(pool_alloc(&hist, sizeof(double) * ld * B * m * 2, st));
+  CCO_CUDA(pool_alloc(&vec, sizeof(double) * V * 7, st));
+  CCO_CUDA(cudaMemsetAsync(vec, 0, sizeof(double) * V * 7, st));
+  CCO_CUDA(pool_alloc(&hist, sizeof(double) * H * 2, st));
   CCO_CUDA(pool_alloc(&dots, sizeof(double) * (size_t)B * m * m * 2, st));
   CCO_CUDA(pool_alloc(&pf, sizeof(double) * B, st));
   if (!in_smem) CCO_CUDA(pool_alloc(&trig, tri_bytes * B, st));
-  A.nblkB = (int)((ld / 2 + 255) / 256);
+  A.nblkB = (int)((L.max_ld / 2 + 255) / 256);
   A.scal_stride = (4 * m + 1 + A.nblkB + 1) & ~1;
-  double* scal = nullptr;
   CCO_CUDA(pool_alloc(&scal, sizeof(double) * (size_t)A.scal_stride * B, st));
   A.scal = scal;
   A.st = stv;
   A.x = vec;
-  A.s = vec + ld * B;
-  A.g = vec + 2 * ld * B;
-  A.dir = vec + 3 * ld * B;
-  A.glo = vec + 4 * ld * B;
-  A.ps = vec + 5 * ld * B;
-  double* pg = vec + 6 * ld * B;
+  A.s = vec + V;
+  A.g = vec + 2 * V;
+  A.dir = vec + 3 * V;
+  A.glo = vec + 4 * V;
+  A.ps = vec + 5 * V;
+  double* pg = vec + 6 * V;
   A.pg = pg;
   A.pf = pf;
   A.Sh = hist;
-  A.Yh = hist + ld * B * m;
+  A.Yh = hist + H;
   A.SYs = dots;
   A.YYs = dots + (size_t)B * m * m;
   A.tri_g = trig;
@@ -901,14 +1036,27 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   const size_t st_stride = sizeof(LbState) / sizeof(int64_t);
   const int64_t* status0 = &stv->status;
   const int nbr = branch_count(B);
-  EvalWS ws[kMaxBranches];
+  EvalSet ws[kMaxBranches];
   LbArgs Ab[kMaxBranches];
   for (int b = 0; b < nbr; ++b) {
-    const int lo = b * B / nbr, nb = (b + 1) * B / nbr - lo;
-    Ab[b] = lbfgs_shift(A, lo, nb);
-    CCO_CUDA(ws[b].alloc(p, nb, st));
-    CCO_CUDA(ws[b].build(p, nb, Ab[b].ps, ld, pf + lo, 1, pg + (size_t)lo * ld, ld,
-                         status0 + (size_t)lo * st_stride, st_stride, st));
+    const int lo = b * B / nbr, hi = (b + 1) * B / nbr;
+    LbArgs r = A;
+    r.B = hi - lo;
+    r.st += lo;
+    r.pf += lo;
+    r.voff += lo; r.soff += lo; r.toff += lo; r.hoff += lo; r.lnd += lo; r.lld += lo;
+    r.SYs += (size_t)lo * m * m;
+    r.YYs += (size_t)lo * m * m;
+    if (r.tri_g) r.tri_g += (size_t)lo * ((size_t)m * (m + 1));
+    r.scal += (size_t)lo * A.scal_stride;
+    if (rec) {
+      r.traj_e += (size_t)lo * A.rec_cap;
+      r.traj_step += (size_t)lo * A.rec_cap;
+      r.traj_it += (size_t)lo * A.rec_cap;
+      r.traj_count += lo;
+    }
+    Ab[b] = r;
+    CCO_CUDA(ws[b].build(L, lo, hi, A.ps, pf, pg, status0, st_stride, st));
   }
   CCO_CUDA(lbfgs_init(A, s0, st));
   auto tick = [&](cudaStream_t s, int b) -> cudaError_t {
@@ -927,8 +1075,9 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
     if (e != cudaSuccess) rc = cuda_fail(e, "lbfgs_finalize");
   }
   out->ticks = ticks;
-  out->launches = ticks * 7 * nbr + ticks / kGraphTicks + 2 + nbr;
+  out->launches = ticks * 7 * nbr + ticks / kGraphTicks + 2;
   for (int b = 0; b < nbr; ++b) ws[b].release(st);
+  la.release(st);
   cudaFreeAsync(stv, st);
   cudaFreeAsync(vec, st);
   cudaFreeAsync(hist, st);
@@ -939,4 +1088,50 @@ extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const do
   cudaError_t e = cudaStreamSynchronize(st);
   if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "relax lbfgs");
   return rc;
+}
+
+}  // namespace
+
+extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const double* s0,
+                                 const cco_descent_settings* cfg, int chunk_iters,
+                                 cco_relax_out* out) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  std::vector<cco_problem*> probs(batch, p);
+  LaneSet L;
+  if (make_laneset(probs.data(), batch, 1, &L) != CCO_OK) return CCO_ERR_ARG;
+  return relax_descent_set(L, (cudaStream_t)stream, s0, cfg, out);
+}
+
+extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const double* s0,
+                               const cco_lbfgs_settings* cfg, int chunk_iters,
+                               cco_relax_out* out) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  std::vector<cco_problem*> probs(batch, p);
+  LaneSet L;
+  if (make_laneset(probs.data(), batch, 4, &L) != CCO_OK) return CCO_ERR_ARG;
+  return relax_lbfgs_set(L, (cudaStream_t)stream, s0, cfg, out);
+}
+
+extern "C" int cco_relax_descent_mixed(cco_problem* const* problems, void* stream, int batch,
+                                       const double* s0, const cco_descent_settings* cfg,
+                                       int chunk_iters, cco_relax_out* out) {
+  if (!problems) return fail(CCO_ERR_ARG, "null problem array");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  LaneSet L;
+  if (make_laneset(problems, batch, 1, &L) != CCO_OK) return CCO_ERR_ARG;
+  return relax_descent_set(L, (cudaStream_t)stream, s0, cfg, out);
+}
+
+extern "C" int cco_relax_lbfgs_mixed(cco_problem* const* problems, void* stream, int batch,
+                                     const double* s0, const cco_lbfgs_settings* cfg,
+                                     int chunk_iters, cco_relax_out* out) {
+  if (!problems) return fail(CCO_ERR_ARG, "null problem array");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  LaneSet L;
+  if (make_laneset(problems, batch, 4, &L) != CCO_OK) return CCO_ERR_ARG;
+  return relax_lbfgs_set(L, (cudaStream_t)stream, s0, cfg, out);
 }

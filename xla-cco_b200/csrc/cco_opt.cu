@@ -71,16 +71,18 @@ __device__ void descent_record(const DescentArgs& a, int lane, int64_t it, const
   }
   __syncthreads();
   if (row >= 0) {
-    double* o = a.traj_s + ((size_t)lane * a.rec_cap + row) * a.nd;
-    for (int e = threadIdx.x; e < a.nd; e += blockDim.x) o[e] = wrap01(s[e]);
+    const int nd = a.lnd[lane];
+    double* o = a.traj_s + a.toff[lane] + (size_t)row * nd;
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) o[e] = wrap01(s[e]);
   }
 }
 
 __global__ void k_descent_init(DescentArgs a, const double* __restrict__ s0) {
   const int lane = blockIdx.x;
-  const size_t off = (size_t)lane * a.nd;
-  for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
-    const double v = s0[off + e];
+  const size_t off = a.voff[lane], so = a.soff[lane];
+  const int nd = a.lnd[lane];
+  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
+    const double v = s0[so + e];
     a.ps[off + e] = v;
     a.s[off + e] = v;
   }
@@ -98,10 +100,11 @@ __global__ void k_descent_init(DescentArgs a, const double* __restrict__ s0) {
 
 // Gradient norm and the exact all-zero test of the accepted gradient.
 __device__ void descent_norm(const DescentArgs& a, int lane, double* red) {
-  const double* g = a.g + (size_t)lane * a.nd;
+  const double* g = a.g + a.voff[lane];
+  const int nd = a.lnd[lane];
   double ss = 0.0;
   int nz = 0;
-  for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
     const double v = g[e];
     ss += v * v;
     nz |= (v != 0.0);
@@ -119,14 +122,15 @@ __global__ void __launch_bounds__(kUpdThreads) k_descent_update(DescentArgs a) {
   __shared__ int s_reject, s_status;
   const int lane = blockIdx.x;
   if (a.status[lane] != CCO_STATUS_RUNNING) return;
-  const size_t off = (size_t)lane * a.nd;
+  const size_t off = a.voff[lane];
+  const int nd = a.lnd[lane];
   double* s = a.s + off;
   double* g = a.g + off;
   double* ps = a.ps + off;
   const double* pg = a.pg + off;
   if (a.phase[lane] == PH_INIT) {
     // init_one (descent.py:121-141): one evaluation at s0, no iteration
-    for (int e = threadIdx.x; e < a.nd; e += blockDim.x) g[e] = pg[e];
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) g[e] = pg[e];
     descent_norm(a, lane, red);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_descent_update(DescentArgs a) {
     }
     __syncthreads();
     if (!s_reject) {
-      for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+      for (int e = threadIdx.x; e < nd; e += blockDim.x) {
         s[e] = ps[e];
         g[e] = pg[e];
       }
@@ -173,7 +177,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_descent_update(DescentArgs a) {
   if (s_status == CCO_STATUS_RUNNING) {
     // next probe: xn = s - (g / |g|) * step  (0 * g when |g| = 0)
     const double norm = a.norm[lane], step = a.step[lane];
-    for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) {
       const double gn = norm > 0.0 ? __ddiv_rn(g[e], norm) : 0.0 * g[e];
       ps[e] = __dsub_rn(s[e], __dmul_rn(gn, step));
     }
@@ -185,12 +189,13 @@ __global__ void k_descent_finalize(DescentArgs a, double* s_out, double* e_out, 
                                    int64_t* lat_out) {
   __shared__ double red[32];
   const int lane = blockIdx.x;
-  const size_t off = (size_t)lane * a.nd;
+  const size_t off = a.voff[lane], so = a.soff[lane];
+  const int nd = a.lnd[lane];
   double ss = 0.0;
-  for (int e = threadIdx.x; e < a.nd; e += blockDim.x) {
+  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
     const double v = a.g[off + e];
     ss += v * v;
-    s_out[off + e] = wrap01(a.s[off + e]);
+    s_out[so + e] = wrap01(a.s[off + e]);
   }
   ss = block_sum(ss, red);
   if (threadIdx.x == 0) {
@@ -317,8 +322,9 @@ __device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double*
   }
   __syncthreads();
   if (row >= 0) {
-    double* o = A.traj_s + ((size_t)lane * A.rec_cap + row) * A.nd;
-    for (int e = threadIdx.x; e < A.nd; e += blockDim.x) o[e] = wrap01(s[e]);
+    const int nd = A.lnd[lane];
+    double* o = A.traj_s + A.toff[lane] + (size_t)row * nd;
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) o[e] = wrap01(s[e]);
   }
   __syncthreads();
 }
@@ -329,8 +335,8 @@ __device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double*
 // is flagged for a new direction (passes A, scalar, B of this tick).
 __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
   LbState& L = sh.L;
-  const int ld = A.ld, h2 = A.ld >> 1, m = A.m;
-  const size_t off = (size_t)lane * ld;
+  const int ld = A.lld[lane], h2 = ld >> 1, m = A.m;
+  const size_t off = A.voff[lane];
   double* x = A.x + off;
   double* s = A.s + off;
   double* g = A.g + off;
@@ -346,8 +352,8 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
     const bool probe = outcome == LS_ACCEPT_PROBE;
     const double al = probe ? L.alpha : L.a_lo;
     const int sl = L.hhead;
-    double* Sr = A.Sh + ((size_t)lane * m + sl) * ld;
-    double* Yr = A.Yh + ((size_t)lane * m + sl) * ld;
+    double* Sr = A.Sh + A.hoff[lane] + (size_t)sl * ld;
+    double* Yr = A.Yh + A.hoff[lane] + (size_t)sl * ld;
     for (int e = threadIdx.x; e < h2; e += blockDim.x) {
       const double2 xo = ld2(x, e), dv = ld2(dir, e), go = ld2(g, e);
       const double2 xn = make_double2(xo.x + al * dv.x, xo.y + al * dv.y);
@@ -431,8 +437,8 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
 
 __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
   const int lane = blockIdx.x;
-  for (int e = threadIdx.x; e < A.nd; e += blockDim.x)
-    A.ps[(size_t)lane * A.ld + e] = s0[(size_t)lane * A.nd + e];
+  const int nd = A.lnd[lane];
+  for (int e = threadIdx.x; e < nd; e += blockDim.x) A.ps[A.voff[lane] + e] = s0[A.soff[lane] + e];
   if (threadIdx.x == 0) {
     LbState L = {};
     L.phase = PH_INIT;
@@ -454,8 +460,8 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
   __syncthreads();
   if (sh.L.status != CCO_STATUS_RUNNING) return;
   LbState& L = sh.L;
-  const int h2 = A.ld >> 1;
-  const size_t off = (size_t)lane * A.ld;
+  const int h2 = A.lld[lane] >> 1;
+  const size_t off = A.voff[lane];
   if (L.phase == PH_INIT) {
     // init_one (lbfgs.py:163-197): x = R0 s0, g_x = g_s / R0, one evaluation
     const double R0 = L.R;
@@ -556,14 +562,14 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
   const int p = blockIdx.x * (kUpdThreads / 32) + warp;
   if (p >= k) return;
-  const int ld = A.ld, h2 = A.ld >> 1, m = A.m;
+  const int ld = A.lld[lane], h2 = ld >> 1, m = A.m;
   const int head = Lp->hhead;
   const bool np = Lp->newpair != 0;
   const int sp = (head - k + p + m) % m, sn = (head - 1 + m) % m;
-  const double* g = A.g + (size_t)lane * ld;
-  const double* sr = A.Sh + ((size_t)lane * m + sp) * ld;
-  const double* yr = A.Yh + ((size_t)lane * m + sp) * ld;
-  const double* yn = A.Yh + ((size_t)lane * m + sn) * ld;
+  const double* g = A.g + A.voff[lane];
+  const double* sr = A.Sh + A.hoff[lane] + (size_t)sp * ld;
+  const double* yr = A.Yh + A.hoff[lane] + (size_t)sp * ld;
+  const double* yn = A.Yh + A.hoff[lane] + (size_t)sn * ld;
   double ag = 0.0, bg = 0.0, sy = 0.0, yy = 0.0;
   int e = wl;
   for (; e + 96 < h2; e += 128) {
@@ -674,9 +680,9 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
     }
   } else {
     // gamma (optax scale_by_lbfgs) on a fresh pass: min(1, 1/|g|)
-    const double* g = A.g + (size_t)lane * A.ld;
+    const double* g = A.g + A.voff[lane];
     double ss = 0.0;
-    for (int e = threadIdx.x; e < (A.ld >> 1); e += blockDim.x) {
+    for (int e = threadIdx.x; e < (A.lld[lane] >> 1); e += blockDim.x) {
       const double2 v = ld2(g, e);
       ss += v.x * v.x + v.y * v.y;
     }
@@ -763,7 +769,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passB(LbArgs A) {
   const LbState* Lp = A.st + lane;
   if (Lp->status != CCO_STATUS_RUNNING || !Lp->need_dir) return;
   const int k = Lp->hk, m = A.m, head = Lp->hhead;
-  const int ld = A.ld, h2 = A.ld >> 1;
+  const int ld = A.lld[lane], h2 = ld >> 1;
   const double R = Lp->R;
   double* sc = scal_row(A, lane);
   const double gam = sc[2 * m];
@@ -777,13 +783,13 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passB(LbArgs A) {
   __syncthreads();
   const double* cy = in_smem ? cyv : sc + 2 * m + 1;
   const double* cs = in_smem ? csv : sc + 3 * m + 1;
-  const size_t off = (size_t)lane * ld;
+  const size_t off = A.voff[lane];
   const double* g = A.g + off;
   const double* x = A.x + off;
   double* dir = A.dir + off;
   double* ps = A.ps + off;
-  const double* Sh = A.Sh + (size_t)lane * m * ld;
-  const double* Yh = A.Yh + (size_t)lane * m * ld;
+  const double* Sh = A.Sh + A.hoff[lane];
+  const double* Yh = A.Yh + A.hoff[lane];
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   double dp = 0.0;
   if (e < h2) {
@@ -824,12 +830,13 @@ __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double*
                                  int64_t* lat_out) {
   __shared__ double red[32];
   const int lane = blockIdx.x;
-  const size_t off = (size_t)lane * A.ld;
+  const size_t off = A.voff[lane], so = A.soff[lane];
+  const int nd = A.lnd[lane];
   double ss = 0.0;
-  for (int e = threadIdx.x; e < A.nd; e += blockDim.x) {
+  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
     const double v = A.g[off + e];
     ss += v * v;
-    s_out[(size_t)lane * A.nd + e] = wrap01(A.s[off + e]);
+    s_out[so + e] = wrap01(A.s[off + e]);
   }
   ss = block_sum(ss, red);
   if (threadIdx.x == 0) {

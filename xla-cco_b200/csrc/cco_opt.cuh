@@ -8,8 +8,16 @@ namespace cco {
 enum : int { PH_INIT = 0, PH_ITER = 1, PH_EXPAND = 1, PH_ZOOM = 2 };
 
 // ------------------------------------------------------------ descent
+// Lane layouts: lanes may differ in N and d (mixed batches, the serving
+// pool). Every per-lane array is addressed through device offset arrays:
+//   voff[i]  offset (doubles) of lane i in each lane-vector array
+//   soff[i]  offset of lane i in the caller's packed positions (N_i d_i each)
+//   toff[i]  offset of lane i's trajectory rows in traj_s
+//   lnd[i]   N_i d_i
 struct DescentArgs {
-  int B, N, d, nd;
+  int B;
+  const int64_t *voff, *soff, *toff;
+  const int* lnd;
   double step_init, step_min, shrink, grow, rel_tol, energy_tol;
   int64_t max_iters;      // max_evals // 2
   int64_t rec_every, rec_cap;
@@ -42,8 +50,11 @@ struct LbState {
 };
 
 struct LbArgs {
-  int B, N, d, nd, m, n_pass;
-  int ld;                 // padded vector length (multiple of 4 doubles)
+  int B, m, n_pass;
+  // lane layouts (see DescentArgs); lld[i] = N_i d_i rounded up to 4 doubles
+  // (16-byte rows, zero padding); hoff[i] = offset of lane i in Sh and Yh
+  const int64_t *voff, *soff, *toff, *hoff;
+  const int *lnd, *lld;
   double rescales[CCO_MAX_RESCALES];
   double energy_tol, grad_tol;
   int64_t budget, patience, max_ls;

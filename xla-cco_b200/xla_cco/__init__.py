@@ -22,7 +22,7 @@ from xla_cco.kvectors import (
     ka_from_chi,
     unit_ball_volume,
 )
-from xla_cco.minimize import relax
+from xla_cco.minimize import relax, relax_mixed
 from xla_cco.minimize.descent import DescentSettings, adaptive_descent
 from xla_cco.minimize.lbfgs import LBFGSSettings, lbfgs
 from xla_cco.minimize.result import RelaxResult, Trajectory
@@ -46,6 +46,7 @@ __all__ = [
     "lbfgs",
     "make_stealthy_energy",
     "relax",
+    "relax_mixed",
     "require_float64",
     "unit_ball_volume",
     "wrap_fractional",

@@ -103,6 +103,16 @@ SIGNATURES = {
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(LBFGSSettingsC), ctypes.c_int,
          ctypes.POINTER(RelaxOutC)],
     ),  # fmt: skip
+    "cco_relax_descent_mixed": (
+        ctypes.c_int,
+        [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(DescentSettingsC), ctypes.c_int,
+         ctypes.POINTER(RelaxOutC)],
+    ),  # fmt: skip
+    "cco_relax_lbfgs_mixed": (
+        ctypes.c_int,
+        [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(LBFGSSettingsC), ctypes.c_int,
+         ctypes.POINTER(RelaxOutC)],
+    ),  # fmt: skip
 }
 
 _lock = threading.Lock()

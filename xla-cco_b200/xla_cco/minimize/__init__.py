@@ -11,7 +11,7 @@ result does not depend on it (the reference guarantees the same).
 
 from __future__ import annotations
 
-from typing import Any, Union
+from typing import Any, List, Sequence, Tuple, Union
 
 import numpy as np
 
@@ -21,7 +21,8 @@ from xla_cco.minimize.descent import DescentSettings
 from xla_cco.minimize.lbfgs import LBFGSSettings
 from xla_cco.minimize.result import RelaxResult, Trajectory
 
-__all__ = ["relax", "relax_device", "DescentSettings", "LBFGSSettings"]
+__all__ = ["relax", "relax_device", "relax_mixed", "relax_mixed_device", "DescentSettings",
+           "LBFGSSettings"]
 
 
 def _descent_c(st: DescentSettings) -> _native.DescentSettingsC:
@@ -50,6 +51,60 @@ def _lbfgs_c(st: LBFGSSettings) -> _native.LBFGSSettingsC:
     return c
 
 
+def _settings_c(settings: Any, mixed: bool = False):
+    suffix = "_mixed" if mixed else ""
+    if isinstance(settings, DescentSettings):
+        return _descent_c(settings), "cco_relax_descent" + suffix
+    if isinstance(settings, LBFGSSettings):
+        return _lbfgs_c(settings), "cco_relax_lbfgs" + suffix
+    raise TypeError(f"unsupported settings type {type(settings).__name__}")
+
+
+def _outputs(b: int, s_shape: tuple, traj_s_shape: tuple, settings: Any, dev: Any) -> dict:
+    import torch
+
+    f64, i64 = torch.float64, torch.int64
+    out = {
+        "s": torch.empty(s_shape, dtype=f64, device=dev),
+        "energy": torch.empty(b, dtype=f64, device=dev),
+        "grad_norm": torch.empty(b, dtype=f64, device=dev),
+        "n_evals": torch.empty(b, dtype=i64, device=dev),
+        "n_iters": torch.empty(b, dtype=i64, device=dev),
+        "status": torch.empty(b, dtype=i64, device=dev),
+        "latency_ns": torch.empty(b, dtype=i64, device=dev),
+    }
+    if settings.record_every > 0 and settings.max_records > 0:
+        cap = int(settings.max_records)
+        out["traj_s"] = torch.zeros(traj_s_shape, dtype=f64, device=dev)
+        out["traj_energy"] = torch.zeros((b, cap), dtype=f64, device=dev)
+        out["traj_step"] = torch.zeros((b, cap), dtype=f64, device=dev)
+        out["traj_iteration"] = torch.zeros((b, cap), dtype=i64, device=dev)
+        out["traj_count"] = torch.zeros(b, dtype=i64, device=dev)
+    return out
+
+
+def _call_relax(fn: str, first: Any, dev: Any, b: int, s0_ptr: int, cset: Any, chunk_iters: int,
+                out: dict) -> None:  # fmt: skip
+    import torch
+
+    co = _native.RelaxOutC()
+    for key in ("s", "energy", "grad_norm", "n_evals", "n_iters", "status", "latency_ns",
+                "traj_s", "traj_energy", "traj_step", "traj_iteration", "traj_count"):  # fmt: skip
+        if key in out:
+            setattr(co, key, out[key].data_ptr())
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        code = getattr(_native.load(), fn)(
+            first, stream, b, s0_ptr, _native.ctypes.byref(cset), int(chunk_iters),
+            _native.ctypes.byref(co),
+        )  # fmt: skip
+    if code == _native.CCO_ERR_ROUNDS:
+        raise RuntimeError("relax did not finish within the round bound")
+    _native.check(code, fn)
+    out["ticks"] = int(co.ticks)
+    out["launches"] = int(co.launches)
+
+
 def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
                  chunk_iters: int = 2_000) -> dict:  # fmt: skip
     """Run the device relaxation on a CUDA tensor ``s0`` (B, N, d); results stay on the device.
@@ -63,53 +118,15 @@ def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSet
 
     if not isinstance(energy, StealthyEnergy):
         raise TypeError("the B200 relax path evaluates a StealthyEnergy on the device")
-    if isinstance(settings, DescentSettings):
-        cset, fn = _descent_c(settings), "cco_relax_descent"
-    elif isinstance(settings, LBFGSSettings):
-        cset, fn = _lbfgs_c(settings), "cco_relax_lbfgs"
-    else:
-        raise TypeError(f"unsupported settings type {type(settings).__name__}")
+    cset, fn = _settings_c(settings)
     if energy._zero_weight != 0.0:
         raise ValueError("zero k rows with nonzero weight are not supported by relax")
     b, n, d = s0.shape
     assert d == energy.dim, "dimension mismatch"
     dev = s0.device
     h = energy.problem_handle(dev.index if dev.index is not None else torch.cuda.current_device(), n)
-    f64, i64 = torch.float64, torch.int64
-    out = {
-        "s": torch.empty_like(s0),
-        "energy": torch.empty(b, dtype=f64, device=dev),
-        "grad_norm": torch.empty(b, dtype=f64, device=dev),
-        "n_evals": torch.empty(b, dtype=i64, device=dev),
-        "n_iters": torch.empty(b, dtype=i64, device=dev),
-        "status": torch.empty(b, dtype=i64, device=dev),
-        "latency_ns": torch.empty(b, dtype=i64, device=dev),
-    }
-    rec = settings.record_every > 0 and settings.max_records > 0
-    cap = int(settings.max_records)
-    if rec:
-        out["traj_s"] = torch.zeros((b, cap, n, d), dtype=f64, device=dev)
-        out["traj_energy"] = torch.zeros((b, cap), dtype=f64, device=dev)
-        out["traj_step"] = torch.zeros((b, cap), dtype=f64, device=dev)
-        out["traj_iteration"] = torch.zeros((b, cap), dtype=i64, device=dev)
-        out["traj_count"] = torch.zeros(b, dtype=i64, device=dev)
-    co = _native.RelaxOutC()
-    for key in ("s", "energy", "grad_norm", "n_evals", "n_iters", "status", "latency_ns"):
-        setattr(co, key, out[key].data_ptr())
-    if rec:
-        for key in ("traj_s", "traj_energy", "traj_step", "traj_iteration", "traj_count"):
-            setattr(co, key, out[key].data_ptr())
-    with torch.cuda.device(dev):
-        stream = torch.cuda.current_stream(dev).cuda_stream
-        code = getattr(_native.load(), fn)(
-            h, stream, b, s0.data_ptr(), _native.ctypes.byref(cset), int(chunk_iters),
-            _native.ctypes.byref(co),
-        )  # fmt: skip
-    if code == _native.CCO_ERR_ROUNDS:
-        raise RuntimeError("relax did not finish within the round bound")
-    _native.check(code, fn)
-    out["ticks"] = int(co.ticks)
-    out["launches"] = int(co.launches)
+    out = _outputs(b, tuple(s0.shape), (b, int(settings.max_records), n, d), settings, dev)
+    _call_relax(fn, h, dev, b, s0.data_ptr(), cset, chunk_iters, out)
     return out
 
 
@@ -149,3 +166,95 @@ def relax(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
         n_evals=conv(out["n_evals"]), n_iters=conv(out["n_iters"]), status=conv(out["status"]),
         trajectory=traj,
     )  # fmt: skip
+
+
+def relax_mixed_device(energies: Sequence[Any], s0: Any, shapes: Sequence[Tuple[int, int]],
+                       settings: Union[DescentSettings, LBFGSSettings],
+                       chunk_iters: int = 2_000) -> dict:  # fmt: skip
+    """One device relaxation over lanes of different problems (N, d and k-set).
+
+    ``energies[i]`` is lane i's ``StealthyEnergy`` and ``shapes[i]`` its
+    (N_i, d_i); ``s0`` is a flat CUDA float64 tensor with every lane's
+    positions packed one after the other. Returns a dict of CUDA tensors:
+    ``s`` packed the same way, per-lane scalars of shape (B,), ``traj_s``
+    packed with ``max_records`` rows per lane, plus ``offsets`` (B + 1 element
+    offsets into ``s``), ``ticks`` and ``launches``.
+    """
+    import torch
+
+    from xla_cco.energy import StealthyEnergy
+
+    cset, fn = _settings_c(settings, mixed=True)
+    b = len(energies)
+    if b < 1 or len(shapes) != b:
+        raise ValueError("need one (N, d) shape per energy and at least one configuration")
+    dev = s0.device
+    index = dev.index if dev.index is not None else torch.cuda.current_device()
+    handles = (_native.ctypes.c_void_p * b)()
+    offsets = [0]
+    for i, (en, (n, d)) in enumerate(zip(energies, shapes)):
+        if not isinstance(en, StealthyEnergy):
+            raise TypeError("the B200 relax path evaluates a StealthyEnergy on the device")
+        if en._zero_weight != 0.0:
+            raise ValueError("zero k rows with nonzero weight are not supported by relax")
+        assert d == en.dim, f"lane {i}: dimension mismatch"
+        handles[i] = en.problem_handle(index, int(n))
+        offsets.append(offsets[-1] + int(n) * int(d))
+    assert s0.numel() == offsets[-1], "s0 does not hold the packed positions of every lane"
+    cap = int(settings.max_records)
+    out = _outputs(b, (offsets[-1],), (cap * offsets[-1],), settings, dev)
+    _call_relax(fn, handles, dev, b, s0.data_ptr(), cset, chunk_iters, out)
+    out["offsets"] = offsets
+    return out
+
+
+def relax_mixed(energies: Sequence[Any], s0: Sequence[Any],
+                settings: Union[DescentSettings, LBFGSSettings],
+                chunk_iters: int = 2_000) -> List[RelaxResult]:  # fmt: skip
+    """Relax instances of different N, d and k-set together in one device run.
+
+    ``energies[i]`` and ``s0[i]`` (an (N_i, d_i) float64 array, NumPy or
+    torch) form lane i. Returns one ``RelaxResult`` per lane with a batch axis
+    of 1, bit-identical to ``relax(energies[i], s0[i][None], settings)``.
+    """
+    import torch
+
+    assert chunk_iters >= 1, "chunk_iters must be positive"
+    if len(energies) != len(s0) or not energies:
+        raise ValueError("need one initial configuration per energy and at least one")
+    if not isinstance(settings, (DescentSettings, LBFGSSettings)):
+        raise TypeError(f"unsupported settings type {type(settings).__name__}")
+    _native.require_gpu()
+    host = not (isinstance(s0[0], torch.Tensor) and s0[0].is_cuda)
+    shapes = []
+    for x in s0:
+        require_float64(x, "s0")
+        assert x.ndim == 2, "each configuration must have shape (n, d)"
+        shapes.append((int(x.shape[0]), int(x.shape[1])))
+    if host:
+        flat = np.concatenate([np.asarray(x.cpu() if isinstance(x, torch.Tensor) else x).ravel()
+                               for x in s0])  # fmt: skip
+        s_dev = torch.from_numpy(flat).pin_memory().cuda(non_blocking=True)
+    else:
+        s_dev = torch.cat([x.reshape(-1) for x in s0])
+    out = relax_mixed_device(energies, s_dev, shapes, settings, chunk_iters)
+    conv = (lambda t: t.cpu().numpy()) if host else (lambda t: t)
+    keys = ("s", "energy", "grad_norm", "n_evals", "n_iters", "status")
+    tkeys = ("traj_s", "traj_energy", "traj_step", "traj_iteration", "traj_count")
+    res = {k: conv(out[k]) for k in keys + tkeys if k in out}
+    off, cap = out["offsets"], int(settings.max_records)
+    results = []
+    for i, (n, d) in enumerate(shapes):
+        traj = None
+        if "traj_s" in res:
+            traj = Trajectory(
+                s=res["traj_s"][cap * off[i]:cap * off[i + 1]].reshape(1, cap, n, d),
+                energy=res["traj_energy"][i:i + 1], step=res["traj_step"][i:i + 1],
+                iteration=res["traj_iteration"][i:i + 1], count=res["traj_count"][i:i + 1],
+            )  # fmt: skip
+        results.append(RelaxResult(
+            s=res["s"][off[i]:off[i + 1]].reshape(1, n, d), energy=res["energy"][i:i + 1],
+            grad_norm=res["grad_norm"][i:i + 1], n_evals=res["n_evals"][i:i + 1],
+            n_iters=res["n_iters"][i:i + 1], status=res["status"][i:i + 1], trajectory=traj,
+        ))  # fmt: skip
+    return results
