@@ -164,6 +164,8 @@ typedef struct {
                            lane's completion (%globaltimer), NULL to skip */
   int64_t ticks;        /* out: device ticks (one energy evaluation per running lane each) */
   int64_t launches;     /* out: kernel launches issued by the call */
+  int32_t branches;     /* out: graph branches of the tick schedule used */
+  int32_t graph_ticks;  /* out: ticks per captured graph of that schedule */
 } cco_relax_out;
 
 /*
@@ -200,6 +202,16 @@ int cco_relax_descent_mixed(cco_problem* const* problems, void* stream, int batc
 int cco_relax_lbfgs_mixed(cco_problem* const* problems, void* stream, int batch,
                           const double* s0, const cco_lbfgs_settings* settings,
                           int chunk_iters, cco_relax_out* out);
+
+/*
+ * Tick schedules (graph branches, ticks per graph) are tuned online on the
+ * first relaxation of each shape class (minimizer, lane count and total
+ * N M bucketed by powers of two, largest d) and cached for the process;
+ * results never depend on the schedule. This forgets every cached schedule.
+ * The environment variables CCO_BRANCHES and CCO_GRAPH_TICKS force a
+ * schedule, CCO_AUTOTUNE=0 keeps the default (2 branches, 16 ticks).
+ */
+int cco_schedule_reset(void);
 
 #ifdef __cplusplus
 }

@@ -9,14 +9,20 @@
 #include <string>
 #include <vector>
 
+#include "cco_host.cuh"
 #include "cco_internal.cuh"
 #include "cco_opt.cuh"
 
 using namespace cco;
 
 namespace {
-
 thread_local std::string g_last_error;
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxPoolDevices] = {};
+}  // namespace
+
+namespace cco {
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -33,20 +39,9 @@ int cuda_fail(cudaError_t e, const char* what) {
   return fail(CCO_ERR_DEVICE, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define CCO_CUDA(call)                                 \
-  do {                                                 \
-    cudaError_t e_ = (call);                           \
-    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
-  } while (0)
-
-// Stream-ordered allocations come from one memory pool per device that keeps
-// its memory (release threshold = max): a relaxation's ~GB of lane state is
-// reused by the next call instead of being unmapped at every synchronize, as
-// the default pool (threshold 0) would do.
-constexpr int kMaxPoolDevices = 64;
-std::mutex g_pool_mu;
-cudaMemPool_t g_pool[kMaxPoolDevices] = {};
-
+// One pool per device that keeps its memory (release threshold = max): a
+// relaxation's lane records are reused by the next call instead of being
+// unmapped at every synchronize, as the default pool (threshold 0) would do.
 cudaError_t device_pool(cudaMemPool_t* out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -71,40 +66,8 @@ cudaError_t device_pool(cudaMemPool_t* out) {
   return cudaSuccess;
 }
 
-template <class T>
-cudaError_t pool_alloc(T** ptr, size_t bytes, cudaStream_t st) {
-  cudaMemPool_t pool;
-  const cudaError_t e = device_pool(&pool);
-  if (e != cudaSuccess) return e;
-  return cudaMallocFromPoolAsync(reinterpret_cast<void**>(ptr), bytes, pool, st);
-}
+}  // namespace cco
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
-
-}  // namespace
-
-struct cco_problem {
-  int device = 0;
-  int d = 0, N = 0, M = 0;
-  ProbDev host{};         // pointers are device pointers
-  ProbDev* dev = nullptr; // device copy
-  SegHdr* seg1 = nullptr;
-  SegHdr* seg2 = nullptr;
-  double* w_run = nullptr;
-  int* run2ref = nullptr;
-  size_t smem1 = 0, smem2 = 0;
-};
 
 namespace {
 
@@ -564,574 +527,3 @@ extern "C" int cco_energy_grad_noalloc(cco_problem* p, void* stream, int batch, 
   return CCO_OK;
 }
 
-// ------------------------------------------------------------ relax drivers
-namespace {
-
-// Runs ticks (one evaluation + one update per running lane) in captured CUDA
-// graphs of kGraphTicks ticks until no lane is RUNNING or the tick bound is
-// reached. The lanes are split into `nbr` independent branches of the graph:
-// a branch's FP64-bound evaluation overlaps another branch's HBM-bound
-// minimizer update on the device. Completion is checked kInflight graphs
-// behind, so host or driver hiccups (a clock sampler, a busy CPU) do not
-// leave the device idle; lanes already finished make the surplus graphs
-// near-empty launches.
-constexpr int kGraphTicks = 16;
-constexpr int kInflight = 3;
-constexpr int kMaxBranches = 4;
-
-int branch_count(int B) {
-  int nbr = 2;
-  if (const char* env = getenv("CCO_BRANCHES")) nbr = atoi(env);
-  nbr = std::max(1, std::min(nbr, kMaxBranches));
-  while (nbr > 1 && B / nbr < 32) --nbr;
-  return nbr;
-}
-
-template <class TickFn>
-int run_ticks(cudaStream_t st, int nbr, TickFn tick, const int64_t* status, size_t stride, int B,
-              int64_t max_ticks, int64_t* ticks_out) {
-  constexpr int kSlots = kInflight + 1;
-  int* d_count = nullptr;
-  // pinned completion counters: allocated once per host thread (cudaMallocHost
-  // is slow and may synchronize, so it stays out of every call)
-  static thread_local int* h_count = nullptr;
-  CCO_CUDA(pool_alloc(&d_count, kSlots * sizeof(int), st));
-  if (h_count == nullptr) CCO_CUDA(cudaMallocHost(&h_count, kSlots * sizeof(int)));
-  cudaEvent_t ev[kSlots];
-  for (int i = 0; i < kSlots; ++i) CCO_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  int rc = CCO_OK;
-  // capture kGraphTicks ticks of every branch; branches fork from and join
-  // back into the first capture stream
-  cudaStream_t cap[kMaxBranches];
-  cudaEvent_t fork, join[kMaxBranches];
-  for (int b = 0; b < nbr; ++b) CCO_CUDA(cudaStreamCreateWithFlags(&cap[b], cudaStreamNonBlocking));
-  CCO_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-  for (int b = 0; b < nbr; ++b) CCO_CUDA(cudaEventCreateWithFlags(&join[b], cudaEventDisableTiming));
-  cudaError_t e = cudaStreamBeginCapture(cap[0], cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    e = cudaEventRecord(fork, cap[0]);
-    for (int b = 1; b < nbr && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(cap[b], fork, 0);
-    for (int t = 0; t < kGraphTicks && e == cudaSuccess; ++t)
-      for (int b = 0; b < nbr && e == cudaSuccess; ++b) e = tick(cap[b], b);
-    for (int b = 1; b < nbr && e == cudaSuccess; ++b) {
-      e = cudaEventRecord(join[b], cap[b]);
-      if (e == cudaSuccess) e = cudaStreamWaitEvent(cap[0], join[b], 0);
-    }
-    cudaError_t e2 = cudaStreamEndCapture(cap[0], &graph);
-    if (e == cudaSuccess) e = e2;
-  }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-  int64_t ticks = 0;
-  int launched = 0, checked = 0;
-  bool done = false;
-  while (e == cudaSuccess && !done) {
-    if (ticks >= max_ticks) break;
-    e = cudaGraphLaunch(exec, st);
-    if (e != cudaSuccess) break;
-    ticks += kGraphTicks;
-    const int slot = launched % kSlots;
-    e = count_running(status, stride, B, d_count + slot, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_count + slot, d_count + slot, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[slot], st);
-    ++launched;
-    if (e == cudaSuccess && launched - checked > kInflight) {
-      const int old = checked % kSlots;
-      e = cudaEventSynchronize(ev[old]);
-      ++checked;
-      if (e == cudaSuccess && h_count[old] == 0) done = true;
-    }
-  }
-  // drain the launches still in flight, oldest first
-  while (e == cudaSuccess && !done && checked < launched) {
-    const int old = checked % kSlots;
-    e = cudaEventSynchronize(ev[old]);
-    ++checked;
-    if (e == cudaSuccess && h_count[old] == 0) done = true;
-  }
-  if (e != cudaSuccess) rc = cuda_fail(e, "relax ticks");
-  else if (!done) rc = fail(CCO_ERR_ROUNDS, "relax did not finish within the round bound (%lld ticks)", (long long)max_ticks);
-  if (exec) cudaGraphExecDestroy(exec);
-  if (graph) cudaGraphDestroy(graph);
-  for (int b = 0; b < nbr; ++b) {
-    cudaStreamDestroy(cap[b]);
-    cudaEventDestroy(join[b]);
-  }
-  cudaEventDestroy(fork);
-  for (int i = 0; i < kSlots; ++i) cudaEventDestroy(ev[i]);
-  cudaFreeAsync(d_count, st);
-  cudaStreamSynchronize(st);
-  if (ticks_out) *ticks_out = ticks;
-  return rc;
-}
-
-// Lanes of one relaxation: each lane has its own problem (mixed N, d and
-// k-set) or all lanes share one. Positions are packed in the caller's
-// buffers (soff, N_i d_i each); the device lane vectors use padded lengths
-// (voff, ld_i).
-struct LaneSet {
-  int B = 0, device = 0;
-  std::vector<const cco_problem*> prob;   // [B]
-  std::vector<int> nd, ld;                 // [B]
-  std::vector<int64_t> soff, voff;         // [B]
-  int64_t s_total = 0, v_total = 0;
-  int max_ld = 0;
-  std::vector<const cco_problem*> uniq;    // distinct problems
-  std::vector<int> pidx;                   // [B] index into uniq
-};
-
-int make_laneset(cco_problem* const* probs, int B, int pad, LaneSet* L) {
-  if (B < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
-  L->B = B;
-  L->prob.resize(B);
-  L->nd.resize(B);
-  L->ld.resize(B);
-  L->soff.resize(B);
-  L->voff.resize(B);
-  L->pidx.resize(B);
-  for (int i = 0; i < B; ++i) {
-    const cco_problem* p = probs[i];
-    if (!p) return fail(CCO_ERR_ARG, "null problem for lane %d", i);
-    if (i == 0) L->device = p->device;
-    if (p->device != L->device) return fail(CCO_ERR_ARG, "lanes must share one device");
-    const int nd = p->N * p->d;
-    const int ld = (nd + pad - 1) / pad * pad;
-    L->prob[i] = p;
-    L->nd[i] = nd;
-    L->ld[i] = ld;
-    L->soff[i] = L->s_total;
-    L->voff[i] = L->v_total;
-    L->s_total += nd;
-    L->v_total += ld;
-    L->max_ld = std::max(L->max_ld, ld);
-    int u = 0;
-    while (u < (int)L->uniq.size() && L->uniq[u] != p) ++u;
-    if (u == (int)L->uniq.size()) L->uniq.push_back(p);
-    L->pidx[i] = u;
-  }
-  return CCO_OK;
-}
-
-template <class T>
-cudaError_t upload(T** dst, const std::vector<T>& src, cudaStream_t st) {
-  cudaError_t e = pool_alloc(dst, sizeof(T) * std::max<size_t>(src.size(), 1), st);
-  if (e == cudaSuccess && !src.empty())
-    e = cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, st);
-  return e;
-}
-
-// Evaluation plan of lanes [lo, hi) of a lane set, built on the host.
-struct EvalSet {
-  ProbDev* probs = nullptr;
-  EvalLane* lanes = nullptr;
-  EvalItem* it1 = nullptr;
-  EvalItem* it2 = nullptr;
-  double2* dens = nullptr;   // rho, w rho and the pass-1 partials of every lane
-  EvalPlan plan{};
-
-  cudaError_t build(const LaneSet& L, int lo, int hi, double* s_base, double* f_base,
-                    double* g_base, const int64_t* status_base, size_t status_stride,
-                    cudaStream_t st) {
-    std::vector<ProbDev> pv;
-    size_t smem1 = 0, smem2 = 0;
-    int max_d = 1;
-    for (const cco_problem* p : L.uniq) {
-      pv.push_back(p->host);
-      smem1 = std::max(smem1, p->smem1);
-      smem2 = std::max(smem2, p->smem2);
-      max_d = std::max(max_d, p->d);
-    }
-    size_t dn = 0;
-    for (int i = lo; i < hi; ++i) dn += (size_t)L.prob[i]->M * (2 + L.prob[i]->host.ntile1);
-    cudaError_t e = pool_alloc(&dens, sizeof(double2) * std::max<size_t>(dn, 1), st);
-    std::vector<EvalLane> lv;
-    std::vector<EvalItem> i1, i2;
-    size_t o = 0;
-    for (int i = lo; i < hi; ++i) {
-      const cco_problem* p = L.prob[i];
-      const size_t M = p->M;
-      EvalLane ln{};
-      ln.s = s_base + L.voff[i];
-      ln.f = f_base + i;
-      ln.g = g_base ? g_base + L.voff[i] : nullptr;
-      ln.rho = dens + o;
-      ln.rhow = dens + o + M;
-      ln.part = dens + o + 2 * M;
-      o += M * (2 + p->host.ntile1);
-      ln.status = status_base ? status_base + (size_t)i * status_stride : nullptr;
-      ln.prob = L.pidx[i];
-      const int j = i - lo;
-      for (int t = 0; t < p->host.ntile1; ++t) i1.push_back(EvalItem{j, t});
-      for (int t = 0; t < p->host.ntile2; ++t) i2.push_back(EvalItem{j, t});
-      lv.push_back(ln);
-    }
-    if (e == cudaSuccess) e = upload(&probs, pv, st);
-    if (e == cudaSuccess) e = upload(&lanes, lv, st);
-    if (e == cudaSuccess) e = upload(&it1, i1, st);
-    if (e == cudaSuccess) e = upload(&it2, i2, st);
-    plan.probs = probs;
-    plan.lanes = lanes;
-    plan.items1 = it1;
-    plan.items2 = it2;
-    plan.n_lanes = hi - lo;
-    plan.n_items1 = (int)i1.size();
-    plan.n_items2 = (int)i2.size();
-    plan.max_d = max_d;
-    plan.smem1 = smem1;
-    plan.smem2 = smem2;
-    plan.want_grad = g_base != nullptr;
-    return e;
-  }
-  void release(cudaStream_t st) {
-    cudaFreeAsync(probs, st);
-    cudaFreeAsync(lanes, st);
-    cudaFreeAsync(it1, st);
-    cudaFreeAsync(it2, st);
-    cudaFreeAsync(dens, st);
-  }
-};
-
-bool out_ok(const cco_relax_out* o) {
-  return o && o->s && o->energy && o->grad_norm && o->n_evals && o->n_iters && o->status;
-}
-
-// Device copies of the lane layout arrays (offsets and lengths).
-struct LaneArrays {
-  int64_t *voff = nullptr, *soff = nullptr, *toff = nullptr, *hoff = nullptr;
-  int *lnd = nullptr, *lld = nullptr;
-  cudaError_t build(const LaneSet& L, int64_t cap, int m, cudaStream_t st) {
-    std::vector<int64_t> th(L.B), hh(L.B);
-    int64_t t = 0, h = 0;
-    for (int i = 0; i < L.B; ++i) {
-      th[i] = t;
-      hh[i] = h;
-      t += cap * L.nd[i];
-      h += (int64_t)m * L.ld[i];
-    }
-    cudaError_t e = upload(&voff, L.voff, st);
-    if (e == cudaSuccess) e = upload(&soff, L.soff, st);
-    if (e == cudaSuccess) e = upload(&toff, th, st);
-    if (e == cudaSuccess) e = upload(&hoff, hh, st);
-    if (e == cudaSuccess) e = upload(&lnd, L.nd, st);
-    if (e == cudaSuccess) e = upload(&lld, L.ld, st);
-    return e;
-  }
-  int64_t hist_total(const LaneSet& L, int m) const {
-    int64_t h = 0;
-    for (int i = 0; i < L.B; ++i) h += (int64_t)m * L.ld[i];
-    return h;
-  }
-  void release(cudaStream_t st) {
-    cudaFreeAsync(voff, st);
-    cudaFreeAsync(soff, st);
-    cudaFreeAsync(toff, st);
-    cudaFreeAsync(hoff, st);
-    cudaFreeAsync(lnd, st);
-    cudaFreeAsync(lld, st);
-  }
-};
-
-int check_traj(const cco_relax_out* out, bool rec) {
-  if (rec && (!out->traj_s || !out->traj_energy || !out->traj_step || !out->traj_iteration ||
-              !out->traj_count))
-    return fail(CCO_ERR_ARG, "trajectory recording needs the traj_* outputs");
-  return CCO_OK;
-}
-
-int relax_descent_set(const LaneSet& L, cudaStream_t st, const double* s0,
-                      const cco_descent_settings* cfg, cco_relax_out* out) {
-  if (!cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
-  if (!out_ok(out)) return fail(CCO_ERR_ARG, "incomplete output struct");
-  if (cfg->max_evals < 0) return fail(CCO_ERR_ARG, "max_evals must be >= 0");
-  const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
-  if (check_traj(out, rec) != CCO_OK) return CCO_ERR_ARG;
-  DeviceGuard guard(L.device);
-  const int B = L.B;
-  const size_t V = L.v_total;
-  DescentArgs a{};
-  a.B = B;
-  a.step_init = cfg->step_init;
-  a.step_min = cfg->step_min;
-  a.shrink = cfg->shrink;
-  a.grow = cfg->grow;
-  a.rel_tol = cfg->rel_tol;
-  a.energy_tol = cfg->energy_tol;
-  a.max_iters = cfg->max_evals / 2;
-  a.rec_every = rec ? cfg->record_every : 1;
-  a.rec_cap = rec ? cfg->max_records : 0;
-  LaneArrays la;
-  CCO_CUDA(la.build(L, a.rec_cap, 0, st));
-  a.voff = la.voff;
-  a.soff = la.soff;
-  a.toff = la.toff;
-  a.lnd = la.lnd;
-  double* vec = nullptr;   // s, g, ps, pg
-  double* sc = nullptr;    // f, step, norm, pf
-  int64_t* ic = nullptr;   // it, n_evals, status, t0, t1
-  int* ph = nullptr;       // phase, nonzero
-  CCO_CUDA(pool_alloc(&vec, sizeof(double) * V * 4, st));
-  CCO_CUDA(pool_alloc(&sc, sizeof(double) * B * 4, st));
-  CCO_CUDA(pool_alloc(&ic, sizeof(int64_t) * B * 5, st));
-  CCO_CUDA(pool_alloc(&ph, sizeof(int) * B * 2, st));
-  a.s = vec;
-  a.g = vec + V;
-  a.ps = vec + 2 * V;
-  double* pg = vec + 3 * V;
-  a.pg = pg;
-  a.f = sc;
-  a.step = sc + B;
-  a.norm = sc + 2 * B;
-  double* pf = sc + 3 * B;
-  a.pf = pf;
-  a.it = ic;
-  a.n_evals = ic + B;
-  a.status = ic + 2 * B;
-  a.t0 = ic + 3 * B;
-  a.t1 = ic + 4 * B;
-  a.phase = ph;
-  a.nonzero = ph + B;
-  if (rec) {
-    a.traj_s = out->traj_s;
-    a.traj_e = out->traj_energy;
-    a.traj_step = out->traj_step;
-    a.traj_it = out->traj_iteration;
-    a.traj_count = out->traj_count;
-  }
-  const int nbr = branch_count(B);
-  EvalSet ws[kMaxBranches];
-  DescentArgs ab[kMaxBranches];
-  for (int b = 0; b < nbr; ++b) {
-    const int lo = b * B / nbr, hi = (b + 1) * B / nbr;
-    DescentArgs r = a;
-    r.B = hi - lo;
-    r.voff += lo; r.soff += lo; r.toff += lo; r.lnd += lo;
-    r.pf += lo; r.f += lo; r.step += lo; r.norm += lo;
-    r.it += lo; r.n_evals += lo; r.status += lo; r.phase += lo; r.nonzero += lo;
-    r.t0 += lo; r.t1 += lo;
-    if (rec) {
-      r.traj_e += (size_t)lo * a.rec_cap;
-      r.traj_step += (size_t)lo * a.rec_cap;
-      r.traj_it += (size_t)lo * a.rec_cap;
-      r.traj_count += lo;
-    }
-    ab[b] = r;
-    CCO_CUDA(ws[b].build(L, lo, hi, a.ps, pf, pg, a.status, 1, st));
-  }
-  CCO_CUDA(descent_init(a, s0, st));
-  auto tick = [&](cudaStream_t s, int b) -> cudaError_t {
-    cudaError_t e = eval_launch(ws[b].plan, s);
-    if (e == cudaSuccess) e = descent_update(ab[b], s);
-    return e;
-  };
-  const int64_t max_ticks = 1 + a.max_iters + (kInflight + 1) * kGraphTicks;
-  int64_t ticks = 0;
-  int rc = run_ticks(st, nbr, tick, a.status, 1, B, max_ticks, &ticks);
-  if (rc == CCO_OK) {
-    cudaError_t e = descent_finalize(a, out->s, out->energy, out->grad_norm, out->n_evals,
-                                     out->n_iters, out->status, out->latency_ns, st);
-    if (e != cudaSuccess) rc = cuda_fail(e, "descent_finalize");
-  }
-  out->ticks = ticks;
-  out->launches = ticks * 4 * nbr + ticks / kGraphTicks + 2;
-  for (int b = 0; b < nbr; ++b) ws[b].release(st);
-  la.release(st);
-  cudaFreeAsync(vec, st);
-  cudaFreeAsync(sc, st);
-  cudaFreeAsync(ic, st);
-  cudaFreeAsync(ph, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "relax descent");
-  return rc;
-}
-
-int relax_lbfgs_set(const LaneSet& L, cudaStream_t st, const double* s0,
-                    const cco_lbfgs_settings* cfg, cco_relax_out* out) {
-  if (!cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
-  if (!out_ok(out)) return fail(CCO_ERR_ARG, "incomplete output struct");
-  if (cfg->n_rescales < 1 || cfg->n_rescales > CCO_MAX_RESCALES)
-    return fail(CCO_ERR_ARG, "need 1..%d rescale passes", CCO_MAX_RESCALES);
-  if (cfg->memory < 1) return fail(CCO_ERR_ARG, "memory must be >= 1");
-  if (cfg->memory > 256) return fail(CCO_ERR_ARG, "memory must be <= 256 on this build");
-  if (cfg->max_linesearch_steps < 1) return fail(CCO_ERR_ARG, "max_linesearch_steps must be >= 1");
-  const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
-  if (check_traj(out, rec) != CCO_OK) return CCO_ERR_ARG;
-  DeviceGuard guard(L.device);
-  const int B = L.B;
-  const size_t V = L.v_total;
-  const int m = (int)cfg->memory;
-  LbArgs A{};
-  A.B = B;
-  A.m = m;
-  A.n_pass = cfg->n_rescales;
-  for (int i = 0; i < CCO_MAX_RESCALES; ++i) A.rescales[i] = i < cfg->n_rescales ? cfg->rescales[i] : 1.0;
-  A.energy_tol = cfg->energy_tol;
-  A.grad_tol = cfg->grad_tol;
-  A.budget = cfg->max_evals_per_pass;
-  A.patience = cfg->stagnation_patience;
-  A.max_ls = cfg->max_linesearch_steps;
-  A.rec_every = rec ? cfg->record_every : 1;
-  A.rec_cap = rec ? cfg->max_records : 0;
-  const size_t tri_bytes = lbfgs_update_smem(m);
-  const bool in_smem = tri_bytes <= 200 * 1024;
-  A.smem_tri = in_smem ? tri_bytes : 0;
-  if (in_smem) {
-    static std::mutex mu;
-    static size_t configured = 0;
-    std::lock_guard<std::mutex> lk(mu);
-    if (tri_bytes > configured) {
-      CCO_CUDA(lbfgs_configure(200 * 1024));
-      configured = 200 * 1024;
-    }
-  }
-  LaneArrays la;
-  CCO_CUDA(la.build(L, A.rec_cap, m, st));
-  A.voff = la.voff;
-  A.soff = la.soff;
-  A.toff = la.toff;
-  A.hoff = la.hoff;
-  A.lnd = la.lnd;
-  A.lld = la.lld;
-  const size_t H = la.hist_total(L, m);
-  LbState* stv = nullptr;
-  double* vec = nullptr;   // x, s, g, dir, glo, ps, pg
-  double* hist = nullptr;  // S, Y
-  double* dots = nullptr;  // SY, YY
-  double* pf = nullptr;
-  double* trig = nullptr;
-  double* scal = nullptr;
-  CCO_CUDA(pool_alloc(&stv, sizeof(LbState) * B, st));
-  CCO_CUDA(pool_alloc(&vec, sizeof(double) * V * 7, st));
-  CCO_CUDA(cudaMemsetAsync(vec, 0, sizeof(double) * V * 7, st));
-  CCO_CUDA(pool_alloc(&hist, sizeof(double) * H * 2, st));
-  CCO_CUDA(pool_alloc(&dots, sizeof(double) * (size_t)B * m * m * 2, st));
-  CCO_CUDA(pool_alloc(&pf, sizeof(double) * B, st));
-  if (!in_smem) CCO_CUDA(pool_alloc(&trig, tri_bytes * B, st));
-  A.nblkB = (int)((L.max_ld / 2 + 255) / 256);
-  A.scal_stride = (4 * m + 1 + A.nblkB + 1) & ~1;
-  CCO_CUDA(pool_alloc(&scal, sizeof(double) * (size_t)A.scal_stride * B, st));
-  A.scal = scal;
-  A.st = stv;
-  A.x = vec;
-  A.s = vec + V;
-  A.g = vec + 2 * V;
-  A.dir = vec + 3 * V;
-  A.glo = vec + 4 * V;
-  A.ps = vec + 5 * V;
-  double* pg = vec + 6 * V;
-  A.pg = pg;
-  A.pf = pf;
-  A.Sh = hist;
-  A.Yh = hist + H;
-  A.SYs = dots;
-  A.YYs = dots + (size_t)B * m * m;
-  A.tri_g = trig;
-  if (rec) {
-    A.traj_s = out->traj_s;
-    A.traj_e = out->traj_energy;
-    A.traj_step = out->traj_step;
-    A.traj_it = out->traj_iteration;
-    A.traj_count = out->traj_count;
-  }
-  const size_t st_stride = sizeof(LbState) / sizeof(int64_t);
-  const int64_t* status0 = &stv->status;
-  const int nbr = branch_count(B);
-  EvalSet ws[kMaxBranches];
-  LbArgs Ab[kMaxBranches];
-  for (int b = 0; b < nbr; ++b) {
-    const int lo = b * B / nbr, hi = (b + 1) * B / nbr;
-    LbArgs r = A;
-    r.B = hi - lo;
-    r.st += lo;
-    r.pf += lo;
-    r.voff += lo; r.soff += lo; r.toff += lo; r.hoff += lo; r.lnd += lo; r.lld += lo;
-    r.SYs += (size_t)lo * m * m;
-    r.YYs += (size_t)lo * m * m;
-    if (r.tri_g) r.tri_g += (size_t)lo * ((size_t)m * (m + 1));
-    r.scal += (size_t)lo * A.scal_stride;
-    if (rec) {
-      r.traj_e += (size_t)lo * A.rec_cap;
-      r.traj_step += (size_t)lo * A.rec_cap;
-      r.traj_it += (size_t)lo * A.rec_cap;
-      r.traj_count += lo;
-    }
-    Ab[b] = r;
-    CCO_CUDA(ws[b].build(L, lo, hi, A.ps, pf, pg, status0, st_stride, st));
-  }
-  CCO_CUDA(lbfgs_init(A, s0, st));
-  auto tick = [&](cudaStream_t s, int b) -> cudaError_t {
-    cudaError_t e = eval_launch(ws[b].plan, s);
-    if (e == cudaSuccess) e = lbfgs_update(Ab[b], s);
-    return e;
-  };
-  const int64_t max_ticks =
-      1 + (int64_t)cfg->n_rescales * (cfg->max_evals_per_pass + cfg->max_linesearch_steps + 1) +
-      (kInflight + 1) * kGraphTicks;
-  int64_t ticks = 0;
-  int rc = run_ticks(st, nbr, tick, status0, st_stride, B, max_ticks, &ticks);
-  if (rc == CCO_OK) {
-    cudaError_t e = lbfgs_finalize(A, out->s, out->energy, out->grad_norm, out->n_evals,
-                                   out->n_iters, out->status, out->latency_ns, st);
-    if (e != cudaSuccess) rc = cuda_fail(e, "lbfgs_finalize");
-  }
-  out->ticks = ticks;
-  out->launches = ticks * 7 * nbr + ticks / kGraphTicks + 2;
-  for (int b = 0; b < nbr; ++b) ws[b].release(st);
-  la.release(st);
-  cudaFreeAsync(stv, st);
-  cudaFreeAsync(vec, st);
-  cudaFreeAsync(hist, st);
-  cudaFreeAsync(dots, st);
-  cudaFreeAsync(pf, st);
-  if (trig) cudaFreeAsync(trig, st);
-  cudaFreeAsync(scal, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "relax lbfgs");
-  return rc;
-}
-
-}  // namespace
-
-extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const double* s0,
-                                 const cco_descent_settings* cfg, int chunk_iters,
-                                 cco_relax_out* out) {
-  if (!p) return fail(CCO_ERR_ARG, "null problem");
-  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
-  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
-  std::vector<cco_problem*> probs(batch, p);
-  LaneSet L;
-  if (make_laneset(probs.data(), batch, 1, &L) != CCO_OK) return CCO_ERR_ARG;
-  return relax_descent_set(L, (cudaStream_t)stream, s0, cfg, out);
-}
-
-extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const double* s0,
-                               const cco_lbfgs_settings* cfg, int chunk_iters,
-                               cco_relax_out* out) {
-  if (!p) return fail(CCO_ERR_ARG, "null problem");
-  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
-  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
-  std::vector<cco_problem*> probs(batch, p);
-  LaneSet L;
-  if (make_laneset(probs.data(), batch, 4, &L) != CCO_OK) return CCO_ERR_ARG;
-  return relax_lbfgs_set(L, (cudaStream_t)stream, s0, cfg, out);
-}
-
-extern "C" int cco_relax_descent_mixed(cco_problem* const* problems, void* stream, int batch,
-                                       const double* s0, const cco_descent_settings* cfg,
-                                       int chunk_iters, cco_relax_out* out) {
-  if (!problems) return fail(CCO_ERR_ARG, "null problem array");
-  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
-  LaneSet L;
-  if (make_laneset(problems, batch, 1, &L) != CCO_OK) return CCO_ERR_ARG;
-  return relax_descent_set(L, (cudaStream_t)stream, s0, cfg, out);
-}
-
-extern "C" int cco_relax_lbfgs_mixed(cco_problem* const* problems, void* stream, int batch,
-                                     const double* s0, const cco_lbfgs_settings* cfg,
-                                     int chunk_iters, cco_relax_out* out) {
-  if (!problems) return fail(CCO_ERR_ARG, "null problem array");
-  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
-  LaneSet L;
-  if (make_laneset(problems, batch, 4, &L) != CCO_OK) return CCO_ERR_ARG;
-  return relax_lbfgs_set(L, (cudaStream_t)stream, s0, cfg, out);
-}

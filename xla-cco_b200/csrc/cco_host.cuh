@@ -1,0 +1,251 @@
+// Host-side internals shared by the C-ABI translation units: error reporting,
+// the per-device memory pool, the problem object and the lane-set runtime
+// (lane records, evaluation plans, the CUDA-graph tick driver) that both the
+// one-shot relaxations and the serving pool run on.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "cco.h"
+#include "cco_internal.cuh"
+#include "cco_opt.cuh"
+
+struct cco_problem {
+  int device = 0;
+  int d = 0, N = 0, M = 0;
+  cco::ProbDev host{};         // pointers are device pointers
+  cco::ProbDev* dev = nullptr; // device copy
+  cco::SegHdr* seg1 = nullptr;
+  cco::SegHdr* seg2 = nullptr;
+  double* w_run = nullptr;
+  int* run2ref = nullptr;
+  size_t smem1 = 0, smem2 = 0;
+};
+
+namespace cco {
+
+// Records the message for cco_last_error and returns `code`.
+int fail(int code, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define CCO_CUDA(call)                                       \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return ::cco::cuda_fail(e_, #call); \
+  } while (0)
+
+// Stream-ordered allocations come from one memory pool per device that keeps
+// its memory (release threshold = max).
+cudaError_t device_pool(cudaMemPool_t* out);
+
+template <class T>
+cudaError_t pool_alloc(T** ptr, size_t bytes, cudaStream_t st) {
+  cudaMemPool_t pool;
+  const cudaError_t e = device_pool(&pool);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(reinterpret_cast<void**>(ptr), bytes, pool, st);
+}
+
+template <class T>
+cudaError_t upload(T** dst, const std::vector<T>& src, cudaStream_t st) {
+  cudaError_t e = pool_alloc(dst, sizeof(T) * std::max<size_t>(src.size(), 1), st);
+  if (e == cudaSuccess && !src.empty())
+    e = cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, st);
+  return e;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// ------------------------------------------------------------ lane records
+enum class Method { Descent, Lbfgs };
+
+// What every record of one launch shares: the minimizer and, for L-BFGS,
+// the memory m and whether the scalar kernel's triangles live in the record.
+struct RecordShape {
+  Method method = Method::Lbfgs;
+  int m = 0, tri_len = 0;
+};
+
+inline size_t record_doubles(const RecordShape& R, const cco_problem* p) {
+  const int ld = pad4(p->N * p->d);
+  const size_t n = R.method == Method::Descent
+                       ? ds_record_doubles(ld, p->M, p->host.ntile1)
+                       : lb_record_doubles(R.m, R.tri_len, ld, p->M, p->host.ntile1);
+  return (n + 31) & ~(size_t)31;   // records start on 256-byte boundaries
+}
+
+inline size_t record_bytes(const RecordShape& R, const cco_problem* p) {
+  return record_doubles(R, p) * sizeof(double);
+}
+
+// Evaluation view of a lane record: probe positions in, energy, gradient and
+// densities out, status read by the evaluation kernels.
+inline EvalLane eval_lane(const RecordShape& R, const LaneRef& L, const cco_problem* p,
+                          int prob_index) {
+  EvalLane e{};
+  double2* dens;
+  if (R.method == Method::Descent) {
+    const DsView v = ds_view(L.rec, L.ld);
+    e.s = v.ps;
+    e.g = v.pg;
+    e.f = v.pf;
+    dens = v.dens;
+  } else {
+    const LbView v = lb_view(L.rec, R.m, R.tri_len, L.ld);
+    e.s = v.ps;
+    e.g = v.pg;
+    e.f = v.pf;
+    dens = v.dens;
+  }
+  e.rho = dens;
+  e.rhow = dens + p->M;
+  e.part = dens + 2 * (size_t)p->M;
+  e.status = rec_status(L.rec);
+  e.prob = prob_index;
+  e.pad_ = 0;
+  return e;
+}
+
+// Evaluation plan of a list of lanes, built on the host and uploaded.
+struct EvalSet {
+  ProbDev* probs = nullptr;
+  EvalLane* lanes = nullptr;
+  EvalItem* it1 = nullptr;
+  EvalItem* it2 = nullptr;
+  EvalPlan plan{};
+
+  cudaError_t build(const RecordShape& R, const std::vector<LaneRef>& refs,
+                    const std::vector<const cco_problem*>& probs_of, int lo, int hi,
+                    cudaStream_t st) {
+    std::vector<const cco_problem*> uniq;
+    std::vector<ProbDev> pv;
+    std::vector<EvalLane> lv;
+    std::vector<EvalItem> i1, i2;
+    size_t smem1 = 0, smem2 = 0;
+    int max_d = 1;
+    for (int i = lo; i < hi; ++i) {
+      const cco_problem* p = probs_of[i];
+      int u = 0;
+      while (u < (int)uniq.size() && uniq[u] != p) ++u;
+      if (u == (int)uniq.size()) {
+        uniq.push_back(p);
+        pv.push_back(p->host);
+        smem1 = std::max(smem1, p->smem1);
+        smem2 = std::max(smem2, p->smem2);
+        max_d = std::max(max_d, p->d);
+      }
+      const int j = i - lo;
+      lv.push_back(eval_lane(R, refs[i], p, u));
+      for (int t = 0; t < p->host.ntile1; ++t) i1.push_back(EvalItem{j, t});
+      for (int t = 0; t < p->host.ntile2; ++t) i2.push_back(EvalItem{j, t});
+    }
+    cudaError_t e = upload(&probs, pv, st);
+    if (e == cudaSuccess) e = upload(&lanes, lv, st);
+    if (e == cudaSuccess) e = upload(&it1, i1, st);
+    if (e == cudaSuccess) e = upload(&it2, i2, st);
+    plan.probs = probs;
+    plan.lanes = lanes;
+    plan.items1 = it1;
+    plan.items2 = it2;
+    plan.n_lanes = hi - lo;
+    plan.n_items1 = (int)i1.size();
+    plan.n_items2 = (int)i2.size();
+    plan.max_d = max_d;
+    plan.smem1 = smem1;
+    plan.smem2 = smem2;
+    plan.want_grad = true;
+    return e;
+  }
+  void release(cudaStream_t st) {
+    if (probs) cudaFreeAsync(probs, st);
+    if (lanes) cudaFreeAsync(lanes, st);
+    if (it1) cudaFreeAsync(it1, st);
+    if (it2) cudaFreeAsync(it2, st);
+    probs = nullptr;
+    lanes = nullptr;
+    it1 = it2 = nullptr;
+  }
+};
+
+// ------------------------------------------------------------ tick schedule
+// A tick evaluates every RUNNING lane once and runs its minimizer update.
+// Ticks are captured into CUDA graphs of `graph_ticks` ticks, with the lanes
+// split into `branches` independent graph branches so that one branch's
+// FP64-bound evaluation overlaps another branch's HBM-bound update.
+struct Schedule {
+  int branches = 2;
+  int graph_ticks = 16;
+};
+constexpr int kMaxBranches = 4;
+constexpr int kInflight = 3;    // graphs in flight before the host checks completion
+
+// Lane ranges [bounds[b], bounds[b + 1]) of the branches, balanced by the
+// evaluation work (N M) of each lane.
+std::vector<int> branch_bounds(const std::vector<const cco_problem*>& probs, int nbr);
+
+// Tuned schedules, cached per shape class (minimizer, lane count and total
+// N M bucketed by powers of two, largest d).
+bool schedule_cached(const std::vector<const cco_problem*>& probs, Method method, Schedule* out);
+void schedule_store(const std::vector<const cco_problem*>& probs, Method method,
+                    const Schedule& s);
+void schedule_clear();
+
+// The lanes of one launch: their problems, records and the minimizer
+// arguments (lanes = d_refs, B = all lanes) that every branch slices.
+struct LaneTable {
+  RecordShape shape;
+  std::vector<const cco_problem*> probs;
+  std::vector<LaneRef> refs;
+  LaneRef* d_refs = nullptr;
+  DescentArgs ds{};
+  LbArgs lb{};
+  int upload_refs(cudaStream_t st);
+  void release(cudaStream_t st);
+};
+
+// One schedule of a lane table captured as an executable graph of
+// sch.graph_ticks ticks.
+struct TickPlan {
+  Method method = Method::Lbfgs;
+  Schedule sch;
+  int nbr = 1;
+  std::vector<int> bounds;
+  EvalSet ev[kMaxBranches];
+  DescentArgs ds[kMaxBranches];
+  LbArgs lb[kMaxBranches];
+  cudaGraphExec_t exec = nullptr;
+  int build(const LaneTable& T, const Schedule& sch, cudaStream_t st);
+  cudaError_t tick(cudaStream_t s, int b) const;
+  int launches_per_tick() const;
+  void release(cudaStream_t st);
+};
+
+struct RunStats {
+  int64_t ticks = 0, launches = 0;
+  Schedule schedule;
+};
+
+// Runs tick graphs until no lane of T is RUNNING (CCO_ERR_ROUNDS past
+// max_ticks). The schedule is forced by CCO_BRANCHES / CCO_GRAPH_TICKS,
+// cached for the shape class, or tuned online on the live lanes.
+int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* stats);
+
+// L-BFGS settings -> kernel arguments and record shape.
+int lbfgs_args(const cco_lbfgs_settings* cfg, LbArgs* A, RecordShape* shape);
+
+}  // namespace cco

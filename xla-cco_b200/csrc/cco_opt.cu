@@ -28,7 +28,6 @@ namespace cco {
 
 namespace {
 
-constexpr int kUpdThreads = 256;
 constexpr int kPassBMaxPairs = 512;  // direction coefficients staged in smem up to this
 constexpr int kScalarMaxPairs = 256; // L-BFGS memory supported by the scalar kernel
 
@@ -55,8 +54,8 @@ __device__ int descent_status(double f, bool nonzero, double step, int64_t it,
   return code;
 }
 
-__device__ void descent_record(const DescentArgs& a, int lane, int64_t it, const double* s,
-                               double f, double step) {
+__device__ void descent_record(const DescentArgs& a, int lane, const LaneRef& R, int64_t it,
+                               const double* s, double f, double step) {
   if (a.traj_count == nullptr) return;
   __shared__ int64_t row;
   if (threadIdx.x == 0) {
@@ -71,49 +70,47 @@ __device__ void descent_record(const DescentArgs& a, int lane, int64_t it, const
   }
   __syncthreads();
   if (row >= 0) {
-    const int nd = a.lnd[lane];
-    double* o = a.traj_s + a.toff[lane] + (size_t)row * nd;
-    for (int e = threadIdx.x; e < nd; e += blockDim.x) o[e] = wrap01(s[e]);
+    double* o = a.traj_s + R.toff + (size_t)row * R.nd;
+    for (int e = threadIdx.x; e < R.nd; e += blockDim.x) o[e] = wrap01(s[e]);
   }
 }
 
 __global__ void k_descent_init(DescentArgs a, const double* __restrict__ s0) {
   const int lane = blockIdx.x;
-  const size_t off = a.voff[lane], so = a.soff[lane];
-  const int nd = a.lnd[lane];
-  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-    const double v = s0[so + e];
-    a.ps[off + e] = v;
-    a.s[off + e] = v;
+  const LaneRef R = a.lanes[lane];
+  const DsView v = ds_view(R.rec, R.ld);
+  for (int e = threadIdx.x; e < R.ld; e += blockDim.x) {
+    const double x = e < R.nd ? s0[R.soff + e] : 0.0;
+    v.ps[e] = x;
+    v.s[e] = x;
+    v.g[e] = 0.0;
+    v.pg[e] = 0.0;
   }
   if (threadIdx.x == 0) {
-    a.phase[lane] = PH_INIT;
-    a.status[lane] = CCO_STATUS_RUNNING;
-    a.it[lane] = 0;
-    a.n_evals[lane] = 0;
-    a.step[lane] = a.step_init;
-    a.t0[lane] = gtimer();
-    a.t1[lane] = 0;
+    DsState S = {};
+    S.phase = PH_INIT;
+    S.status = CCO_STATUS_RUNNING;
+    S.step = a.step_init;
+    S.t0 = gtimer();
+    *v.st = S;
     if (a.traj_count) a.traj_count[lane] = 0;
   }
 }
 
 // Gradient norm and the exact all-zero test of the accepted gradient.
-__device__ void descent_norm(const DescentArgs& a, int lane, double* red) {
-  const double* g = a.g + a.voff[lane];
-  const int nd = a.lnd[lane];
+__device__ void descent_norm(const LaneRef& R, const DsView& v, double* red) {
   double ss = 0.0;
   int nz = 0;
-  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-    const double v = g[e];
-    ss += v * v;
-    nz |= (v != 0.0);
+  for (int e = threadIdx.x; e < R.nd; e += blockDim.x) {
+    const double x = v.g[e];
+    ss += x * x;
+    nz |= (x != 0.0);
   }
   ss = block_sum(ss, red);
   nz = __syncthreads_or(nz);
   if (threadIdx.x == 0) {
-    a.norm[lane] = sqrt(ss);
-    a.nonzero[lane] = nz;
+    v.st->norm = sqrt(ss);
+    v.st->nonzero = nz;
   }
 }
 
@@ -121,65 +118,63 @@ __global__ void __launch_bounds__(kUpdThreads) k_descent_update(DescentArgs a) {
   __shared__ double red[32];
   __shared__ int s_reject, s_status;
   const int lane = blockIdx.x;
-  if (a.status[lane] != CCO_STATUS_RUNNING) return;
-  const size_t off = a.voff[lane];
-  const int nd = a.lnd[lane];
-  double* s = a.s + off;
-  double* g = a.g + off;
-  double* ps = a.ps + off;
-  const double* pg = a.pg + off;
-  if (a.phase[lane] == PH_INIT) {
+  const LaneRef R = a.lanes[lane];
+  const DsView v = ds_view(R.rec, R.ld);
+  DsState* S = v.st;
+  if (S->status != CCO_STATUS_RUNNING) return;
+  const int nd = R.nd;
+  if (S->phase == PH_INIT) {
     // init_one (descent.py:121-141): one evaluation at s0, no iteration
-    for (int e = threadIdx.x; e < nd; e += blockDim.x) g[e] = pg[e];
-    descent_norm(a, lane, red);
+    for (int e = threadIdx.x; e < nd; e += blockDim.x) v.g[e] = v.pg[e];
+    descent_norm(R, v, red);
     __syncthreads();
     if (threadIdx.x == 0) {
-      a.f[lane] = a.pf[lane];
-      a.phase[lane] = PH_ITER;
-      s_status = descent_status(a.f[lane], a.nonzero[lane] != 0, a.step[lane], 0, a);
-      a.status[lane] = s_status;
-      if (s_status != CCO_STATUS_RUNNING) a.t1[lane] = gtimer();
+      S->f = *v.pf;
+      S->phase = PH_ITER;
+      s_status = descent_status(S->f, S->nonzero != 0, S->step, 0, a);
+      S->status = s_status;
+      if (s_status != CCO_STATUS_RUNNING) S->t1 = gtimer();
     }
     __syncthreads();
-    descent_record(a, lane, 0, s, a.f[lane], a.step[lane]);
+    descent_record(a, lane, R, 0, v.s, S->f, S->step);
   } else {
     // step_fn (descent.py:153-175) with the probe evaluated at xn
     if (threadIdx.x == 0) {
-      const double f = a.f[lane], f2 = a.pf[lane];
-      const double step = a.step[lane], norm = a.norm[lane];
+      const double f = S->f, f2 = *v.pf;
+      const double step = S->step, norm = S->norm;
       const double df = f - f2;
       const double df2 = step * norm;
       const bool reject = fabs(df - df2) / df2 > a.rel_tol;  // NaN accepts
-      a.step[lane] = reject ? step * a.shrink : step * a.grow;
-      if (!reject) a.f[lane] = f2;
-      a.it[lane] += 1;
-      a.n_evals[lane] += 2;
+      S->step = reject ? step * a.shrink : step * a.grow;
+      if (!reject) S->f = f2;
+      S->it += 1;
+      S->n_evals += 2;
       s_reject = reject;
     }
     __syncthreads();
     if (!s_reject) {
       for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-        s[e] = ps[e];
-        g[e] = pg[e];
+        v.s[e] = v.ps[e];
+        v.g[e] = v.pg[e];
       }
-      descent_norm(a, lane, red);
+      descent_norm(R, v, red);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      s_status = descent_status(a.f[lane], a.nonzero[lane] != 0, a.step[lane], a.it[lane], a);
-      a.status[lane] = s_status;
-      if (s_status != CCO_STATUS_RUNNING) a.t1[lane] = gtimer();
+      s_status = descent_status(S->f, S->nonzero != 0, S->step, S->it, a);
+      S->status = s_status;
+      if (s_status != CCO_STATUS_RUNNING) S->t1 = gtimer();
     }
     __syncthreads();
-    descent_record(a, lane, a.it[lane], s, a.f[lane], a.step[lane]);
+    descent_record(a, lane, R, S->it, v.s, S->f, S->step);
   }
   __syncthreads();
   if (s_status == CCO_STATUS_RUNNING) {
     // next probe: xn = s - (g / |g|) * step  (0 * g when |g| = 0)
-    const double norm = a.norm[lane], step = a.step[lane];
+    const double norm = S->norm, step = S->step;
     for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-      const double gn = norm > 0.0 ? __ddiv_rn(g[e], norm) : 0.0 * g[e];
-      ps[e] = __dsub_rn(s[e], __dmul_rn(gn, step));
+      const double gn = norm > 0.0 ? __ddiv_rn(v.g[e], norm) : 0.0 * v.g[e];
+      v.ps[e] = __dsub_rn(v.s[e], __dmul_rn(gn, step));
     }
   }
 }
@@ -189,22 +184,23 @@ __global__ void k_descent_finalize(DescentArgs a, double* s_out, double* e_out, 
                                    int64_t* lat_out) {
   __shared__ double red[32];
   const int lane = blockIdx.x;
-  const size_t off = a.voff[lane], so = a.soff[lane];
-  const int nd = a.lnd[lane];
+  const LaneRef R = a.lanes[lane];
+  const DsView v = ds_view(R.rec, R.ld);
   double ss = 0.0;
-  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-    const double v = a.g[off + e];
-    ss += v * v;
-    s_out[so + e] = wrap01(a.s[off + e]);
+  for (int e = threadIdx.x; e < R.nd; e += blockDim.x) {
+    const double x = v.g[e];
+    ss += x * x;
+    s_out[R.soff + e] = wrap01(v.s[e]);
   }
   ss = block_sum(ss, red);
   if (threadIdx.x == 0) {
-    e_out[lane] = a.f[lane];
+    const DsState S = *v.st;
+    e_out[lane] = S.f;
     gn_out[lane] = sqrt(ss);
-    ne_out[lane] = a.n_evals[lane];
-    ni_out[lane] = a.it[lane];
-    st_out[lane] = a.status[lane];
-    if (lat_out) lat_out[lane] = a.t1[lane] - a.t0[lane];
+    ne_out[lane] = S.n_evals;
+    ni_out[lane] = S.it;
+    st_out[lane] = S.status;
+    if (lat_out) lat_out[lane] = S.t1 - S.t0;
   }
 }
 
@@ -300,13 +296,12 @@ __device__ __forceinline__ void st2(double* p, int i, double2 v) {
   reinterpret_cast<double2*>(p)[i] = v;
 }
 
-// Per-lane scalar rows in A.scal: a_p, b_p (m each), gamma + cy (1 + m),
-// cs (m), then the pass-B partials of g.dir (nblkB).
-__device__ __forceinline__ double* scal_row(const LbArgs& A, int lane) {
-  return A.scal + (size_t)lane * A.scal_stride;
+__device__ __forceinline__ LbView lane_view(const LbArgs& A, const LaneRef& R) {
+  return lb_view(R.rec, A.m, A.tri_len, R.ld);
 }
 
-__device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double* s) {
+__device__ void lb_record(const LbArgs& A, int lane, const LaneRef& R, LbShared& sh,
+                          const double* s) {
   if (A.traj_count == nullptr) return;
   __shared__ int64_t row;
   if (threadIdx.x == 0) {
@@ -322,9 +317,8 @@ __device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double*
   }
   __syncthreads();
   if (row >= 0) {
-    const int nd = A.lnd[lane];
-    double* o = A.traj_s + A.toff[lane] + (size_t)row * nd;
-    for (int e = threadIdx.x; e < nd; e += blockDim.x) o[e] = wrap01(s[e]);
+    double* o = A.traj_s + R.toff + (size_t)row * R.nd;
+    for (int e = threadIdx.x; e < R.nd; e += blockDim.x) o[e] = wrap01(s[e]);
   }
   __syncthreads();
 }
@@ -333,41 +327,38 @@ __device__ void lb_record(const LbArgs& A, int lane, LbShared& sh, const double*
 // push the new (s, y) pair, update counters and statuses, and advance the
 // rescale pass (history reset) when the pass ends. A lane that keeps running
 // is flagged for a new direction (passes A, scalar, B of this tick).
-__device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
+__device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, const LbView& v,
+                                 LbShared& sh) {
   LbState& L = sh.L;
-  const int ld = A.lld[lane], h2 = ld >> 1, m = A.m;
-  const size_t off = A.voff[lane];
-  double* x = A.x + off;
-  double* s = A.s + off;
-  double* g = A.g + off;
-  const double* dir = A.dir + off;
-  const double* pg = A.pg + off;
-  const double* glo = A.glo + off;
+  const int ld = R.ld, h2 = ld >> 1, m = A.m;
+  double* x = v.x;
+  double* s = v.s;
+  double* g = v.g;
   const int outcome = sh.outcome;
   const bool fail = outcome == LS_FAIL;
-  const double R = L.R;
+  const double Rs = L.R;
   const double f_old = L.f;
   __syncthreads();
   if (!fail) {
     const bool probe = outcome == LS_ACCEPT_PROBE;
     const double al = probe ? L.alpha : L.a_lo;
     const int sl = L.hhead;
-    double* Sr = A.Sh + A.hoff[lane] + (size_t)sl * ld;
-    double* Yr = A.Yh + A.hoff[lane] + (size_t)sl * ld;
+    double* Sr = v.Sh + (size_t)sl * ld;
+    double* Yr = v.Yh + (size_t)sl * ld;
     for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-      const double2 xo = ld2(x, e), dv = ld2(dir, e), go = ld2(g, e);
+      const double2 xo = ld2(x, e), dv = ld2(v.dir, e), go = ld2(g, e);
       const double2 xn = make_double2(xo.x + al * dv.x, xo.y + al * dv.y);
       double2 gn;
       if (probe) {
-        const double2 pv = ld2(pg, e);
-        gn = make_double2(pv.x / R, pv.y / R);
+        const double2 pv = ld2(v.pg, e);
+        gn = make_double2(pv.x / Rs, pv.y / Rs);
       } else {
-        gn = ld2(glo, e);
+        gn = ld2(v.glo, e);
       }
       st2(Sr, e, make_double2(xn.x - xo.x, xn.y - xo.y));
       st2(Yr, e, make_double2(gn.x - go.x, gn.y - go.y));
       st2(x, e, xn);
-      st2(s, e, make_double2(xn.x / R, xn.y / R));
+      st2(s, e, make_double2(xn.x / Rs, xn.y / Rs));
       st2(g, e, gn);
     }
     __syncthreads();
@@ -385,8 +376,8 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
   // |g_s| = |g_x| R
   double ss = 0.0;
   for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-    const double2 v = ld2(g, e);
-    ss += v.x * v.x + v.y * v.y;
+    const double2 gv = ld2(g, e);
+    ss += gv.x * gv.x + gv.y * gv.y;
   }
   ss = block_sum(ss, sh.red);
   if (threadIdx.x == 0) {
@@ -395,7 +386,7 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
     L.pass_evals += ev;
     L.n_evals += ev;
     L.it += 1;
-    const double gnorm = sqrt(ss) * R;
+    const double gnorm = sqrt(ss) * Rs;
     int glob = gnorm < A.grad_tol ? CCO_STATUS_GRAD_TOL : CCO_STATUS_RUNNING;
     if (L.f < A.energy_tol) glob = CCO_STATUS_ENERGY_TOL;
     int local = L.pass_evals >= A.budget ? CCO_STATUS_BUDGET : CCO_STATUS_RUNNING;
@@ -417,7 +408,7 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
     for (int e = threadIdx.x; e < h2; e += blockDim.x) {
       const double2 sv = ld2(s, e), gv = ld2(g, e);
       st2(x, e, make_double2(sv.x * rn, sv.y * rn));
-      st2(g, e, make_double2(gv.x * R / rn, gv.y * R / rn));
+      st2(g, e, make_double2(gv.x * Rs / rn, gv.y * Rs / rn));
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -431,21 +422,25 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, LbShared& sh) {
     }
   }
   __syncthreads();
-  lb_record(A, lane, sh, s);
+  lb_record(A, lane, R, sh, s);
   if (threadIdx.x == 0 && L.status == CCO_STATUS_RUNNING) L.need_dir = 1;
 }
 
+// Lane start: probe positions = s0, every vector zero (padding included).
 __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
   const int lane = blockIdx.x;
-  const int nd = A.lnd[lane];
-  for (int e = threadIdx.x; e < nd; e += blockDim.x) A.ps[A.voff[lane] + e] = s0[A.soff[lane] + e];
+  const LaneRef R = A.lanes[lane];
+  const LbView v = lane_view(A, R);
+  for (int e = threadIdx.x; e < 7 * R.ld; e += blockDim.x) v.x[e] = 0.0;
+  __syncthreads();
+  for (int e = threadIdx.x; e < R.nd; e += blockDim.x) v.ps[e] = s0[R.soff + e];
   if (threadIdx.x == 0) {
     LbState L = {};
     L.phase = PH_INIT;
     L.status = CCO_STATUS_RUNNING;
     L.R = A.rescales[0];
     L.t0 = gtimer();
-    A.st[lane] = L;
+    *v.st = L;
     if (A.traj_count) A.traj_count[lane] = 0;
   }
 }
@@ -456,28 +451,24 @@ __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
 __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
   __shared__ LbShared sh;
   const int lane = blockIdx.x;
-  if (threadIdx.x == 0) sh.L = A.st[lane];
+  const LaneRef R = A.lanes[lane];
+  const LbView v = lane_view(A, R);
+  if (threadIdx.x == 0) sh.L = *v.st;
   __syncthreads();
   if (sh.L.status != CCO_STATUS_RUNNING) return;
   LbState& L = sh.L;
-  const int h2 = A.lld[lane] >> 1;
-  const size_t off = A.voff[lane];
+  const int h2 = R.ld >> 1;
   if (L.phase == PH_INIT) {
     // init_one (lbfgs.py:163-197): x = R0 s0, g_x = g_s / R0, one evaluation
     const double R0 = L.R;
-    double* x = A.x + off;
-    double* s = A.s + off;
-    double* g = A.g + off;
-    const double* ps = A.ps + off;
-    const double* pg = A.pg + off;
     for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-      const double2 v = ld2(ps, e), gv = ld2(pg, e);
-      st2(s, e, v);
-      st2(x, e, make_double2(v.x * R0, v.y * R0));
-      st2(g, e, make_double2(gv.x / R0, gv.y / R0));
+      const double2 sv = ld2(v.ps, e), gv = ld2(v.pg, e);
+      st2(v.s, e, sv);
+      st2(v.x, e, make_double2(sv.x * R0, sv.y * R0));
+      st2(v.g, e, make_double2(gv.x / R0, gv.y / R0));
     }
     if (threadIdx.x == 0) {
-      L.f = A.pf[lane];
+      L.f = *v.pf;
       L.n_evals = 1;
       L.status = L.f < A.energy_tol ? CCO_STATUS_ENERGY_TOL : CCO_STATUS_RUNNING;
       L.last_step = 0.0;
@@ -486,14 +477,15 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
       else L.need_dir = 1;
     }
     __syncthreads();
-    lb_record(A, lane, sh, s);
+    lb_record(A, lane, R, sh, v.s);
   } else {
     if (L.need_dir) {
       // the direction and the first probe (alpha = 1) were written by pass B
       if (threadIdx.x == 0) {
-        const double* dpart = scal_row(A, lane) + 4 * A.m + 1;
+        const double* dpart = v.scal + 4 * A.m + 1;
+        const int nb = lb_nblk(R.ld);
         double dp = 0.0;
-        for (int b = 0; b < A.nblkB; ++b) dp += dpart[b];
+        for (int b = 0; b < nb; ++b) dp += dpart[b];
         L.f0 = L.f;
         L.dphi0 = dp;
         L.phase = PH_EXPAND;
@@ -509,46 +501,41 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
       __syncthreads();
     }
     // one probe of the line search
-    const double R = L.R;
-    const double* pg = A.pg + off;
-    const double* dir = A.dir + off;
+    const double Rs = L.R;
     double dp = 0.0;
     for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-      const double2 pv = ld2(pg, e), dv = ld2(dir, e);
-      dp += (pv.x / R) * dv.x + (pv.y / R) * dv.y;
+      const double2 pv = ld2(v.pg, e), dv = ld2(v.dir, e);
+      dp += (pv.x / Rs) * dv.x + (pv.y / Rs) * dv.y;
     }
     dp = block_sum(dp, sh.red);
     if (threadIdx.x == 0) {
       L.ls_steps += 1;
       int nl = 0;
-      const double fp = A.pf[lane];
+      const double fp = *v.pf;
       sh.outcome = ls_decide(L, fp, dp, A.max_ls, &nl);
       sh.new_lo = nl;
       if (sh.outcome == LS_ACCEPT_PROBE) L.f_lo = fp;  // read by end_iteration
     }
     __syncthreads();
     if (sh.new_lo) {
-      double* glo = A.glo + off;
       for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-        const double2 pv = ld2(pg, e);
-        st2(glo, e, make_double2(pv.x / R, pv.y / R));
+        const double2 pv = ld2(v.pg, e);
+        st2(v.glo, e, make_double2(pv.x / Rs, pv.y / Rs));
       }
     }
     if (sh.outcome == LS_CONTINUE) {
       const double al = L.alpha;
-      const double* x = A.x + off;
-      double* ps = A.ps + off;
       for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-        const double2 xv = ld2(x, e), dv = ld2(dir, e);
-        st2(ps, e, make_double2((xv.x + al * dv.x) / R, (xv.y + al * dv.y) / R));
+        const double2 xv = ld2(v.x, e), dv = ld2(v.dir, e);
+        st2(v.ps, e, make_double2((xv.x + al * dv.x) / Rs, (xv.y + al * dv.y) / Rs));
       }
     } else {
       __syncthreads();
-      lb_end_iteration(A, lane, sh);
+      lb_end_iteration(A, lane, R, v, sh);
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0) A.st[lane] = sh.L;
+  if (threadIdx.x == 0) *v.st = sh.L;
 }
 
 // Pass A (grid: pair blocks x lanes): a_p = s_p.g, b_p = y_p.g for every
@@ -556,20 +543,22 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
 // One warp per pair with four double2 words per lane in flight.
 __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
   const int lane = blockIdx.y;
-  const LbState* Lp = A.st + lane;
+  const LaneRef R = A.lanes[lane];
+  const LbView v = lane_view(A, R);
+  const LbState* Lp = v.st;
   const int k = Lp->hk;
   if (Lp->status != CCO_STATUS_RUNNING || !Lp->need_dir || k == 0) return;
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
   const int p = blockIdx.x * (kUpdThreads / 32) + warp;
   if (p >= k) return;
-  const int ld = A.lld[lane], h2 = ld >> 1, m = A.m;
+  const int ld = R.ld, h2 = ld >> 1, m = A.m;
   const int head = Lp->hhead;
   const bool np = Lp->newpair != 0;
   const int sp = (head - k + p + m) % m, sn = (head - 1 + m) % m;
-  const double* g = A.g + A.voff[lane];
-  const double* sr = A.Sh + A.hoff[lane] + (size_t)sp * ld;
-  const double* yr = A.Yh + A.hoff[lane] + (size_t)sp * ld;
-  const double* yn = A.Yh + A.hoff[lane] + (size_t)sn * ld;
+  const double* g = v.g;
+  const double* sr = v.Sh + (size_t)sp * ld;
+  const double* yr = v.Yh + (size_t)sp * ld;
+  const double* yn = v.Yh + (size_t)sn * ld;
   double ag = 0.0, bg = 0.0, sy = 0.0, yy = 0.0;
   int e = wl;
   for (; e + 96 < h2; e += 128) {
@@ -612,15 +601,13 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
     yy += __shfl_xor_sync(0xffffffffu, yy, o);
   }
   if (wl == 0) {
-    double* sc = scal_row(A, lane);
+    double* sc = v.scal;
     sc[p] = ag;
     sc[m + p] = bg;
     if (np) {
-      double* SYt = A.SYs + (size_t)lane * m * m;   // row = newer slot
-      double* YYs = A.YYs + (size_t)lane * m * m;
-      SYt[(size_t)sn * m + sp] = sy;
-      YYs[(size_t)sp * m + sn] = yy;
-      YYs[(size_t)sn * m + sp] = yy;
+      v.SY[(size_t)sn * m + sp] = sy;   // row = newer slot
+      v.YY[(size_t)sp * m + sn] = yy;
+      v.YY[(size_t)sn * m + sp] = yy;
     }
   }
 }
@@ -628,7 +615,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
 // Scalar kernel (one CTA per lane): gamma and the coefficients of the
 // direction from the inner products. The lower triangles of SY (s_older .
 // y_newer) and YY are copied row by row into shared memory from the slot
-// matrices (rows are contiguous: SYt row = newer slot), then loop 1 runs
+// matrices (rows are contiguous: SY row = newer slot), then loop 1 runs
 // column-oriented (one shuffle per step) and loop 2 row-oriented (one warp
 // reduction per step); both read contiguous shared-memory rows.
 __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
@@ -639,20 +626,22 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
   __shared__ double red[32];
   __shared__ double gam_s;
   const int lane = blockIdx.x;
-  const LbState* Lp = A.st + lane;
+  const LaneRef R = A.lanes[lane];
+  const LbView v = lane_view(A, R);
+  const LbState* Lp = v.st;
   if (Lp->status != CCO_STATUS_RUNNING || !Lp->need_dir) return;
   const int k = Lp->hk, m = A.m, head = Lp->hhead;
-  double* sc = scal_row(A, lane);
+  double* sc = v.scal;
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
   // two packings of SY[p][q] = s_p . y_q (p older than q): triSY by newer
   // rows (tri(p, q) = q (q + 1) / 2 + p) for loop 1, triSO by older rows
   // (off(p) + q - p, off(p) = p k - p (p - 1) / 2) for loop 2
-  double* triSY = A.smem_tri ? dsm : A.tri_g + (size_t)lane * ((size_t)m * (m + 1));
+  double* triSY = A.smem_tri ? dsm : v.tri;
   double* triSO = triSY + (size_t)m * (m + 1) / 2;
-  const double* YYs = A.YYs + (size_t)lane * m * m;
+  const double* YYs = v.YY;
   if (k > 0) {
-    const double* SYt = A.SYs + (size_t)lane * m * m;
+    const double* SYt = v.SY;
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
       sl[p] = (head - k + p + m) % m;
       av[p] = sc[p];
@@ -663,9 +652,9 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
       const double* rs = SYt + (size_t)sl[q] * m;
       const int base = q * (q + 1) / 2;
       for (int p = wl; p <= q; p += 32) {
-        const double v = rs[sl[p]];
-        triSY[base + p] = v;
-        triSO[p * k - p * (p - 1) / 2 + (q - p)] = v;
+        const double x = rs[sl[p]];
+        triSY[base + p] = x;
+        triSO[p * k - p * (p - 1) / 2 + (q - p)] = x;
       }
     }
     __syncthreads();
@@ -680,11 +669,10 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
     }
   } else {
     // gamma (optax scale_by_lbfgs) on a fresh pass: min(1, 1/|g|)
-    const double* g = A.g + A.voff[lane];
     double ss = 0.0;
-    for (int e = threadIdx.x; e < (A.lld[lane] >> 1); e += blockDim.x) {
-      const double2 v = ld2(g, e);
-      ss += v.x * v.x + v.y * v.y;
+    for (int e = threadIdx.x; e < (R.ld >> 1); e += blockDim.x) {
+      const double2 gv = ld2(v.g, e);
+      ss += gv.x * gv.x + gv.y * gv.y;
     }
     ss = block_sum(ss, red);
     if (threadIdx.x == 0) gam_s = fmin(1.0, 1.0 / sqrt(ss));
@@ -766,12 +754,15 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passB(LbArgs A) {
   __shared__ double cyv[kPassBMaxPairs], csv[kPassBMaxPairs];
   __shared__ double red[32];
   const int lane = blockIdx.y;
-  const LbState* Lp = A.st + lane;
+  const LaneRef R = A.lanes[lane];
+  if ((int)blockIdx.x >= lb_nblk(R.ld)) return;   // this lane has fewer element blocks
+  const LbView v = lane_view(A, R);
+  const LbState* Lp = v.st;
   if (Lp->status != CCO_STATUS_RUNNING || !Lp->need_dir) return;
   const int k = Lp->hk, m = A.m, head = Lp->hhead;
-  const int ld = A.lld[lane], h2 = ld >> 1;
-  const double R = Lp->R;
-  double* sc = scal_row(A, lane);
+  const int ld = R.ld, h2 = ld >> 1;
+  const double Rs = Lp->R;
+  double* sc = v.scal;
   const double gam = sc[2 * m];
   const bool in_smem = k <= kPassBMaxPairs;
   if (in_smem) {
@@ -783,13 +774,8 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passB(LbArgs A) {
   __syncthreads();
   const double* cy = in_smem ? cyv : sc + 2 * m + 1;
   const double* cs = in_smem ? csv : sc + 3 * m + 1;
-  const size_t off = A.voff[lane];
-  const double* g = A.g + off;
-  const double* x = A.x + off;
-  double* dir = A.dir + off;
-  double* ps = A.ps + off;
-  const double* Sh = A.Sh + A.hoff[lane];
-  const double* Yh = A.Yh + A.hoff[lane];
+  const double* Sh = v.Sh;
+  const double* Yh = v.Yh;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   double dp = 0.0;
   if (e < h2) {
@@ -815,11 +801,11 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passB(LbArgs A) {
       ax += cy[q] * yv.x + cs[q] * sv.x;
       ay += cy[q] * yv.y + cs[q] * sv.y;
     }
-    const double2 gv = ld2(g, e), xv = ld2(x, e);
+    const double2 gv = ld2(v.g, e), xv = ld2(v.x, e);
     const double2 de = make_double2(ax - gam * gv.x, ay - gam * gv.y);
-    st2(dir, e, de);
+    st2(v.dir, e, de);
     dp = gv.x * de.x + gv.y * de.y;
-    st2(ps, e, make_double2((xv.x + 1.0 * de.x) / R, (xv.y + 1.0 * de.y) / R));
+    st2(v.ps, e, make_double2((xv.x + 1.0 * de.x) / Rs, (xv.y + 1.0 * de.y) / Rs));
   }
   dp = block_sum(dp, red);
   if (threadIdx.x == 0) sc[4 * m + 1 + blockIdx.x] = dp;
@@ -830,17 +816,17 @@ __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double*
                                  int64_t* lat_out) {
   __shared__ double red[32];
   const int lane = blockIdx.x;
-  const size_t off = A.voff[lane], so = A.soff[lane];
-  const int nd = A.lnd[lane];
+  const LaneRef R = A.lanes[lane];
+  const LbView v = lane_view(A, R);
   double ss = 0.0;
-  for (int e = threadIdx.x; e < nd; e += blockDim.x) {
-    const double v = A.g[off + e];
-    ss += v * v;
-    s_out[so + e] = wrap01(A.s[off + e]);
+  for (int e = threadIdx.x; e < R.nd; e += blockDim.x) {
+    const double gv = v.g[e];
+    ss += gv * gv;
+    s_out[R.soff + e] = wrap01(v.s[e]);
   }
   ss = block_sum(ss, red);
   if (threadIdx.x == 0) {
-    const LbState L = A.st[lane];
+    const LbState L = *v.st;
     e_out[lane] = L.f;
     gn_out[lane] = sqrt(ss) * L.R;
     ne_out[lane] = L.n_evals;
@@ -850,13 +836,18 @@ __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double*
   }
 }
 
-__global__ void k_count_running(const int64_t* status, size_t stride, int B, int* out) {
+__global__ void k_count_running(const LaneRef* lanes, int B, int* out) {
   __shared__ double red[32];
   double c = 0.0;
   for (int i = threadIdx.x; i < B; i += blockDim.x)
-    c += (status[(size_t)i * stride] == CCO_STATUS_RUNNING) ? 1.0 : 0.0;
+    c += (*rec_status(lanes[i].rec) == CCO_STATUS_RUNNING) ? 1.0 : 0.0;
   c = block_sum(c, red);
   if (threadIdx.x == 0) *out = (int)c;
+}
+
+__global__ void k_gather_status(const LaneRef* lanes, int B, int64_t* out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < B; i += gridDim.x * blockDim.x)
+    out[i] = *rec_status(lanes[i].rec);
 }
 
 }  // namespace
@@ -904,9 +895,13 @@ cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double
                                                 lat_out);
   return cudaGetLastError();
 }
-cudaError_t count_running(const int64_t* status, size_t stride, int B, int* out,
-                          cudaStream_t st) {
-  k_count_running<<<1, 256, 0, st>>>(status, stride, B, out);
+cudaError_t count_running(const LaneRef* lanes, int B, int* out, cudaStream_t st) {
+  k_count_running<<<1, 256, 0, st>>>(lanes, B, out);
+  return cudaGetLastError();
+}
+cudaError_t gather_status(const LaneRef* lanes, int B, int64_t* out, cudaStream_t st) {
+  int blocks = (B + 255) / 256;
+  k_gather_status<<<blocks < 1 ? 1 : blocks, 256, 0, st>>>(lanes, B, out);
   return cudaGetLastError();
 }
 

@@ -1,4 +1,11 @@
 // Per-lane minimizer state machines (device side). See cco_opt.cu.
+//
+// Every lane owns one contiguous record in device memory holding its whole
+// state: the state machine scalars, its vectors, its L-BFGS history and the
+// scratch of its energy evaluations (densities and pass-1 partials). Kernels
+// reach a lane through a LaneRef table, so a batch may mix lanes of different
+// N, d and k-set, and the serving pool can add and retire lanes between
+// launches without moving any lane's state.
 #pragma once
 
 #include "cco_internal.cuh"
@@ -7,69 +14,140 @@ namespace cco {
 
 enum : int { PH_INIT = 0, PH_ITER = 1, PH_EXPAND = 1, PH_ZOOM = 2 };
 
+// One lane of a launch.
+struct LaneRef {
+  double* rec;      // lane record (layouts below)
+  int nd, ld;       // N d, and N d rounded up to a multiple of 4 doubles
+  int64_t soff;     // offset of the lane in the caller's packed positions
+  int64_t toff;     // offset of the lane's trajectory rows in traj_s
+};
+
+__host__ __device__ __forceinline__ int pad4(int nd) { return (nd + 3) & ~3; }
+
+// Both state structs start with the status word, so a lane's status is the
+// first int64 of its record whatever the minimizer.
+__host__ __device__ __forceinline__ int64_t* rec_status(double* rec) {
+  return reinterpret_cast<int64_t*>(rec);
+}
+
 // ------------------------------------------------------------ descent
-// Lane layouts: lanes may differ in N and d (mixed batches, the serving
-// pool). Every per-lane array is addressed through device offset arrays:
-//   voff[i]  offset (doubles) of lane i in each lane-vector array
-//   soff[i]  offset of lane i in the caller's packed positions (N_i d_i each)
-//   toff[i]  offset of lane i's trajectory rows in traj_s
-//   lnd[i]   N_i d_i
+// Record: [0, 16) DsState and the probe energy pf at [15]; then s, g, ps, pg
+// (ld each); then the evaluation scratch (double2: rho M, rhow M, part nt1 M).
+struct DsState {
+  int64_t status, it, n_evals, t0, t1;   // t0/t1: %globaltimer at start / completion
+  double f, step, norm;
+  int32_t phase, nonzero;
+};
+constexpr int kDsHead = 16;
+
+struct DsView {
+  DsState* st;
+  double *pf, *s, *g, *ps, *pg;
+  double2* dens;
+};
+
+__host__ __device__ __forceinline__ DsView ds_view(double* rec, int ld) {
+  DsView v;
+  v.st = reinterpret_cast<DsState*>(rec);
+  v.pf = rec + kDsHead - 1;
+  v.s = rec + kDsHead;
+  v.g = v.s + ld;
+  v.ps = v.s + 2 * (size_t)ld;
+  v.pg = v.s + 3 * (size_t)ld;
+  v.dens = reinterpret_cast<double2*>(v.s + 4 * (size_t)ld);
+  return v;
+}
+
+__host__ __device__ __forceinline__ size_t ds_record_doubles(int ld, int M, int nt1) {
+  return kDsHead + 4 * (size_t)ld + 2 * (size_t)M * (2 + nt1);
+}
+
 struct DescentArgs {
   int B;
-  const int64_t *voff, *soff, *toff;
-  const int* lnd;
+  const LaneRef* lanes;
   double step_init, step_min, shrink, grow, rel_tol, energy_tol;
   int64_t max_iters;      // max_evals // 2
   int64_t rec_every, rec_cap;
-  // lane state (SoA)
-  double *s, *g;          // [B][nd] accepted point and its gradient
-  double* ps;             // [B][nd] probe positions (evaluation input)
-  const double* pg;       // [B][nd] probe gradient (evaluation output)
-  const double* pf;       // [B]     probe energy
-  double *f, *step, *norm;
-  int64_t *it, *n_evals, *status;
-  int* phase;
-  int* nonzero;           // [B] any(g != 0)
-  int64_t *t0, *t1;       // [B] %globaltimer at start / completion
-  // trajectory (null when off)
+  // trajectory (null when off): traj_e/step/it/count indexed by lane, traj_s by toff
   double *traj_s, *traj_e, *traj_step;
   int64_t *traj_it, *traj_count;
 };
 
 // ------------------------------------------------------------ L-BFGS
 struct LbState {
+  int64_t status, it, n_evals, pass_evals, stag;
+  int64_t t0, t1;         // %globaltimer at start / completion
   double f, R;
   double f0, dphi0, alpha;
   double a_prev, f_prev, d_prev;
   double a_lo, f_lo, d_lo;
   double a_hi, f_hi, d_hi;
   double gamma, last_step;
-  int64_t it, n_evals, pass_evals, stag, status;
-  int64_t t0, t1;         // %globaltimer at start / completion
   int32_t phase, ls_steps, pass_idx, hk, hhead, have_lo, newpair, need_dir;
 };
+constexpr int kLbHead = 32;   // LbState (27 doubles) and pf at [31]
+static_assert(sizeof(LbState) <= (kLbHead - 1) * sizeof(double), "LbState outgrew its slot");
+static_assert(sizeof(DsState) <= (kDsHead - 1) * sizeof(double), "DsState outgrew its slot");
+
+constexpr int kUpdThreads = 256;
+
+// Pass-B element blocks of a lane: one double2 word per thread.
+__host__ __device__ __forceinline__ int lb_nblk(int ld) {
+  return ((ld >> 1) + kUpdThreads - 1) / kUpdThreads;
+}
+// Scalar row: a_p, b_p (m each), gamma + cy (1 + m), cs (m), pass-B partials.
+__host__ __device__ __forceinline__ size_t lb_scal_len(int m, int ld) {
+  return ((size_t)4 * m + 1 + lb_nblk(ld) + 3) & ~(size_t)3;
+}
+
+// Record: [0, 32) LbState, pf at [31]; SY (m m, row = newer slot), YY (m m);
+// the packed triangles (tri_len = m (m + 1) when they do not fit in shared
+// memory, else 0); the scalar row; x, s, g, dir, glo, ps, pg (ld each); the
+// history rings S and Y (m ld each); the evaluation scratch.
+struct LbView {
+  LbState* st;
+  double *pf, *SY, *YY, *tri, *scal;
+  double *x, *s, *g, *dir, *glo, *ps, *pg, *Sh, *Yh;
+  double2* dens;
+};
+
+__host__ __device__ __forceinline__ LbView lb_view(double* rec, int m, int tri_len, int ld) {
+  LbView v;
+  const size_t mm = (size_t)m * m;
+  v.st = reinterpret_cast<LbState*>(rec);
+  v.pf = rec + kLbHead - 1;
+  v.SY = rec + kLbHead;
+  v.YY = v.SY + mm;
+  v.tri = v.YY + mm;
+  v.scal = v.tri + tri_len;
+  v.x = v.scal + lb_scal_len(m, ld);
+  v.s = v.x + ld;
+  v.g = v.x + 2 * (size_t)ld;
+  v.dir = v.x + 3 * (size_t)ld;
+  v.glo = v.x + 4 * (size_t)ld;
+  v.ps = v.x + 5 * (size_t)ld;
+  v.pg = v.x + 6 * (size_t)ld;
+  v.Sh = v.x + 7 * (size_t)ld;
+  v.Yh = v.Sh + (size_t)m * ld;
+  v.dens = reinterpret_cast<double2*>(v.Yh + (size_t)m * ld);
+  return v;
+}
+
+__host__ __device__ __forceinline__ size_t lb_record_doubles(int m, int tri_len, int ld, int M,
+                                                             int nt1) {
+  return kLbHead + 2 * (size_t)m * m + tri_len + lb_scal_len(m, ld) + (7 + 2 * (size_t)m) * ld +
+         2 * (size_t)M * (2 + nt1);
+}
 
 struct LbArgs {
-  int B, m, n_pass;
-  // lane layouts (see DescentArgs); lld[i] = N_i d_i rounded up to 4 doubles
-  // (16-byte rows, zero padding); hoff[i] = offset of lane i in Sh and Yh
-  const int64_t *voff, *soff, *toff, *hoff;
-  const int *lnd, *lld;
+  int B, m, n_pass, tri_len;
+  const LaneRef* lanes;
   double rescales[CCO_MAX_RESCALES];
   double energy_tol, grad_tol;
   int64_t budget, patience, max_ls;
   int64_t rec_every, rec_cap;
-  LbState* st;            // [B]
-  double *x, *s, *g, *dir, *glo;   // [B][nd]
-  double* ps;             // [B][nd] probe s = (x + alpha dir) / R (evaluation input)
-  const double* pg;       // [B][nd] probe dPhi/ds (evaluation output)
-  const double* pf;       // [B]
-  double *Sh, *Yh;        // [B][m][nd] history rings
-  double *SYs, *YYs;      // [B][m][m] slot inner products (SYs: row = newer slot)
-  double* tri_g;          // [B][m (m+1) + 7m] packed triangles when they do not fit in smem
-  double* scal;           // [B][scal_stride] a_p, b_p, gamma, cy, cs, pass-B partials
-  int scal_stride, nblkB; // row length of scal; pass-B element blocks per lane
-  size_t smem_tri;        // 0: triangles in global memory
+  int nblkB;              // grid width of pass B (max over the lanes)
+  size_t smem_tri;        // 0: triangles in the record (global memory)
   double *traj_s, *traj_e, *traj_step;
   int64_t *traj_it, *traj_count;
 };
@@ -88,8 +166,9 @@ cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double
                            int64_t* ne_out, int64_t* ni_out, int64_t* st_out, int64_t* lat_out,
                            cudaStream_t st);
 
-// Count lanes whose status is RUNNING (status stride in int64 units).
-cudaError_t count_running(const int64_t* status, size_t stride, int B, int* out,
-                          cudaStream_t st);
+// Count lanes whose status is RUNNING.
+cudaError_t count_running(const LaneRef* lanes, int B, int* out, cudaStream_t st);
+// Copy every lane's status into out[B].
+cudaError_t gather_status(const LaneRef* lanes, int B, int64_t* out, cudaStream_t st);
 
 }  // namespace cco

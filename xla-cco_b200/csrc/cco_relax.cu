@@ -1,0 +1,588 @@
+// Batched relaxations on lane records: the uniform entry points
+// (cco_relax_descent / cco_relax_lbfgs, one problem for every lane), the
+// mixed ones (a problem per lane), the CUDA-graph tick driver and the
+// schedule autotuner they share with the serving pool (cco_serve.cu).
+//
+// Reference: relax (src/xla_cco/minimize/__init__.py:102-151) runs host
+// rounds of jitted chunks over the RUNNING lanes, padded to a power of two,
+// with a host sync per round. Here every lane is a device state machine
+// (cco_opt.cu); the host only launches captured graphs of ticks and checks,
+// a few graphs behind, whether any lane is still RUNNING.
+#include <cmath>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "cco.h"
+#include "cco_host.cuh"
+
+using namespace cco;
+
+namespace cco {
+
+std::vector<int> branch_bounds(const std::vector<const cco_problem*>& probs, int nbr) {
+  const int B = (int)probs.size();
+  std::vector<double> cum(B + 1, 0.0);
+  for (int i = 0; i < B; ++i) cum[i + 1] = cum[i] + (double)probs[i]->N * probs[i]->M;
+  std::vector<int> b(nbr + 1, 0);
+  b[nbr] = B;
+  for (int k = 1; k < nbr; ++k) {
+    const double target = cum[B] * k / nbr;
+    int i = (int)(std::lower_bound(cum.begin(), cum.end(), target) - cum.begin());
+    i = std::max(i, b[k - 1] + 1);
+    i = std::min(i, B - (nbr - k));
+    b[k] = i;
+  }
+  return b;
+}
+
+namespace {
+
+// ------------------------------------------------------------ schedule cache
+// Tuned schedules are cached per shape class: the minimizer, the lane count
+// and the total evaluation work (sum of N M), each bucketed by powers of two,
+// and the largest d.
+using ShapeKey = std::tuple<int, int, int, int>;
+std::mutex g_sched_mu;
+std::map<ShapeKey, Schedule> g_sched;
+
+ShapeKey shape_key(const std::vector<const cco_problem*>& probs, Method method) {
+  double work = 0.0;
+  int maxd = 1;
+  for (const cco_problem* p : probs) {
+    work += (double)p->N * p->M;
+    maxd = std::max(maxd, p->d);
+  }
+  const int lb = (int)std::floor(std::log2((double)probs.size()));
+  const int lw = (int)std::floor(std::log2(std::max(work, 1.0)));
+  return ShapeKey((int)method, lb, lw, maxd);
+}
+
+int env_int(const char* name, int fallback) {
+  const char* v = getenv(name);
+  return v ? atoi(v) : fallback;
+}
+
+}  // namespace
+
+bool schedule_cached(const std::vector<const cco_problem*>& probs, Method method, Schedule* out) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  auto it = g_sched.find(shape_key(probs, method));
+  if (it == g_sched.end()) return false;
+  *out = it->second;
+  return true;
+}
+
+void schedule_store(const std::vector<const cco_problem*>& probs, Method method,
+                    const Schedule& s) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  g_sched[shape_key(probs, method)] = s;
+}
+
+void schedule_clear() {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  g_sched.clear();
+}
+
+// ------------------------------------------------------------ tick plans
+int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
+  release(st);
+  this->sch = sch;
+  const int B = (int)T.refs.size();
+  nbr = std::max(1, std::min(sch.branches, std::min(kMaxBranches, B)));
+  bounds = branch_bounds(T.probs, nbr);
+  for (int b = 0; b < nbr; ++b) {
+    const int lo = bounds[b], hi = bounds[b + 1];
+    CCO_CUDA(ev[b].build(T.shape, T.refs, T.probs, lo, hi, st));
+    int nblk = 1;
+    for (int i = lo; i < hi; ++i) nblk = std::max(nblk, lb_nblk(T.refs[i].ld));
+    if (T.shape.method == Method::Descent) {
+      DescentArgs a = T.ds;
+      a.B = hi - lo;
+      a.lanes = T.d_refs + lo;
+      if (a.traj_count) {
+        a.traj_e += (size_t)lo * a.rec_cap;
+        a.traj_step += (size_t)lo * a.rec_cap;
+        a.traj_it += (size_t)lo * a.rec_cap;
+        a.traj_count += lo;
+      }
+      ds[b] = a;
+    } else {
+      LbArgs a = T.lb;
+      a.B = hi - lo;
+      a.lanes = T.d_refs + lo;
+      a.nblkB = nblk;
+      if (a.traj_count) {
+        a.traj_e += (size_t)lo * a.rec_cap;
+        a.traj_step += (size_t)lo * a.rec_cap;
+        a.traj_it += (size_t)lo * a.rec_cap;
+        a.traj_count += lo;
+      }
+      lb[b] = a;
+    }
+  }
+  // capture graph_ticks ticks of every branch; branches fork from and join
+  // back into the first capture stream
+  cudaStream_t cap[kMaxBranches] = {};
+  cudaEvent_t fork = nullptr, join[kMaxBranches] = {};
+  cudaError_t e = cudaSuccess;
+  for (int b = 0; b < nbr && e == cudaSuccess; ++b)
+    e = cudaStreamCreateWithFlags(&cap[b], cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+  for (int b = 0; b < nbr && e == cudaSuccess; ++b)
+    e = cudaEventCreateWithFlags(&join[b], cudaEventDisableTiming);
+  // the capture streams must see the uploads made on `st`
+  cudaEvent_t ready = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventRecord(ready, st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(cap[0], ready, 0);
+  cudaGraph_t graph = nullptr;
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(cap[0], cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    e = cudaEventRecord(fork, cap[0]);
+    for (int b = 1; b < nbr && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(cap[b], fork, 0);
+    for (int t = 0; t < sch.graph_ticks && e == cudaSuccess; ++t)
+      for (int b = 0; b < nbr && e == cudaSuccess; ++b) e = tick(cap[b], b);
+    for (int b = 1; b < nbr && e == cudaSuccess; ++b) {
+      e = cudaEventRecord(join[b], cap[b]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(cap[0], join[b], 0);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(cap[0], &graph);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  for (int b = 0; b < nbr; ++b) {
+    if (cap[b]) cudaStreamDestroy(cap[b]);
+    if (join[b]) cudaEventDestroy(join[b]);
+  }
+  if (fork) cudaEventDestroy(fork);
+  if (ready) cudaEventDestroy(ready);
+  if (e != cudaSuccess) return cuda_fail(e, "tick graph capture");
+  return CCO_OK;
+}
+
+cudaError_t TickPlan::tick(cudaStream_t s, int b) const {
+  cudaError_t e = eval_launch(ev[b].plan, s);
+  if (e != cudaSuccess) return e;
+  return method == Method::Descent ? descent_update(ds[b], s) : lbfgs_update(lb[b], s);
+}
+
+int TickPlan::launches_per_tick() const {
+  return nbr * (method == Method::Descent ? 4 : 7);
+}
+
+void TickPlan::release(cudaStream_t st) {
+  if (exec) cudaGraphExecDestroy(exec);
+  exec = nullptr;
+  for (int b = 0; b < kMaxBranches; ++b) ev[b].release(st);
+}
+
+// ------------------------------------------------------------ lane tables
+int LaneTable::upload_refs(cudaStream_t st) {
+  if (d_refs) cudaFreeAsync(d_refs, st);
+  d_refs = nullptr;
+  CCO_CUDA(upload(&d_refs, refs, st));
+  return CCO_OK;
+}
+
+void LaneTable::release(cudaStream_t st) {
+  if (d_refs) cudaFreeAsync(d_refs, st);
+  d_refs = nullptr;
+}
+
+// ------------------------------------------------------------ the tick driver
+namespace {
+
+// Candidate schedules of the online tuner: branch counts 1..4.
+std::vector<Schedule> candidates(int B) {
+  std::vector<Schedule> c;
+  for (int nb = 1; nb <= kMaxBranches; ++nb) {
+    if (nb > 1 && B / nb < 8) break;
+    Schedule s;
+    s.branches = nb;
+    s.graph_ticks = 16;
+    c.push_back(s);
+  }
+  return c;
+}
+
+}  // namespace
+
+int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* stats) {
+  const int B = (int)T.refs.size();
+  constexpr int kSlots = kInflight + 1;
+  int* d_count = nullptr;
+  // pinned completion counters: allocated once per host thread (cudaMallocHost
+  // is slow and may synchronize, so it stays out of every call)
+  static thread_local int* h_count = nullptr;
+  CCO_CUDA(pool_alloc(&d_count, kSlots * sizeof(int), st));
+  if (h_count == nullptr) CCO_CUDA(cudaMallocHost(&h_count, kSlots * sizeof(int)));
+  cudaEvent_t ev[kSlots];
+  for (int i = 0; i < kSlots; ++i) CCO_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+  int64_t ticks = 0, launches = 0;
+  int rc = CCO_OK;
+  cudaError_t e = cudaSuccess;
+  bool done = false;
+
+  // Schedule: forced by the environment, cached for this shape class, or
+  // tuned online. Tuning runs one graph per candidate on the live lanes;
+  // every candidate advances every lane by the same ticks, so the results
+  // do not depend on which schedule wins.
+  Schedule chosen;
+  const int force_br = env_int("CCO_BRANCHES", 0), force_gt = env_int("CCO_GRAPH_TICKS", 0);
+  const bool tune = env_int("CCO_AUTOTUNE", 1) != 0;
+  bool have = false;
+  if (force_br > 0 || force_gt > 0) {
+    if (force_br > 0) chosen.branches = force_br;
+    if (force_gt > 0) chosen.graph_ticks = force_gt;
+    have = true;
+  } else if (schedule_cached(T.probs, T.shape.method, &chosen) || !tune) {
+    have = true;
+  }
+  if (!have) {
+    const std::vector<Schedule> cand = candidates(B);
+    std::vector<cudaEvent_t> t0(cand.size()), t1(cand.size());
+    std::vector<float> ms(cand.size(), 1e30f);
+    for (size_t c = 0; c < cand.size(); ++c) {
+      cudaEventCreate(&t0[c]);
+      cudaEventCreate(&t1[c]);
+    }
+    for (size_t c = 0; c < cand.size() && rc == CCO_OK && ticks < max_ticks; ++c) {
+      TickPlan P;
+      P.method = T.shape.method;
+      rc = P.build(T, cand[c], st);
+      if (rc != CCO_OK) break;
+      e = cudaEventRecord(t0[c], st);
+      if (e == cudaSuccess) e = cudaGraphLaunch(P.exec, st);
+      if (e == cudaSuccess) e = cudaEventRecord(t1[c], st);
+      ticks += cand[c].graph_ticks;
+      launches += (int64_t)cand[c].graph_ticks * P.launches_per_tick();
+      P.release(st);
+      if (e != cudaSuccess) break;
+    }
+    if (rc == CCO_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+    int best = 0;
+    for (size_t c = 0; c < cand.size() && e == cudaSuccess && rc == CCO_OK; ++c) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, t0[c], t1[c]) == cudaSuccess) ms[c] = t / cand[c].graph_ticks;
+      if (ms[c] < ms[best]) best = (int)c;
+    }
+    for (size_t c = 0; c < cand.size(); ++c) {
+      cudaEventDestroy(t0[c]);
+      cudaEventDestroy(t1[c]);
+    }
+    chosen = cand[best];
+    // graphs of about 3 ms of device work: launch overhead amortised, and the
+    // few graphs that run past the last lane's completion stay short
+    const double tick_ms = ms[best] < 1e29f ? ms[best] : 0.2;
+    int gt = (int)std::lround(3.0 / std::max(tick_ms, 1e-3));
+    chosen.graph_ticks = std::max(4, std::min(32, gt));
+    if (rc == CCO_OK && e == cudaSuccess) schedule_store(T.probs, T.shape.method, chosen);
+    // tuning may already have finished every lane
+    if (rc == CCO_OK && e == cudaSuccess) {
+      e = count_running(T.d_refs, B, d_count, st);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(h_count, d_count, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e == cudaSuccess && h_count[0] == 0) done = true;
+    }
+  }
+
+  TickPlan P;
+  P.method = T.shape.method;
+  if (rc == CCO_OK && e == cudaSuccess && !done) rc = P.build(T, chosen, st);
+  int launched = 0, checked = 0;
+  while (rc == CCO_OK && e == cudaSuccess && !done) {
+    if (ticks >= max_ticks) break;
+    e = cudaGraphLaunch(P.exec, st);
+    if (e != cudaSuccess) break;
+    ticks += chosen.graph_ticks;
+    launches += (int64_t)chosen.graph_ticks * P.launches_per_tick() + 1;
+    const int slot = launched % kSlots;
+    e = count_running(T.d_refs, B, d_count + slot, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_count + slot, d_count + slot, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[slot], st);
+    ++launched;
+    if (e == cudaSuccess && launched - checked > kInflight) {
+      const int old = checked % kSlots;
+      e = cudaEventSynchronize(ev[old]);
+      ++checked;
+      if (e == cudaSuccess && h_count[old] == 0) done = true;
+    }
+  }
+  // drain the launches still in flight, oldest first
+  while (rc == CCO_OK && e == cudaSuccess && !done && checked < launched) {
+    const int old = checked % kSlots;
+    e = cudaEventSynchronize(ev[old]);
+    ++checked;
+    if (e == cudaSuccess && h_count[old] == 0) done = true;
+  }
+  if (rc == CCO_OK) {
+    if (e != cudaSuccess) rc = cuda_fail(e, "relax ticks");
+    else if (!done) rc = fail(CCO_ERR_ROUNDS, "relax did not finish within the round bound (%lld ticks)", (long long)max_ticks);
+  }
+  P.release(st);
+  for (int i = 0; i < kSlots; ++i) cudaEventDestroy(ev[i]);
+  cudaFreeAsync(d_count, st);
+  cudaStreamSynchronize(st);
+  if (stats) {
+    stats->ticks = ticks;
+    stats->launches = launches;
+    stats->schedule = chosen;
+  }
+  return rc;
+}
+
+}  // namespace cco
+
+// ------------------------------------------------------------ entry points
+namespace {
+
+bool out_ok(const cco_relax_out* o) {
+  return o && o->s && o->energy && o->grad_norm && o->n_evals && o->n_iters && o->status;
+}
+
+int check_traj(const cco_relax_out* out, bool rec) {
+  if (rec && (!out->traj_s || !out->traj_energy || !out->traj_step || !out->traj_iteration ||
+              !out->traj_count))
+    return fail(CCO_ERR_ARG, "trajectory recording needs the traj_* outputs");
+  return CCO_OK;
+}
+
+// Lane table of a one-shot relaxation: records carved from one allocation,
+// positions packed in the caller's order, trajectory rows `cap` per lane.
+int make_table(cco_problem* const* probs, int B, const RecordShape& shape, int64_t cap,
+               cudaStream_t st, LaneTable* T, double** records) {
+  if (B < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  T->shape = shape;
+  T->probs.resize(B);
+  T->refs.resize(B);
+  size_t total = 0;
+  int device = -1;
+  for (int i = 0; i < B; ++i) {
+    const cco_problem* p = probs[i];
+    if (!p) return fail(CCO_ERR_ARG, "null problem for lane %d", i);
+    if (device < 0) device = p->device;
+    if (p->device != device) return fail(CCO_ERR_ARG, "lanes must share one device");
+    T->probs[i] = p;
+    total += record_doubles(shape, p);
+  }
+  CCO_CUDA(pool_alloc(records, total * sizeof(double), st));
+  size_t o = 0;
+  int64_t soff = 0;
+  for (int i = 0; i < B; ++i) {
+    const cco_problem* p = T->probs[i];
+    LaneRef& r = T->refs[i];
+    r.rec = *records + o;
+    r.nd = p->N * p->d;
+    r.ld = pad4(r.nd);
+    r.soff = soff;
+    r.toff = cap * soff;
+    o += record_doubles(shape, p);
+    soff += r.nd;
+  }
+  return T->upload_refs(st);
+}
+
+int relax_descent_set(cco_problem* const* probs, int B, cudaStream_t st, const double* s0,
+                      const cco_descent_settings* cfg, cco_relax_out* out) {
+  if (!cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
+  if (!out_ok(out)) return fail(CCO_ERR_ARG, "incomplete output struct");
+  if (cfg->max_evals < 0) return fail(CCO_ERR_ARG, "max_evals must be >= 0");
+  if (B < 1 || !probs[0]) return fail(CCO_ERR_ARG, "need at least one configuration");
+  const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
+  if (check_traj(out, rec) != CCO_OK) return CCO_ERR_ARG;
+  DeviceGuard guard(probs[0]->device);
+  RecordShape shape;
+  shape.method = Method::Descent;
+  LaneTable T;
+  DescentArgs& a = T.ds;
+  a.step_init = cfg->step_init;
+  a.step_min = cfg->step_min;
+  a.shrink = cfg->shrink;
+  a.grow = cfg->grow;
+  a.rel_tol = cfg->rel_tol;
+  a.energy_tol = cfg->energy_tol;
+  a.max_iters = cfg->max_evals / 2;
+  a.rec_every = rec ? cfg->record_every : 1;
+  a.rec_cap = rec ? cfg->max_records : 0;
+  if (rec) {
+    a.traj_s = out->traj_s;
+    a.traj_e = out->traj_energy;
+    a.traj_step = out->traj_step;
+    a.traj_it = out->traj_iteration;
+    a.traj_count = out->traj_count;
+  }
+  double* records = nullptr;
+  int rc = make_table(probs, B, shape, a.rec_cap, st, &T, &records);
+  if (rc != CCO_OK) {
+    if (records) cudaFreeAsync(records, st);
+    return rc;
+  }
+  a.B = B;
+  a.lanes = T.d_refs;
+  CCO_CUDA(descent_init(a, s0, st));
+  const int64_t max_ticks = 1 + a.max_iters + 4 * (kInflight + 1) * 32;
+  RunStats rs;
+  rc = run_lane_table(T, st, max_ticks, &rs);
+  if (rc == CCO_OK) {
+    cudaError_t e = descent_finalize(a, out->s, out->energy, out->grad_norm, out->n_evals,
+                                     out->n_iters, out->status, out->latency_ns, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "descent_finalize");
+  }
+  out->ticks = rs.ticks;
+  out->launches = rs.launches + 3;
+  out->branches = rs.schedule.branches;
+  out->graph_ticks = rs.schedule.graph_ticks;
+  T.release(st);
+  cudaFreeAsync(records, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "relax descent");
+  return rc;
+}
+
+std::mutex g_cfg_mu;
+size_t g_scalar_smem_configured = 0;
+
+int relax_lbfgs_set(cco_problem* const* probs, int B, cudaStream_t st, const double* s0,
+                    const cco_lbfgs_settings* cfg, cco_relax_out* out) {
+  if (!cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
+  if (!out_ok(out)) return fail(CCO_ERR_ARG, "incomplete output struct");
+  if (cfg->n_rescales < 1 || cfg->n_rescales > CCO_MAX_RESCALES)
+    return fail(CCO_ERR_ARG, "need 1..%d rescale passes", CCO_MAX_RESCALES);
+  if (cfg->memory < 1) return fail(CCO_ERR_ARG, "memory must be >= 1");
+  if (cfg->memory > 256) return fail(CCO_ERR_ARG, "memory must be <= 256 on this build");
+  if (cfg->max_linesearch_steps < 1) return fail(CCO_ERR_ARG, "max_linesearch_steps must be >= 1");
+  if (B < 1 || !probs[0]) return fail(CCO_ERR_ARG, "need at least one configuration");
+  const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
+  if (check_traj(out, rec) != CCO_OK) return CCO_ERR_ARG;
+  DeviceGuard guard(probs[0]->device);
+  LaneTable T;
+  LbArgs& A = T.lb;
+  int rc = lbfgs_args(cfg, &A, &T.shape);
+  if (rc != CCO_OK) return rc;
+  if (rec) {
+    A.traj_s = out->traj_s;
+    A.traj_e = out->traj_energy;
+    A.traj_step = out->traj_step;
+    A.traj_it = out->traj_iteration;
+    A.traj_count = out->traj_count;
+  }
+  A.rec_every = rec ? cfg->record_every : 1;
+  A.rec_cap = rec ? cfg->max_records : 0;
+  double* records = nullptr;
+  rc = make_table(probs, B, T.shape, A.rec_cap, st, &T, &records);
+  if (rc != CCO_OK) {
+    if (records) cudaFreeAsync(records, st);
+    return rc;
+  }
+  A.B = B;
+  A.lanes = T.d_refs;
+  int nblk = 1;
+  for (const LaneRef& r : T.refs) nblk = std::max(nblk, lb_nblk(r.ld));
+  A.nblkB = nblk;
+  CCO_CUDA(lbfgs_init(A, s0, st));
+  const int64_t max_ticks =
+      1 + (int64_t)cfg->n_rescales * (cfg->max_evals_per_pass + cfg->max_linesearch_steps + 1) +
+      4 * (kInflight + 1) * 32;
+  RunStats rs;
+  rc = run_lane_table(T, st, max_ticks, &rs);
+  if (rc == CCO_OK) {
+    cudaError_t e = lbfgs_finalize(A, out->s, out->energy, out->grad_norm, out->n_evals,
+                                   out->n_iters, out->status, out->latency_ns, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "lbfgs_finalize");
+  }
+  out->ticks = rs.ticks;
+  out->launches = rs.launches + 3;
+  out->branches = rs.schedule.branches;
+  out->graph_ticks = rs.schedule.graph_ticks;
+  T.release(st);
+  cudaFreeAsync(records, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "relax lbfgs");
+  return rc;
+}
+
+}  // namespace
+
+namespace cco {
+
+// Settings -> kernel arguments shared by the one-shot relaxation and the
+// serving pool; also sizes the scalar kernel's shared-memory triangles.
+int lbfgs_args(const cco_lbfgs_settings* cfg, LbArgs* A, RecordShape* shape) {
+  *A = LbArgs{};
+  const int m = (int)cfg->memory;
+  A->m = m;
+  A->n_pass = cfg->n_rescales;
+  for (int i = 0; i < CCO_MAX_RESCALES; ++i)
+    A->rescales[i] = i < cfg->n_rescales ? cfg->rescales[i] : 1.0;
+  A->energy_tol = cfg->energy_tol;
+  A->grad_tol = cfg->grad_tol;
+  A->budget = cfg->max_evals_per_pass;
+  A->patience = cfg->stagnation_patience;
+  A->max_ls = cfg->max_linesearch_steps;
+  A->rec_every = 1;
+  A->rec_cap = 0;
+  const size_t tri_bytes = lbfgs_update_smem(m);
+  const bool in_smem = tri_bytes <= 200 * 1024;
+  A->smem_tri = in_smem ? tri_bytes : 0;
+  A->tri_len = in_smem ? 0 : m * (m + 1);
+  if (in_smem) {
+    std::lock_guard<std::mutex> lk(g_cfg_mu);
+    if (g_scalar_smem_configured < 200 * 1024) {
+      CCO_CUDA(lbfgs_configure(200 * 1024));
+      g_scalar_smem_configured = 200 * 1024;
+    }
+  }
+  shape->method = Method::Lbfgs;
+  shape->m = m;
+  shape->tri_len = A->tri_len;
+  return CCO_OK;
+}
+
+}  // namespace cco
+
+extern "C" int cco_relax_descent(cco_problem* p, void* stream, int batch, const double* s0,
+                                 const cco_descent_settings* cfg, int chunk_iters,
+                                 cco_relax_out* out) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  std::vector<cco_problem*> probs(batch, p);
+  return relax_descent_set(probs.data(), batch, (cudaStream_t)stream, s0, cfg, out);
+}
+
+extern "C" int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const double* s0,
+                               const cco_lbfgs_settings* cfg, int chunk_iters,
+                               cco_relax_out* out) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  std::vector<cco_problem*> probs(batch, p);
+  return relax_lbfgs_set(probs.data(), batch, (cudaStream_t)stream, s0, cfg, out);
+}
+
+extern "C" int cco_relax_descent_mixed(cco_problem* const* problems, void* stream, int batch,
+                                       const double* s0, const cco_descent_settings* cfg,
+                                       int chunk_iters, cco_relax_out* out) {
+  if (!problems) return fail(CCO_ERR_ARG, "null problem array");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  return relax_descent_set(problems, batch, (cudaStream_t)stream, s0, cfg, out);
+}
+
+extern "C" int cco_relax_lbfgs_mixed(cco_problem* const* problems, void* stream, int batch,
+                                     const double* s0, const cco_lbfgs_settings* cfg,
+                                     int chunk_iters, cco_relax_out* out) {
+  if (!problems) return fail(CCO_ERR_ARG, "null problem array");
+  if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  return relax_lbfgs_set(problems, batch, (cudaStream_t)stream, s0, cfg, out);
+}
+
+extern "C" int cco_schedule_reset(void) {
+  schedule_clear();
+  return CCO_OK;
+}

@@ -75,6 +75,8 @@ class RelaxOutC(ctypes.Structure):
         ("latency_ns", _vp),
         ("ticks", ctypes.c_int64),
         ("launches", ctypes.c_int64),
+        ("branches", ctypes.c_int32),
+        ("graph_ticks", ctypes.c_int32),
     ]
 
 
@@ -103,6 +105,7 @@ SIGNATURES = {
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(LBFGSSettingsC), ctypes.c_int,
          ctypes.POINTER(RelaxOutC)],
     ),  # fmt: skip
+    "cco_schedule_reset": (ctypes.c_int, []),
     "cco_relax_descent_mixed": (
         ctypes.c_int,
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(DescentSettingsC), ctypes.c_int,

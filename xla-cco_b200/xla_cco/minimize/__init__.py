@@ -103,6 +103,7 @@ def _call_relax(fn: str, first: Any, dev: Any, b: int, s0_ptr: int, cset: Any, c
     _native.check(code, fn)
     out["ticks"] = int(co.ticks)
     out["launches"] = int(co.launches)
+    out["schedule"] = (int(co.branches), int(co.graph_ticks))
 
 
 def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
