@@ -53,6 +53,7 @@ extern "C" {
 #define CCO_STATUS_LINESEARCH_FAIL 5
 #define CCO_STATUS_GRAD_TOL 6
 #define CCO_STATUS_DRIFT 7
+#define CCO_STATUS_CANCELLED 8  /* serving pool only: the request was cancelled */
 
 typedef struct cco_problem cco_problem;
 
@@ -212,6 +213,62 @@ int cco_relax_lbfgs_mixed(cco_problem* const* problems, void* stream, int batch,
  * schedule, CCO_AUTOTUNE=0 keeps the default (2 branches, 16 ticks).
  */
 int cco_schedule_reset(void);
+
+/*
+ * Serving pool (no reference counterpart; the reference relaxes one batch
+ * per call). A server owns one device and one L-BFGS setting. Requests - one
+ * configuration of any problem on that device - are submitted from any host
+ * thread and queue in arrival order. A driver thread admits them while the
+ * lane records fit both max_lanes and the HBM budget (footprint per lane:
+ * positions, gradients and search vectors 7 N d, history 2 m N d, the
+ * density and pass-1 partials M (2 + ceil(N / 64)) complex, all FP64),
+ * continuously: a request that arrives while others run joins the running
+ * set at the next graph boundary, and a finished lane leaves it and frees
+ * its memory. Every lane's result is bit-identical to the same
+ * configuration relaxed alone by cco_relax_lbfgs with the same settings.
+ * Problems must outlive the requests that use them.
+ */
+typedef struct cco_server cco_server;
+
+typedef struct {
+  int64_t max_lanes;        /* lanes on the device at once (0: 4096) */
+  int64_t hbm_budget_bytes; /* admission budget for lane records (0: 150 GB), clamped to 90%
+                               of the device memory free at creation */
+  int32_t graph_ticks;      /* ticks per launched graph (0: 8) */
+  int32_t branches;         /* graph branches (0: 2 when >= 64 lanes run, else 1) */
+} cco_server_config;
+
+typedef struct {
+  double* s;                /* in: host [N][d] buffer for the final positions, or NULL */
+  double energy, grad_norm;
+  int64_t n_evals, n_iters, status;  /* status: CCO_STATUS_*, CANCELLED included */
+  int64_t submit_ns, admit_ns, done_ns;  /* host steady clock (ns) */
+  int64_t device_ns;        /* device time from the lane's first tick to its completion */
+  int32_t error;            /* CCO_OK, or the code of a device failure that ended it */
+  int32_t pad_;
+} cco_request_result;
+
+typedef struct {
+  int64_t submitted, admitted, completed, cancelled, pending, running;
+  int64_t bytes_in_use, peak_bytes, peak_lanes, budget_bytes;
+  int64_t graphs, ticks, rebuilds;
+} cco_server_stats;
+
+int cco_server_create(int device, const cco_lbfgs_settings* settings,
+                      const cco_server_config* config, cco_server** out);
+/* Cancels what is still queued or running, stops the driver and frees all. */
+int cco_server_destroy(cco_server* server);
+/* Copies s0 (host [N][d]) and queues it. CCO_ERR_ADMISSION if this request
+ * alone exceeds the budget; the driver's error code once it has failed. */
+int cco_server_submit(cco_server* server, cco_problem* p, const double* s0, int64_t* ticket);
+/* Waits up to timeout_ms (0: no wait, < 0: until done) for the request.
+ * CCO_OK: done, `out` filled (out->s copied if non-NULL) and the ticket
+ * released; CCO_ERR_TIMEOUT: not done yet; CCO_ERR_ARG: unknown ticket. */
+int cco_server_poll(cco_server* server, int64_t ticket, int timeout_ms, cco_request_result* out);
+/* Queued requests end at once, running ones at the next graph boundary,
+ * both with status CCO_STATUS_CANCELLED. Finished ones are unaffected. */
+int cco_server_cancel(cco_server* server, int64_t ticket);
+int cco_server_get_stats(cco_server* server, cco_server_stats* out);
 
 #ifdef __cplusplus
 }

@@ -67,3 +67,24 @@ def test_no_device_is_reported_not_hidden():
         pytest.skip("a GPU is visible")
     with pytest.raises(RuntimeError, match="needs a CUDA device"):
         _native.require_gpu()
+
+
+def test_server_without_device_is_refused():
+    if _native.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    from xla_cco.minimize import _lbfgs_c
+    from xla_cco.minimize.lbfgs import LBFGSSettings
+
+    lib = _native.load()
+    cset = _lbfgs_c(LBFGSSettings())
+    cfg = _native.ServerConfigC(0, 0, 0, 0)
+    h = ctypes.c_void_p()
+    code = lib.cco_server_create(0, ctypes.byref(cset), ctypes.byref(cfg), ctypes.byref(h))
+    assert code == _native.CCO_ERR_NODEVICE and not h.value
+    assert lib.cco_server_destroy(None) == _native.CCO_OK
+
+
+def test_serving_structs_match_header():
+    assert ctypes.sizeof(_native.ServerConfigC) == 3 * 8
+    assert ctypes.sizeof(_native.RequestResultC) == 11 * 8
+    assert ctypes.sizeof(_native.ServerStatsC) == 13 * 8

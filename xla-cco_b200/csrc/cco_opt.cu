@@ -850,6 +850,14 @@ __global__ void k_gather_status(const LaneRef* lanes, int B, int64_t* out) {
     out[i] = *rec_status(lanes[i].rec);
 }
 
+__global__ void k_cancel_lbfgs(double* rec) {
+  LbState* L = reinterpret_cast<LbState*>(rec);
+  if (L->status == CCO_STATUS_RUNNING) {
+    L->status = CCO_STATUS_CANCELLED;
+    L->t1 = gtimer();
+  }
+}
+
 }  // namespace
 
 cudaError_t descent_init(const DescentArgs& a, const double* s0, cudaStream_t st) {
@@ -902,6 +910,11 @@ cudaError_t count_running(const LaneRef* lanes, int B, int* out, cudaStream_t st
 cudaError_t gather_status(const LaneRef* lanes, int B, int64_t* out, cudaStream_t st) {
   int blocks = (B + 255) / 256;
   k_gather_status<<<blocks < 1 ? 1 : blocks, 256, 0, st>>>(lanes, B, out);
+  return cudaGetLastError();
+}
+
+cudaError_t cancel_lbfgs_lane(double* rec, cudaStream_t st) {
+  k_cancel_lbfgs<<<1, 1, 0, st>>>(rec);
   return cudaGetLastError();
 }
 

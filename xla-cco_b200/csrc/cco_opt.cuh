@@ -170,5 +170,7 @@ cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double
 cudaError_t count_running(const LaneRef* lanes, int B, int* out, cudaStream_t st);
 // Copy every lane's status into out[B].
 cudaError_t gather_status(const LaneRef* lanes, int B, int64_t* out, cudaStream_t st);
+// Ends an L-BFGS lane with CCO_STATUS_CANCELLED if it is still RUNNING.
+cudaError_t cancel_lbfgs_lane(double* rec, cudaStream_t st);
 
 }  // namespace cco

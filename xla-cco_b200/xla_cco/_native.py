@@ -80,6 +80,39 @@ class RelaxOutC(ctypes.Structure):
     ]
 
 
+class ServerConfigC(ctypes.Structure):
+    _fields_ = [
+        ("max_lanes", ctypes.c_int64),
+        ("hbm_budget_bytes", ctypes.c_int64),
+        ("graph_ticks", ctypes.c_int32),
+        ("branches", ctypes.c_int32),
+    ]
+
+
+class RequestResultC(ctypes.Structure):
+    _fields_ = [
+        ("s", _vp),
+        ("energy", ctypes.c_double),
+        ("grad_norm", ctypes.c_double),
+        ("n_evals", ctypes.c_int64),
+        ("n_iters", ctypes.c_int64),
+        ("status", ctypes.c_int64),
+        ("submit_ns", ctypes.c_int64),
+        ("admit_ns", ctypes.c_int64),
+        ("done_ns", ctypes.c_int64),
+        ("device_ns", ctypes.c_int64),
+        ("error", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+    ]
+
+
+class ServerStatsC(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_int64) for name in (
+        "submitted", "admitted", "completed", "cancelled", "pending", "running",
+        "bytes_in_use", "peak_bytes", "peak_lanes", "budget_bytes", "graphs", "ticks", "rebuilds",
+    )]  # fmt: skip
+
+
 # (name, restype, argtypes) for every symbol include/cco.h declares
 SIGNATURES = {
     "cco_abi_version": (ctypes.c_int, []),
@@ -106,6 +139,16 @@ SIGNATURES = {
          ctypes.POINTER(RelaxOutC)],
     ),  # fmt: skip
     "cco_schedule_reset": (ctypes.c_int, []),
+    "cco_server_create": (
+        ctypes.c_int,
+        [ctypes.c_int, ctypes.POINTER(LBFGSSettingsC), ctypes.POINTER(ServerConfigC),
+         ctypes.POINTER(_vp)],
+    ),  # fmt: skip
+    "cco_server_destroy": (ctypes.c_int, [_vp]),
+    "cco_server_submit": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_int64)]),
+    "cco_server_poll": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(RequestResultC)]),
+    "cco_server_cancel": (ctypes.c_int, [_vp, ctypes.c_int64]),
+    "cco_server_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServerStatsC)]),
     "cco_relax_descent_mixed": (
         ctypes.c_int,
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(DescentSettingsC), ctypes.c_int,

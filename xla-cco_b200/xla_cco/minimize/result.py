@@ -22,6 +22,7 @@ STATUS_STAGNATED: int = 4
 STATUS_LINESEARCH_FAIL: int = 5
 STATUS_GRAD_TOL: int = 6
 STATUS_DRIFT: int = 7
+STATUS_CANCELLED: int = 8  # serving pool only (no reference counterpart)
 
 
 @dataclasses.dataclass
