@@ -331,6 +331,167 @@ def run_device(args) -> None:
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ mixed batch
+def _flops(evals, inst) -> float:
+    return float(sum(float(e) * i.n * i.m * F_PAIR[i.d] for e, i in zip(evals, inst)))
+
+
+def plain_dropin(inst, settings, sample: int) -> dict:
+    """The reference's usage on a mixed ensemble: one relax call per instance
+    (relax takes one energy, so instances of different N, d, chi cannot share
+    a call). Times `sample` instances one after another, after one untimed
+    pass over the same instances."""
+    import torch
+
+    from xla_cco.minimize import relax_device
+
+    sub = inst[:sample]
+    dev = [torch.from_numpy(i.s0[None]).cuda() for i in sub]
+    for i, x in zip(sub, dev):
+        relax_device(i.energy, x, settings)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    outs = [relax_device(i.energy, x, settings) for i, x in zip(sub, dev)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    succ = sum(int((o["energy"] < TOL).sum().item()) for o in outs)
+    return {"value": succ / (ms / 1e3), "unit": UNIT, "instances": len(sub), "success": succ,
+            "ms": ms, "how": "relax(energy_i, s0_i[None]) per instance, sequential, same device"}  # fmt: skip
+
+
+def run_mixed(args) -> None:
+    import torch
+
+    from xla_cco import LBFGSSettings
+    from xla_cco.minimize import relax_mixed_device
+    from xla_cco.workloads import mixed_ensemble
+
+    torch.cuda.set_device(0)
+    inst = mixed_ensemble(args.mixed_count, seed=SEED)
+    energies = [i.energy for i in inst]
+    shapes = [(i.n, i.d) for i in inst]
+    for i in inst:
+        i.energy.problem_handle(0, i.n)
+    flat = torch.from_numpy(np.concatenate([i.s0.ravel() for i in inst])).cuda()
+    settings = LBFGSSettings(energy_tol=TOL)
+    for _ in range(args.warmup):
+        relax_mixed_device(energies, flat, shapes, settings)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    outs = [relax_mixed_device(energies, flat, shapes, settings) for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    succ = sum(int((o["energy"] < TOL).sum().item()) for o in outs)
+    evals = outs[-1]["n_evals"].cpu().numpy()
+    lat = np.concatenate([o["latency_ns"].cpu().numpy() for o in outs]) / 1e6
+    flops = _flops(evals, inst) * args.steps
+    value = succ / (ms / 1e3)
+    plain = plain_dropin(inst, settings, args.plain_sample)
+    peak = fp64_peak_tflops()
+    achieved = flops / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "relaxations/s to Phi<1e-20 (mixed-size batch, one device run, plain FP64)",
+        "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {
+            "workload": f"mixed_lbfgs_{len(inst)}_n200-8000_d123_chi0.05-0.49",
+            "instances": len(inst), "seeds": "xla_cco.workloads.mixed_ensemble(seed=0)",
+            "success": f"{succ}/{len(inst) * args.steps}",
+            "p50_latency_ms": float(np.percentile(lat, 50)),
+            "p99_latency_ms": float(np.percentile(lat, 99)),
+            "evals_per_relax": float(evals.mean()),
+            "schedule": outs[-1]["schedule"], "ticks": outs[-1]["ticks"],
+            "l2": "inputs larger than L2 (lane records of the whole ensemble)",
+        },
+        "plain_fp64_dropin": plain,
+        "speedup_vs_plain_dropin": value / plain["value"] if plain["value"] else None,
+        "roofline": {"kernel": "whole relaxation (evaluations + updates)", "bound": "fp64",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None,
+                     "algorithmic": "sum over lanes of evals x N M x flop/pair(d)"},  # fmt: skip
+        "clocks": clocks,
+        "gpu_launches": sum(o["launches"] for o in outs),
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ request stream
+def run_serve(args) -> None:
+    import torch
+
+    from xla_cco import LBFGSSettings
+    from xla_cco.serve import RelaxServer
+    from xla_cco.workloads import request_stream
+
+    torch.cuda.set_device(0)
+    reqs = request_stream(args.serve_count, seed=SEED, rate=args.serve_rate)
+    for r in reqs:
+        r.energy.problem_handle(0, r.n)
+    settings = LBFGSSettings(energy_tol=TOL)
+    sampler = ClockSampler(0)
+    with RelaxServer(settings, hbm_budget_bytes=150 << 30) as srv:
+        # warm-up: a few requests through the pool before the stream starts
+        for t in [srv.submit(r.energy, r.s0) for r in reqs[: args.warmup]]:
+            srv.result(t)
+        sampler.start()
+        t0 = time.perf_counter()
+        tickets = []
+        for r in reqs:
+            delay = t0 + r.arrival_s - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(srv.submit(r.energy, r.s0))
+        results = [srv.result(t) for t in tickets]
+        clocks = sampler.stop()
+        st = srv.stats()
+    first = min(x.submit_ns for x in results)
+    last = max(x.done_ns for x in results)
+    span = (last - first) * 1e-9
+    succ = sum(1 for x in results if x.energy < TOL)
+    lat = np.array([x.latency_s for x in results]) * 1e3
+    queue = np.array([(x.admit_ns - x.submit_ns) * 1e-6 for x in results])
+    dev = np.array([x.device_ns * 1e-6 for x in results])
+    evals = np.array([x.n_evals for x in results])
+    flops = _flops(evals, reqs)
+    peak = fp64_peak_tflops()
+    line = {
+        "metric": "served relaxations/s to Phi<1e-20 + p50/p99 latency (Poisson stream, plain FP64)",
+        "value": succ / span, "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": args.warmup,
+        "ms_per_step": span * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {
+            "workload": f"serve_lbfgs_{len(reqs)}req_{args.serve_rate:g}rps_n100-20000_d23_chi0.10-0.45",
+            "requests": len(reqs), "rate_rps": args.serve_rate,
+            "seeds": "xla_cco.workloads.request_stream(seed=0)", "hbm_budget_gb": 150,
+            "success": f"{succ}/{len(reqs)}",
+            "p50_latency_ms": float(np.percentile(lat, 50)),
+            "p99_latency_ms": float(np.percentile(lat, 99)),
+            "p50_queue_ms": float(np.percentile(queue, 50)),
+            "p99_queue_ms": float(np.percentile(queue, 99)),
+            "p50_device_ms": float(np.percentile(dev, 50)),
+            "p99_device_ms": float(np.percentile(dev, 99)),
+            "offered_span_s": reqs[-1].arrival_s,
+            "server": {"peak_lanes": st.peak_lanes, "peak_gb": st.peak_bytes / 2**30,
+                       "graphs": st.graphs, "ticks": st.ticks, "rebuilds": st.rebuilds},
+        },
+        "roofline": {"kernel": "whole served stream (evaluations + updates)", "bound": "fp64",
+                     "achieved": flops / span / 1e12, "peak": peak, "unit": "TFLOP/s",
+                     "frac": flops / span / 1e12 / peak if peak else None},
+        "clocks": clocks,
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def run_profile(args) -> None:
     """Kernel-level profiling driver (run under ncu): no timing, no JSON."""
     import torch
@@ -362,9 +523,20 @@ def main() -> None:
     ap.add_argument("--profile", choices=["eval", "relax"], default=None,
                     help="profiling driver for ncu: run the kernels only")  # fmt: skip
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--workload", choices=["batch", "mixed", "serve"], default="batch",
+                    help="batch: the headline 256-lane d2 N1000 relax; mixed: the 512-instance "
+                         "mixed-size ensemble; serve: a Poisson request stream")  # fmt: skip
+    ap.add_argument("--mixed-count", type=int, default=512)
+    ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--serve-count", type=int, default=200)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
     args = ap.parse_args()
     if args.profile:
         run_profile(args)
+    elif args.workload == "mixed" and args.impl == "cco":
+        run_mixed(args)
+    elif args.workload == "serve" and args.impl == "cco":
+        run_serve(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
