@@ -422,6 +422,7 @@ struct EvalWS {
     plan.max_d = p->d;
     plan.smem1 = p->smem1;
     plan.smem2 = p->smem2;
+    plan.red_chunks = reduce_chunks(p->M);
     plan.want_grad = g != nullptr;
     return cudaGetLastError();
   }

@@ -296,15 +296,21 @@ __global__ void __launch_bounds__(kPass1Threads, 4) k_pass1(EvalPlan plan) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_reduce(EvalPlan plan) {
+// Reduction (grid: k-chunks x lanes): rho_k = sum over tiles of the pass-1
+// partials in tile order, the weighted density for pass 2, and this chunk's
+// part of sum w |rho|^2, stored over the chunk's first partial (which only
+// this block reads).
+__global__ void __launch_bounds__(kReduceChunk) k_reduce(EvalPlan plan) {
   __shared__ double red[32];
-  const EvalLane ln = plan.lanes[blockIdx.x];
+  const EvalLane ln = plan.lanes[blockIdx.y];
   if (!lane_active(ln.status)) return;
   const ProbDev& P = plan.probs[ln.prob];
   const int M = P.M, nt = P.ntile1;
-  const double* __restrict__ w = P.w_run;
+  const int k0 = blockIdx.x * kReduceChunk;
+  if (k0 >= M) return;
+  const int k = k0 + threadIdx.x;
   double e = 0.0;
-  for (int k = threadIdx.x; k < M; k += blockDim.x) {
+  if (k < M) {
     double2 t = ln.part[k];
     for (int q = 1; q < nt; ++q) {
       const double2 o = ln.part[(size_t)q * M + k];
@@ -312,11 +318,24 @@ __global__ void __launch_bounds__(256) k_reduce(EvalPlan plan) {
       t.y += o.y;
     }
     ln.rho[k] = t;
-    const double wk = w[k];
+    const double wk = P.w_run[k];
     ln.rhow[k] = make_double2(wk * t.x, wk * t.y);
-    e += wk * (t.x * t.x + t.y * t.y);
+    e = wk * (t.x * t.x + t.y * t.y);
   }
   e = block_sum(e, red);
+  if (threadIdx.x == 0) ln.part[k0] = make_double2(e, 0.0);
+}
+
+// Energy (one warp per lane): the chunk energies summed in a fixed order.
+__global__ void k_energy(EvalPlan plan) {
+  const EvalLane ln = plan.lanes[blockIdx.x];
+  if (!lane_active(ln.status)) return;
+  const ProbDev& P = plan.probs[ln.prob];
+  const int nc = reduce_chunks(P.M);
+  double e = 0.0;
+  for (int c = threadIdx.x; c < nc; c += 32) e += ln.part[(size_t)c * kReduceChunk].x;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
   if (threadIdx.x == 0) *ln.f = e / P.vol;
 }
 
@@ -386,7 +405,10 @@ cudaError_t eval_configure() {
 
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream) {
   if (plan.n_items1 > 0) k_pass1<<<plan.n_items1, kPass1Threads, plan.smem1, stream>>>(plan);
-  if (plan.n_lanes > 0) k_reduce<<<plan.n_lanes, 256, 0, stream>>>(plan);
+  if (plan.n_lanes > 0) {
+    k_reduce<<<dim3(plan.red_chunks, plan.n_lanes), kReduceChunk, 0, stream>>>(plan);
+    k_energy<<<plan.n_lanes, 32, 0, stream>>>(plan);
+  }
   if (plan.want_grad && plan.n_items2 > 0)
     k_pass2<<<plan.n_items2, kPass2Threads, plan.smem2, stream>>>(plan);
   return cudaGetLastError();

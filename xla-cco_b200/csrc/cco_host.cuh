@@ -137,7 +137,7 @@ struct EvalSet {
     std::vector<EvalLane> lv;
     std::vector<EvalItem> i1, i2;
     size_t smem1 = 0, smem2 = 0;
-    int max_d = 1;
+    int max_d = 1, max_m = 1;
     for (int i = lo; i < hi; ++i) {
       const cco_problem* p = probs_of[i];
       int u = 0;
@@ -148,6 +148,7 @@ struct EvalSet {
         smem1 = std::max(smem1, p->smem1);
         smem2 = std::max(smem2, p->smem2);
         max_d = std::max(max_d, p->d);
+        max_m = std::max(max_m, p->M);
       }
       const int j = i - lo;
       lv.push_back(eval_lane(R, refs[i], p, u));
@@ -168,6 +169,7 @@ struct EvalSet {
     plan.max_d = max_d;
     plan.smem1 = smem1;
     plan.smem2 = smem2;
+    plan.red_chunks = reduce_chunks(max_m);
     plan.want_grad = true;
     return e;
   }
@@ -237,12 +239,14 @@ struct TickPlan {
 
 struct RunStats {
   int64_t ticks = 0, launches = 0;
-  Schedule schedule;
+  Schedule schedule;     // of the first (full) table
+  int compactions = 0;   // lane-table compactions
 };
 
 // Runs tick graphs until no lane of T is RUNNING (CCO_ERR_ROUNDS past
-// max_ticks). The schedule is forced by CCO_BRANCHES / CCO_GRAPH_TICKS,
-// cached for the shape class, or tuned online on the live lanes.
+// max_ticks), compacting the lane table as lanes finish. The schedule is
+// forced by CCO_BRANCHES / CCO_GRAPH_TICKS, cached for the shape class, or
+// tuned online on the live lanes; CCO_COMPACT=0 keeps the full table.
 int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* stats);
 
 // L-BFGS settings -> kernel arguments and record shape.

@@ -118,9 +118,18 @@ struct EvalPlan {
   const EvalItem* items2;   // device
   int n_lanes, n_items1, n_items2;
   int max_d;                // largest d in the plan (template dispatch)
+  int red_chunks;           // k-chunks of the reduction: ceil(max M / kReduceChunk)
   size_t smem1, smem2;      // dynamic shared memory of pass 1 / pass 2
   bool want_grad;
 };
+
+// The reduction of the pass-1 partials runs one block per kReduceChunk
+// k-vectors of a lane; a second kernel sums the chunks' energies in a fixed
+// order, so the energy's rounding depends on M alone.
+constexpr int kReduceChunk = 256;
+__host__ __device__ __forceinline__ int reduce_chunks(int M) {
+  return (M + kReduceChunk - 1) / kReduceChunk;
+}
 
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream);
 size_t eval_smem1(const ProbDev& p);

@@ -59,13 +59,13 @@ __device__ void descent_record(const DescentArgs& a, int lane, const LaneRef& R,
   if (a.traj_count == nullptr) return;
   __shared__ int64_t row;
   if (threadIdx.x == 0) {
-    const int64_t c = a.traj_count[lane];
+    const int64_t c = a.traj_count[R.idx];
     row = ((it % a.rec_every) == 0 && c < a.rec_cap) ? c : -1;
     if (row >= 0) {
-      a.traj_e[lane * a.rec_cap + row] = f;
-      a.traj_step[lane * a.rec_cap + row] = step;
-      a.traj_it[lane * a.rec_cap + row] = it;
-      a.traj_count[lane] = c + 1;
+      a.traj_e[R.idx * a.rec_cap + row] = f;
+      a.traj_step[R.idx * a.rec_cap + row] = step;
+      a.traj_it[R.idx * a.rec_cap + row] = it;
+      a.traj_count[R.idx] = c + 1;
     }
   }
   __syncthreads();
@@ -93,7 +93,7 @@ __global__ void k_descent_init(DescentArgs a, const double* __restrict__ s0) {
     S.step = a.step_init;
     S.t0 = gtimer();
     *v.st = S;
-    if (a.traj_count) a.traj_count[lane] = 0;
+    if (a.traj_count) a.traj_count[R.idx] = 0;
   }
 }
 
@@ -305,14 +305,14 @@ __device__ void lb_record(const LbArgs& A, int lane, const LaneRef& R, LbShared&
   if (A.traj_count == nullptr) return;
   __shared__ int64_t row;
   if (threadIdx.x == 0) {
-    const int64_t c = A.traj_count[lane];
+    const int64_t c = A.traj_count[R.idx];
     const int64_t it = sh.L.it;
     row = ((it % A.rec_every) == 0 && c < A.rec_cap) ? c : -1;
     if (row >= 0) {
-      A.traj_e[lane * A.rec_cap + row] = sh.L.f;
-      A.traj_step[lane * A.rec_cap + row] = sh.L.last_step;
-      A.traj_it[lane * A.rec_cap + row] = it;
-      A.traj_count[lane] = c + 1;
+      A.traj_e[R.idx * A.rec_cap + row] = sh.L.f;
+      A.traj_step[R.idx * A.rec_cap + row] = sh.L.last_step;
+      A.traj_it[R.idx * A.rec_cap + row] = it;
+      A.traj_count[R.idx] = c + 1;
     }
   }
   __syncthreads();
@@ -441,7 +441,7 @@ __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
     L.R = A.rescales[0];
     L.t0 = gtimer();
     *v.st = L;
-    if (A.traj_count) A.traj_count[lane] = 0;
+    if (A.traj_count) A.traj_count[R.idx] = 0;
   }
 }
 

@@ -20,6 +20,8 @@ struct LaneRef {
   int nd, ld;       // N d, and N d rounded up to a multiple of 4 doubles
   int64_t soff;     // offset of the lane in the caller's packed positions
   int64_t toff;     // offset of the lane's trajectory rows in traj_s
+  int32_t idx;      // the lane's index in the call: its row of traj_e/step/it/count
+  int32_t pad_;
 };
 
 __host__ __device__ __forceinline__ int pad4(int nd) { return (nd + 3) & ~3; }
@@ -68,7 +70,7 @@ struct DescentArgs {
   double step_init, step_min, shrink, grow, rel_tol, energy_tol;
   int64_t max_iters;      // max_evals // 2
   int64_t rec_every, rec_cap;
-  // trajectory (null when off): traj_e/step/it/count indexed by lane, traj_s by toff
+  // trajectory (null when off): traj_e/step/it/count rows by LaneRef::idx, traj_s by toff
   double *traj_s, *traj_e, *traj_step;
   int64_t *traj_it, *traj_count;
 };

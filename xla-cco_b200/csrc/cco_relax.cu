@@ -102,24 +102,12 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
       DescentArgs a = T.ds;
       a.B = hi - lo;
       a.lanes = T.d_refs + lo;
-      if (a.traj_count) {
-        a.traj_e += (size_t)lo * a.rec_cap;
-        a.traj_step += (size_t)lo * a.rec_cap;
-        a.traj_it += (size_t)lo * a.rec_cap;
-        a.traj_count += lo;
-      }
       ds[b] = a;
     } else {
       LbArgs a = T.lb;
       a.B = hi - lo;
       a.lanes = T.d_refs + lo;
       a.nblkB = nblk;
-      if (a.traj_count) {
-        a.traj_e += (size_t)lo * a.rec_cap;
-        a.traj_step += (size_t)lo * a.rec_cap;
-        a.traj_it += (size_t)lo * a.rec_cap;
-        a.traj_count += lo;
-      }
       lb[b] = a;
     }
   }
@@ -171,7 +159,7 @@ cudaError_t TickPlan::tick(cudaStream_t s, int b) const {
 }
 
 int TickPlan::launches_per_tick() const {
-  return nbr * (method == Method::Descent ? 4 : 7);
+  return nbr * (method == Method::Descent ? 5 : 8);  // 4 evaluation kernels + the update
 }
 
 void TickPlan::release(cudaStream_t st) {
@@ -209,91 +197,175 @@ std::vector<Schedule> candidates(int B) {
   return c;
 }
 
+// Pinned host buffer owned by the calling thread, grown on demand
+// (cudaHostAlloc is slow and may synchronize, so it stays out of most calls).
+int64_t* pinned_status(size_t count) {
+  static thread_local int64_t* buf = nullptr;
+  static thread_local size_t cap = 0;
+  if (count > cap) {
+    if (buf) cudaFreeHost(buf);
+    buf = nullptr;
+    cap = 0;
+    const size_t n = std::max<size_t>(count, 4096);
+    if (cudaHostAlloc(reinterpret_cast<void**>(&buf), n * sizeof(int64_t), cudaHostAllocDefault) !=
+        cudaSuccess)
+      return nullptr;
+    cap = n;
+  }
+  return buf;
+}
+
+// Online tuning: one graph per candidate on the live lanes C, timed with
+// events, then the fastest per tick. Every candidate advances every lane by
+// the same ticks, so results do not depend on which schedule wins.
+int tune_schedule(const LaneTable& C, cudaStream_t st, int64_t max_ticks, int64_t* ticks,
+                  int64_t* launches, Schedule* out) {
+  const std::vector<Schedule> cand = candidates((int)C.refs.size());
+  std::vector<cudaEvent_t> t0(cand.size(), nullptr), t1(cand.size(), nullptr);
+  std::vector<float> ms(cand.size(), 1e30f);
+  int rc = CCO_OK;
+  cudaError_t e = cudaSuccess;
+  for (size_t c = 0; c < cand.size() && e == cudaSuccess; ++c) {
+    e = cudaEventCreate(&t0[c]);
+    if (e == cudaSuccess) e = cudaEventCreate(&t1[c]);
+  }
+  for (size_t c = 0; c < cand.size() && rc == CCO_OK && e == cudaSuccess && *ticks < max_ticks; ++c) {
+    TickPlan P;
+    P.method = C.shape.method;
+    rc = P.build(C, cand[c], st);
+    if (rc != CCO_OK) break;
+    e = cudaEventRecord(t0[c], st);
+    if (e == cudaSuccess) e = cudaGraphLaunch(P.exec, st);
+    if (e == cudaSuccess) e = cudaEventRecord(t1[c], st);
+    *ticks += cand[c].graph_ticks;
+    *launches += (int64_t)cand[c].graph_ticks * P.launches_per_tick();
+    P.release(st);
+  }
+  if (rc == CCO_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+  int best = 0;
+  for (size_t c = 0; c < cand.size() && e == cudaSuccess && rc == CCO_OK; ++c) {
+    float v = 0.f;
+    if (cudaEventElapsedTime(&v, t0[c], t1[c]) == cudaSuccess) ms[c] = v / cand[c].graph_ticks;
+    else cudaGetLastError();
+    if (ms[c] < ms[best]) best = (int)c;
+  }
+  for (size_t c = 0; c < cand.size(); ++c) {
+    if (t0[c]) cudaEventDestroy(t0[c]);
+    if (t1[c]) cudaEventDestroy(t1[c]);
+  }
+  if (rc != CCO_OK) return rc;
+  if (e != cudaSuccess) return cuda_fail(e, "schedule tuning");
+  Schedule s = cand[best];
+  // graphs of about 3 ms of device work: launch overhead amortised, and the
+  // few graphs that run past the last lane's completion stay short
+  const double tick_ms = ms[best] < 1e29f ? ms[best] : 0.2;
+  const int gt = (int)std::lround(3.0 / std::max(tick_ms, 1e-3));
+  s.graph_ticks = std::max(4, std::min(32, gt));
+  *out = s;
+  return CCO_OK;
+}
+
 }  // namespace
 
+// The tick driver. Graphs run on a lane table C that starts as all of T and
+// is compacted - rebuilt from the lanes a status snapshot shows RUNNING -
+// whenever at most half of it still runs, so finished lanes stop costing
+// launch slots (the reference's per-round compaction of active lanes,
+// minimize/__init__.py:75-99, without moving any lane's state). Each
+// compaction looks up or re-tunes the schedule for the smaller table.
 int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* stats) {
   const int B = (int)T.refs.size();
   constexpr int kSlots = kInflight + 1;
-  int* d_count = nullptr;
-  // pinned completion counters: allocated once per host thread (cudaMallocHost
-  // is slow and may synchronize, so it stays out of every call)
-  static thread_local int* h_count = nullptr;
-  CCO_CUDA(pool_alloc(&d_count, kSlots * sizeof(int), st));
-  if (h_count == nullptr) CCO_CUDA(cudaMallocHost(&h_count, kSlots * sizeof(int)));
+  int64_t* d_status = nullptr;
+  int64_t* h_status = pinned_status((size_t)kSlots * B);
+  if (!h_status) return fail(CCO_ERR_OOM, "pinned status buffer");
+  CCO_CUDA(pool_alloc(&d_status, sizeof(int64_t) * kSlots * B, st));
   cudaEvent_t ev[kSlots];
+  int ver[kSlots] = {}, rows[kSlots] = {};
   for (int i = 0; i < kSlots; ++i) CCO_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
   int64_t ticks = 0, launches = 0;
   int rc = CCO_OK;
   cudaError_t e = cudaSuccess;
   bool done = false;
 
-  // Schedule: forced by the environment, cached for this shape class, or
-  // tuned online. Tuning runs one graph per candidate on the live lanes;
-  // every candidate advances every lane by the same ticks, so the results
-  // do not depend on which schedule wins.
-  Schedule chosen;
   const int force_br = env_int("CCO_BRANCHES", 0), force_gt = env_int("CCO_GRAPH_TICKS", 0);
   const bool tune = env_int("CCO_AUTOTUNE", 1) != 0;
-  bool have = false;
-  if (force_br > 0 || force_gt > 0) {
-    if (force_br > 0) chosen.branches = force_br;
-    if (force_gt > 0) chosen.graph_ticks = force_gt;
-    have = true;
-  } else if (schedule_cached(T.probs, T.shape.method, &chosen) || !tune) {
-    have = true;
-  }
-  if (!have) {
-    const std::vector<Schedule> cand = candidates(B);
-    std::vector<cudaEvent_t> t0(cand.size()), t1(cand.size());
-    std::vector<float> ms(cand.size(), 1e30f);
-    for (size_t c = 0; c < cand.size(); ++c) {
-      cudaEventCreate(&t0[c]);
-      cudaEventCreate(&t1[c]);
-    }
-    for (size_t c = 0; c < cand.size() && rc == CCO_OK && ticks < max_ticks; ++c) {
-      TickPlan P;
-      P.method = T.shape.method;
-      rc = P.build(T, cand[c], st);
-      if (rc != CCO_OK) break;
-      e = cudaEventRecord(t0[c], st);
-      if (e == cudaSuccess) e = cudaGraphLaunch(P.exec, st);
-      if (e == cudaSuccess) e = cudaEventRecord(t1[c], st);
-      ticks += cand[c].graph_ticks;
-      launches += (int64_t)cand[c].graph_ticks * P.launches_per_tick();
-      P.release(st);
-      if (e != cudaSuccess) break;
-    }
-    if (rc == CCO_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
-    int best = 0;
-    for (size_t c = 0; c < cand.size() && e == cudaSuccess && rc == CCO_OK; ++c) {
-      float t = 0.f;
-      if (cudaEventElapsedTime(&t, t0[c], t1[c]) == cudaSuccess) ms[c] = t / cand[c].graph_ticks;
-      if (ms[c] < ms[best]) best = (int)c;
-    }
-    for (size_t c = 0; c < cand.size(); ++c) {
-      cudaEventDestroy(t0[c]);
-      cudaEventDestroy(t1[c]);
-    }
-    chosen = cand[best];
-    // graphs of about 3 ms of device work: launch overhead amortised, and the
-    // few graphs that run past the last lane's completion stay short
-    const double tick_ms = ms[best] < 1e29f ? ms[best] : 0.2;
-    int gt = (int)std::lround(3.0 / std::max(tick_ms, 1e-3));
-    chosen.graph_ticks = std::max(4, std::min(32, gt));
-    if (rc == CCO_OK && e == cudaSuccess) schedule_store(T.probs, T.shape.method, chosen);
-    // tuning may already have finished every lane
-    if (rc == CCO_OK && e == cudaSuccess) {
-      e = count_running(T.d_refs, B, d_count, st);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(h_count, d_count, sizeof(int), cudaMemcpyDeviceToHost, st);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-      if (e == cudaSuccess && h_count[0] == 0) done = true;
-    }
-  }
+  const bool compact = env_int("CCO_COMPACT", 1) != 0;
 
+  LaneTable C;           // the live table (owns its own device copy of refs)
+  C.shape = T.shape;
+  C.ds = T.ds;
+  C.lb = T.lb;
+  C.refs = T.refs;
+  C.probs = T.probs;
+  Schedule chosen, first;
+  bool first_set = false;
   TickPlan P;
   P.method = T.shape.method;
-  if (rc == CCO_OK && e == cudaSuccess && !done) rc = P.build(T, chosen, st);
+  int version = 0;
+
+  // (re)start on table C: schedule, graph
+  auto start = [&]() -> int {
+    int r = C.upload_refs(st);
+    if (r != CCO_OK) return r;
+    C.ds.lanes = C.d_refs;
+    C.ds.B = (int)C.refs.size();
+    C.lb.lanes = C.d_refs;
+    C.lb.B = (int)C.refs.size();
+    Schedule s;
+    if (force_br > 0 || force_gt > 0) {
+      if (force_br > 0) s.branches = force_br;
+      if (force_gt > 0) s.graph_ticks = force_gt;
+    } else if (!schedule_cached(C.probs, C.shape.method, &s) && tune) {
+      r = tune_schedule(C, st, max_ticks, &ticks, &launches, &s);
+      if (r != CCO_OK) return r;
+      schedule_store(C.probs, C.shape.method, s);
+    }
+    chosen = s;
+    if (!first_set) {
+      first = s;
+      first_set = true;
+    }
+    ++version;
+    return P.build(C, chosen, st);
+  };
+  rc = start();
+
   int launched = 0, checked = 0;
+  auto land = [&]() -> int {
+    const int slot = checked % kSlots;
+    CCO_CUDA(cudaEventSynchronize(ev[slot]));
+    ++checked;
+    const int64_t* h = h_status + (size_t)slot * B;
+    int running = 0;
+    for (int i = 0; i < rows[slot]; ++i) running += h[i] == CCO_STATUS_RUNNING;
+    if (running == 0) {
+      done = true;
+      return CCO_OK;
+    }
+    const int n = (int)C.refs.size();
+    if (!compact || ver[slot] != version || n < 2 || 2 * running > n) return CCO_OK;
+    // compaction: keep the lanes this snapshot of the current table shows running
+    std::vector<LaneRef> refs;
+    std::vector<const cco_problem*> probs;
+    for (int i = 0; i < n; ++i)
+      if (h[i] == CCO_STATUS_RUNNING) {
+        refs.push_back(C.refs[i]);
+        probs.push_back(C.probs[i]);
+      }
+    // drain the graphs still in flight on the old table first: their snapshots
+    // describe the old row order
+    while (checked < launched) {
+      const int s2 = checked % kSlots;
+      CCO_CUDA(cudaEventSynchronize(ev[s2]));
+      ++checked;
+    }
+    C.refs.swap(refs);
+    C.probs.swap(probs);
+    P.release(st);
+    return start();
+  };
+
   while (rc == CCO_OK && e == cudaSuccess && !done) {
     if (ticks >= max_ticks) break;
     e = cudaGraphLaunch(P.exec, st);
@@ -301,36 +373,33 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
     ticks += chosen.graph_ticks;
     launches += (int64_t)chosen.graph_ticks * P.launches_per_tick() + 1;
     const int slot = launched % kSlots;
-    e = count_running(T.d_refs, B, d_count + slot, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h_count + slot, d_count + slot, sizeof(int), cudaMemcpyDeviceToHost, st);
+    const int n = (int)C.refs.size();
+    e = gather_status(C.d_refs, n, d_status + (size_t)slot * B, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h_status + (size_t)slot * B, d_status + (size_t)slot * B,
+                          sizeof(int64_t) * n, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaEventRecord(ev[slot], st);
+    ver[slot] = version;
+    rows[slot] = n;
     ++launched;
-    if (e == cudaSuccess && launched - checked > kInflight) {
-      const int old = checked % kSlots;
-      e = cudaEventSynchronize(ev[old]);
-      ++checked;
-      if (e == cudaSuccess && h_count[old] == 0) done = true;
-    }
+    if (e == cudaSuccess && launched - checked > kInflight) rc = land();
   }
   // drain the launches still in flight, oldest first
-  while (rc == CCO_OK && e == cudaSuccess && !done && checked < launched) {
-    const int old = checked % kSlots;
-    e = cudaEventSynchronize(ev[old]);
-    ++checked;
-    if (e == cudaSuccess && h_count[old] == 0) done = true;
-  }
+  while (rc == CCO_OK && e == cudaSuccess && !done && checked < launched) rc = land();
   if (rc == CCO_OK) {
     if (e != cudaSuccess) rc = cuda_fail(e, "relax ticks");
     else if (!done) rc = fail(CCO_ERR_ROUNDS, "relax did not finish within the round bound (%lld ticks)", (long long)max_ticks);
   }
   P.release(st);
+  C.release(st);
   for (int i = 0; i < kSlots; ++i) cudaEventDestroy(ev[i]);
-  cudaFreeAsync(d_count, st);
+  cudaFreeAsync(d_status, st);
   cudaStreamSynchronize(st);
   if (stats) {
     stats->ticks = ticks;
     stats->launches = launches;
-    stats->schedule = chosen;
+    stats->schedule = first;
+    stats->compactions = version - 1;
   }
   return rc;
 }
@@ -380,6 +449,7 @@ int make_table(cco_problem* const* probs, int B, const RecordShape& shape, int64
     r.ld = pad4(r.nd);
     r.soff = soff;
     r.toff = cap * soff;
+    r.idx = i;
     o += record_doubles(shape, p);
     soff += r.nd;
   }
