@@ -278,8 +278,15 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   std::stable_sort(s2.begin(), s2.end(), by_len);
   P.nseg1 = (int)s1.size();
   P.nseg2 = (int)s2.size();
+  {
+    // logical pass-2 slices: about two segment pairs each, at most 8
+    const int npairs = (P.nseg2 + 1) / 2;
+    int sl = 1;
+    while (sl < 8 && 4 * sl <= npairs) sl *= 2;
+    P.sl2 = sl;
+  }
 
-  const size_t smem1 = eval_smem1(P), smem2 = eval_smem2(P);
+  const size_t smem1 = eval_smem1(P), smem2 = std::max(eval_smem2(P, 1), eval_smem2(P, 8));
   if (smem1 > 220 * 1024 || smem2 > 220 * 1024)
     return fail(CCO_ERR_ARG, "k-set phase tables too large for shared memory (%d / %d rows)",
                 P.t1.nrows, P.t2.nrows);
@@ -393,8 +400,12 @@ struct EvalWS {
   double2* part = nullptr;
   EvalPlan plan{};
 
+  // pass-2 threads per particle and tiles per configuration for a batch of B
+  static int split_for(const cco_problem* p, int B) {
+    return pass2_split((long long)B * p->host.ntile2);
+  }
   cudaError_t alloc(const cco_problem* p, int B, cudaStream_t st) {
-    const int M = p->M, nt1 = p->host.ntile1, nt2 = p->host.ntile2;
+    const int M = p->M, nt1 = p->host.ntile1, nt2 = pass2_tiles(p->host, split_for(p, B));
     cudaError_t e = pool_alloc(&lanes, sizeof(EvalLane) * B, st);
     if (e == cudaSuccess) e = pool_alloc(&it1, sizeof(EvalItem) * (size_t)B * nt1, st);
     if (e == cudaSuccess) e = pool_alloc(&it2, sizeof(EvalItem) * (size_t)B * nt2, st);
@@ -406,7 +417,8 @@ struct EvalWS {
   cudaError_t build(const cco_problem* p, int B, const double* s, size_t s_stride, double* f,
                     size_t f_stride, double* g, size_t g_stride, const int64_t* status,
                     size_t status_stride, cudaStream_t st) {
-    const int nt1 = p->host.ntile1, nt2 = p->host.ntile2;
+    const int split = split_for(p, B);
+    const int nt1 = p->host.ntile1, nt2 = pass2_tiles(p->host, split);
     const int total = B * std::max(nt1, nt2) + B;
     const int blocks = std::min(1024, (total + 255) / 256);
     k_make_lanes<<<blocks, 256, 0, st>>>(lanes, it1, it2, B, nt1, nt2, total, s, s_stride, f, f_stride,
@@ -421,7 +433,8 @@ struct EvalWS {
     plan.n_items2 = B * nt2;
     plan.max_d = p->d;
     plan.smem1 = p->smem1;
-    plan.smem2 = p->smem2;
+    plan.smem2 = eval_smem2(p->host, split);
+    plan.split2 = split;
     plan.red_chunks = reduce_chunks(p->M);
     plan.want_grad = g != nullptr;
     return cudaGetLastError();
@@ -499,7 +512,8 @@ extern "C" int cco_energy_grad_noalloc(cco_problem* p, void* stream, int batch, 
   if (batch == 0) return CCO_OK;
   if (!s || !phi) return fail(CCO_ERR_ARG, "null s or phi");
   const size_t B = (size_t)batch, M = (size_t)p->M;
-  const size_t nt1 = (size_t)p->host.ntile1, nt2 = (size_t)p->host.ntile2;
+  const size_t nt1 = (size_t)p->host.ntile1;
+  const size_t nt2 = (size_t)pass2_tiles(p->host, EvalWS::split_for(p, batch));
   const size_t b_lanes = round256(sizeof(EvalLane) * B);
   const size_t b_it1 = round256(sizeof(EvalItem) * B * nt1);
   const size_t b_it2 = round256(sizeof(EvalItem) * B * nt2);

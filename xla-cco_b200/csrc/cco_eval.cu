@@ -31,6 +31,7 @@
 //     w(Im rho cos - Re rho sin) and two accumulations; prefix axes are
 //     weighted once per segment.
 #include <cstdio>
+#include <cstdlib>
 
 #include "cco_internal.cuh"
 
@@ -212,35 +213,50 @@ __device__ __forceinline__ void bp_step(double2 r, double2& ph, double2 z, doubl
   ph = cmul(ph, z);
 }
 
-// STAGED: the lane's weighted density (M rows) is copied once into shared
-// memory after the tables and every row read is a shared-memory broadcast;
-// otherwise rows are read through L1 from global memory.
-template <int D, bool STAGED>
-__device__ void pass2_body(const ProbDev& P, const EvalLane& ln, int tile, double2* tab) {
-  const TabLayout& T = P.t2;
-  constexpr int S = kPass2Tile;
-  const int j0 = tile * kPass2Tile;
-  const int nj = min(kPass2Tile, P.N - j0);
-  const double2* __restrict__ rw = ln.rhow;
-  if (STAGED) {
-    double2* st = tab + (size_t)T.nrows * S;
-    for (int k = threadIdx.x; k < P.M; k += blockDim.x) st[k] = rw[k];
-    rw = st;
+// Pairwise (tree) sum of D-vectors pushed in order: push i merges with the
+// partial sums of its completed subtrees, so a power-of-two count n of
+// leaves always sums as the same balanced tree, whichever threads produced
+// the leaves. Depth <= 4 (16 leaves).
+template <int D>
+struct Pairwise {
+  double st[4][D];
+  int n = 0;
+  __device__ __forceinline__ void push(const double (&v)[D]) {
+    double cur[D];
+#pragma unroll
+    for (int a = 0; a < D; ++a) cur[a] = v[a];
+    int lvl = 0;
+    for (int c = n; c & 1; c >>= 1, ++lvl) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) cur[a] = st[lvl][a] + cur[a];
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) st[lvl][a] = cur[a];
+    ++n;
   }
-  build_tables<D>(T, ln.s, j0, nj, kPass2Tile, S, tab);
-  const Levels<D> L = levels<D>(T);
-  __syncthreads();
-  const int j = threadIdx.x;
-  const double2 z = tab[T.zrow * S + j];
-  double G[D];
+  // total of a power-of-two count of leaves
+  __device__ __forceinline__ void total(double (&out)[D]) const {
+    int lvl = 0;
+    while ((1 << lvl) < n) ++lvl;
+#pragma unroll
+    for (int a = 0; a < D; ++a) out[a] = st[lvl][a];
+  }
+};
+
+// Gradient contribution of logical slice q: segment pairs q, q + sl, ...
+template <int D>
+__device__ __forceinline__ void pass2_slice(const ProbDev& P, const Levels<D>& L,
+                                            const double2* __restrict__ rw, const double2* tab,
+                                            int stride, int j, double2 z, int q, int sl,
+                                            double (&G)[D]) {
+  const int nseg = P.nseg2;
 #pragma unroll
   for (int a = 0; a < D; ++a) G[a] = 0.0;
-  const int nseg = P.nseg2;
-  for (int sg = 0; sg < nseg; sg += 2) {
+  for (int sg = 2 * q; sg < nseg; sg += 2 * sl) {
     const SegHdr hA = P.seg2[sg];
     const SegHdr hB = P.seg2[min(sg + 1, nseg - 1)];
-    double2 pA = start_phase<D>(L, hA, tab, S, j);
-    double2 pB = start_phase<D>(L, hB, tab, S, j);
+    double2 pA = start_phase<D>(L, hA, tab, stride, j);
+    double2 pB = start_phase<D>(L, hB, tab, stride, j);
     double SA = 0.0, TA = 0.0, SB = 0.0, TB = 0.0;
     const double2* rA = rw + hA.kstart;
     const double2* rB = rw + hB.kstart;
@@ -274,10 +290,74 @@ __device__ void pass2_body(const ProbDev& P, const EvalLane& ln, int tile, doubl
     for (int a = 0; a < D - 1; ++a) G[a] += (double)hA.n[a] * SA + (double)hB.n[a] * SB;
     G[D - 1] += ((double)hA.n[D - 1] * SA + TA) + ((double)hB.n[D - 1] * SB + TB);
   }
-  if (j < nj) {
-    double* gj = ln.g + (size_t)(j0 + j) * D;
+}
+
+// Pass 2 of one particle tile. The segment pairs of a problem form P.sl2
+// logical slices (slice q: pairs q, q + sl2, ...) whose gradients are summed
+// as a balanced tree, so the result depends on the problem alone. `split`
+// (a launch choice) sets how many threads share one particle: a CTA holds
+// kPass2Tile / split particles and each of a particle's split threads
+// evaluates a contiguous block of slices; the tree's top levels are then
+// finished in shared memory. STAGED: the lane's weighted density (M rows) is
+// copied once into shared memory after the tables and every row read is a
+// shared-memory broadcast; otherwise rows are read through L1.
+template <int D, bool STAGED>
+__device__ void pass2_body(const ProbDev& P, const EvalLane& ln, int tile, int split,
+                           double2* tab) {
+  const TabLayout& T = P.t2;
+  const int tw = kPass2Tile / split;
+  const int j0 = tile * tw;
+  const int nj = min(tw, P.N - j0);
+  const double2* __restrict__ rw = ln.rhow;
+  double2* after = tab + (size_t)T.nrows * tw;
+  if (STAGED) {
+    for (int k = threadIdx.x; k < P.M; k += blockDim.x) after[k] = rw[k];
+    rw = after;
+    after += P.M;
+  }
+  double* comb = reinterpret_cast<double*>(after);   // [split][tw][D]
+  build_tables<D>(T, ln.s, j0, nj, tw, tw, tab);
+  const Levels<D> L = levels<D>(T);
+  __syncthreads();
+  const int j = threadIdx.x % tw, qp = threadIdx.x / tw;
+  const double2 z = tab[T.zrow * tw + j];
+  const int sl = P.sl2;
+  const int per = sl > split ? sl / split : 1;    // slices per thread
+  const int nblk = sl / per;                      // threads of a particle that have slices
+  if (qp < nblk) {
+    Pairwise<D> acc;
+    for (int q = qp * per; q < (qp + 1) * per; ++q) {
+      double G[D];
+      pass2_slice<D>(P, L, rw, tab, tw, j, z, q, sl, G);
+      acc.push(G);
+    }
+    double G[D];
+    acc.total(G);
+    if (nblk > 1) {
 #pragma unroll
-    for (int a = 0; a < D; ++a) gj[a] = P.gpref * G[a];
+      for (int a = 0; a < D; ++a) comb[((size_t)qp * tw + j) * D + a] = G[a];
+    } else if (j < nj) {
+      double* gj = ln.g + (size_t)(j0 + j) * D;
+#pragma unroll
+      for (int a = 0; a < D; ++a) gj[a] = P.gpref * G[a];
+    }
+  }
+  if (nblk > 1) {
+    __syncthreads();
+    if (qp == 0 && j < nj) {
+      Pairwise<D> acc;
+      for (int b = 0; b < nblk; ++b) {
+        double G[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) G[a] = comb[((size_t)b * tw + j) * D + a];
+        acc.push(G);
+      }
+      double G[D];
+      acc.total(G);
+      double* gj = ln.g + (size_t)(j0 + j) * D;
+#pragma unroll
+      for (int a = 0; a < D; ++a) gj[a] = P.gpref * G[a];
+    }
   }
 }
 
@@ -350,15 +430,15 @@ __global__ void __launch_bounds__(kPass2Threads, 4) k_pass2(EvalPlan plan) {
   const bool staged = (size_t)sp.M * sizeof(double2) <= kPass2RhoStage;
   if (staged) {
     switch (sp.d) {
-      case 1: pass2_body<1, true>(sp, ln, it.tile, smem); break;
-      case 2: pass2_body<2, true>(sp, ln, it.tile, smem); break;
-      default: pass2_body<3, true>(sp, ln, it.tile, smem); break;
+      case 1: pass2_body<1, true>(sp, ln, it.tile, plan.split2, smem); break;
+      case 2: pass2_body<2, true>(sp, ln, it.tile, plan.split2, smem); break;
+      default: pass2_body<3, true>(sp, ln, it.tile, plan.split2, smem); break;
     }
   } else {
     switch (sp.d) {
-      case 1: pass2_body<1, false>(sp, ln, it.tile, smem); break;
-      case 2: pass2_body<2, false>(sp, ln, it.tile, smem); break;
-      default: pass2_body<3, false>(sp, ln, it.tile, smem); break;
+      case 1: pass2_body<1, false>(sp, ln, it.tile, plan.split2, smem); break;
+      case 2: pass2_body<2, false>(sp, ln, it.tile, plan.split2, smem); break;
+      default: pass2_body<3, false>(sp, ln, it.tile, plan.split2, smem); break;
     }
   }
 }
@@ -390,9 +470,26 @@ size_t eval_smem1(const ProbDev& p) {
   return ((size_t)p.t1.nrows * kPass1Stride + red) * sizeof(double2);
 }
 
-size_t eval_smem2(const ProbDev& p) {
+size_t eval_smem2(const ProbDev& p, int split) {
   const size_t rho = (size_t)p.M * sizeof(double2);
-  return (size_t)p.t2.nrows * kPass2Tile * sizeof(double2) + (rho <= kPass2RhoStage ? rho : 0);
+  const size_t comb = split > 1 ? (size_t)kPass2Tile * p.d * sizeof(double) : 0;
+  return (size_t)p.t2.nrows * (kPass2Tile / split) * sizeof(double2) +
+         (rho <= kPass2RhoStage ? rho : 0) + comb;
+}
+
+int pass2_tiles(const ProbDev& p, int split) {
+  const int tw = kPass2Tile / split;
+  return (p.N + tw - 1) / tw;
+}
+
+int pass2_split(long long tiles_at_split1) {
+  if (const char* env = getenv("CCO_PASS2_SPLIT")) {
+    const int s = atoi(env);
+    if (s == 1 || s == 2 || s == 4 || s == 8) return s;
+  }
+  int split = 1;
+  while (split < 8 && tiles_at_split1 * split < kPass2TargetCtas) split *= 2;
+  return split;
 }
 
 cudaError_t eval_configure() {

@@ -132,6 +132,9 @@ struct EvalSet {
   cudaError_t build(const RecordShape& R, const std::vector<LaneRef>& refs,
                     const std::vector<const cco_problem*>& probs_of, int lo, int hi,
                     cudaStream_t st) {
+    long long tiles1 = 0;
+    for (int i = lo; i < hi; ++i) tiles1 += probs_of[i]->host.ntile2;
+    const int split = pass2_split(tiles1);
     std::vector<const cco_problem*> uniq;
     std::vector<ProbDev> pv;
     std::vector<EvalLane> lv;
@@ -146,14 +149,15 @@ struct EvalSet {
         uniq.push_back(p);
         pv.push_back(p->host);
         smem1 = std::max(smem1, p->smem1);
-        smem2 = std::max(smem2, p->smem2);
+        smem2 = std::max(smem2, eval_smem2(p->host, split));
         max_d = std::max(max_d, p->d);
         max_m = std::max(max_m, p->M);
       }
       const int j = i - lo;
       lv.push_back(eval_lane(R, refs[i], p, u));
       for (int t = 0; t < p->host.ntile1; ++t) i1.push_back(EvalItem{j, t});
-      for (int t = 0; t < p->host.ntile2; ++t) i2.push_back(EvalItem{j, t});
+      const int nt2 = pass2_tiles(p->host, split);
+      for (int t = 0; t < nt2; ++t) i2.push_back(EvalItem{j, t});
     }
     cudaError_t e = upload(&probs, pv, st);
     if (e == cudaSuccess) e = upload(&lanes, lv, st);
@@ -170,6 +174,7 @@ struct EvalSet {
     plan.smem1 = smem1;
     plan.smem2 = smem2;
     plan.red_chunks = reduce_chunks(max_m);
+    plan.split2 = split;
     plan.want_grad = true;
     return e;
   }

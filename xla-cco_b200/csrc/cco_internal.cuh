@@ -57,7 +57,8 @@ struct TabLayout {
 struct ProbDev {
   int d, N, M, nseg1, nseg2;
   TabLayout t1, t2;          // pass-1 / pass-2 table layouts
-  int ntile1, ntile2;        // particle tiles of pass 1 / pass 2
+  int ntile1, ntile2;        // particle tiles of pass 1 / pass 2 (pass 2 at split 1)
+  int sl2;                   // logical slices of the pass-2 segment pairs (power of 2, <= 8)
   double vol;                // V
   double gpref;              // 2 (2 pi) / V
   const SegHdr* seg1;
@@ -119,6 +120,7 @@ struct EvalPlan {
   int n_lanes, n_items1, n_items2;
   int max_d;                // largest d in the plan (template dispatch)
   int red_chunks;           // k-chunks of the reduction: ceil(max M / kReduceChunk)
+  int split2;               // pass-2 threads per particle (1, 2, 4 or 8)
   size_t smem1, smem2;      // dynamic shared memory of pass 1 / pass 2
   bool want_grad;
 };
@@ -133,7 +135,15 @@ __host__ __device__ __forceinline__ int reduce_chunks(int M) {
 
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream);
 size_t eval_smem1(const ProbDev& p);
-size_t eval_smem2(const ProbDev& p);
+size_t eval_smem2(const ProbDev& p, int split);
+// Pass-2 tiles of one configuration when `split` threads share a particle.
+int pass2_tiles(const ProbDev& p, int split);
+// Threads per particle in pass 2 for a launch whose configurations have
+// `tiles_at_split1` tiles in total at split 1: the smallest power of two
+// (<= 8) that gives kPass2TargetCtas CTAs (CCO_PASS2_SPLIT overrides).
+// It changes how work is spread, never the arithmetic.
+constexpr long long kPass2TargetCtas = 148 * 3;
+int pass2_split(long long tiles_at_split1);
 cudaError_t eval_configure();   // opt-in to large dynamic shared memory
 
 // Copy the run-order density of lane i out in the caller's row order.
