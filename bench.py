@@ -425,6 +425,77 @@ def run_mixed(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ precision
+def run_precision(args) -> None:
+    """d=3 N=4000 chi=0.45 batch 64: plain FP64 vs mixed precision, same seeds."""
+    import oracle
+    import torch
+
+    from xla_cco import LBFGSSettings
+    from xla_cco.minimize import relax_device
+    from xla_cco.workloads import energy_for
+
+    torch.cuda.set_device(0)
+    n, d, chi, b = 4000, 3, 0.45, args.precision_batch
+    en = energy_for(n, d, chi)
+    box_vol = float(n)  # cubic unit-density box
+    s0 = torch.from_numpy(np.random.default_rng(SEED).uniform(size=(b, n, d))).cuda()
+    stream = torch.cuda.current_stream()
+    out = {}
+    sampler = ClockSampler(0)
+    sampler.start()
+    for name, prec in (("fp64", "fp64"), ("mixed", "mixed")):
+        st = LBFGSSettings(energy_tol=TOL, precision=prec)
+        for _ in range(args.warmup):
+            relax_device(en, s0, st)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        runs = [relax_device(en, s0, st) for _ in range(args.steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        r = runs[-1]
+        ok = (r["energy"] < TOL).cpu().numpy()
+        out[name] = {"ms": ms / args.steps, "ok": ok, "energy": r["energy"].cpu().numpy(),
+                     "s": r["s"].cpu().numpy(), "evals": r["n_evals"].cpu().numpy(),
+                     "n32": r["n_evals_fp32"].cpu().numpy(),
+                     "lat": r["latency_ns"].cpu().numpy() / 1e6}  # fmt: skip
+    clocks = sampler.stop()
+    # error of every mixed result against the FP64 oracle (direct sum, host threads)
+    m = out["mixed"]
+    ks_n = en.n_vectors[en._rows].astype(np.int64)
+    w = en.weights[en._rows]
+    e_ref, _ = oracle.energy_grad_batch(m["s"], ks_n, w, box_vol, threads=oracle.max_threads())
+    errs = [abs(float(m["energy"][i]) - float(e_ref[i])) for i in range(b)]
+    p, mx = out["fp64"], out["mixed"]
+    line = {
+        "metric": "relaxations/s to Phi<1e-20, mixed precision vs plain FP64 (same seeds)",
+        "value": float(mx["ok"].sum()) / (mx["ms"] / 1e3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mx["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {
+            "workload": f"lbfgs_relax_d3_n4000_chi0.45_m{en._rows.size}_b{b}_mixed_precision",
+            "switch": "FP32 evaluations until Phi < 1e-6 N (or a stuck FP32 line search), then FP64",
+            "success_mixed": f"{int(mx['ok'].sum())}/{b}", "success_fp64": f"{int(p['ok'].sum())}/{b}",
+            "success_masks_identical": bool((mx["ok"] == p["ok"]).all()),
+            "fp32_eval_fraction": float(mx["n32"].sum() / max(mx["evals"].sum(), 1)),
+            "evals_per_relax_mixed": float(mx["evals"].mean()),
+            "evals_per_relax_fp64": float(p["evals"].mean()),
+            "max_abs_err_vs_fp64_oracle": float(max(errs)),
+            "err_vs_fp64_oracle_per_result": [float(e) for e in errs],
+            "p50_latency_ms": float(np.percentile(mx["lat"], 50)),
+            "p99_latency_ms": float(np.percentile(mx["lat"], 99)),
+        },
+        "plain_fp64": {"value": float(p["ok"].sum()) / (p["ms"] / 1e3), "unit": UNIT,
+                       "ms_per_step": p["ms"]},
+        "speedup_vs_plain_fp64": (p["ms"] / mx["ms"]),
+        "clocks": clocks,
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ request stream
 def run_serve(args) -> None:
     import torch
@@ -523,12 +594,13 @@ def main() -> None:
     ap.add_argument("--profile", choices=["eval", "relax"], default=None,
                     help="profiling driver for ncu: run the kernels only")  # fmt: skip
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--workload", choices=["batch", "mixed", "serve"], default="batch",
+    ap.add_argument("--workload", choices=["batch", "mixed", "serve", "precision"], default="batch",
                     help="batch: the headline 256-lane d2 N1000 relax; mixed: the 512-instance "
                          "mixed-size ensemble; serve: a Poisson request stream")  # fmt: skip
     ap.add_argument("--mixed-count", type=int, default=512)
     ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--serve-count", type=int, default=200)
+    ap.add_argument("--precision-batch", type=int, default=64)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     args = ap.parse_args()
     if args.profile:
@@ -537,6 +609,8 @@ def main() -> None:
         run_mixed(args)
     elif args.workload == "serve" and args.impl == "cco":
         run_serve(args)
+    elif args.workload == "precision" and args.impl == "cco":
+        run_precision(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -91,6 +91,19 @@ int cco_energy_grad(cco_problem* p, void* stream, int batch, const double* s,
                     double* phi, double* grad, double* rho_re, double* rho_im);
 
 /*
+ * The mixed-precision evaluation that relaxations with precision = FP32 use
+ * while a lane's energy is large (no reference counterpart; the reference is
+ * FP64 only): phase tables seeded by FP64 sincospi and stored in FP32, FP32
+ * phase recurrences, Kahan-compensated FP32 accumulation of each tile's
+ * density, FP32 back-projection; the sum over tiles, rho, Phi and the final
+ * gradient sums in FP64. Relative accuracy about 1e-6 of |rho| per term -
+ * fine for descent far from the minimum, useless near Phi = 0, which is pure
+ * cancellation. Same arguments as cco_energy_grad without the density.
+ */
+int cco_energy_grad_fp32(cco_problem* p, void* stream, int batch, const double* s,
+                         double* phi, double* grad);
+
+/*
  * cco_energy_grad without any allocation (no counterpart in the reference).
  *
  * For callers that must not allocate device memory during a call: code that
@@ -136,7 +149,9 @@ typedef struct {
 typedef struct {
   int64_t memory;                      /* 100 */
   int32_t n_rescales;                  /* 3   */
-  int32_t pad_;
+  int32_t precision;                   /* 0: FP64 throughout (the reference); 1: mixed -
+                                          FP32 evaluations until Phi < 1e-6 N, then FP64
+                                          (no reference counterpart) */
   double rescales[CCO_MAX_RESCALES];   /* 1e4, 1, 1e-2 */
   int64_t max_evals_per_pass;          /* 500000 */
   double energy_tol;                   /* 0 */
@@ -163,6 +178,8 @@ typedef struct {
   int64_t* traj_count;  /* [B] */
   int64_t* latency_ns;  /* [B] optional: device time from the start of the call to the
                            lane's completion (%globaltimer), NULL to skip */
+  int64_t* n_evals_fp32; /* [B] optional (L-BFGS): evaluations done in FP32 (precision = 1),
+                           NULL to skip */
   int64_t ticks;        /* out: device ticks (one energy evaluation per running lane each) */
   int64_t launches;     /* out: kernel launches issued by the call */
   int32_t branches;     /* out: graph branches of the tick schedule used */
@@ -246,6 +263,7 @@ typedef struct {
   int64_t device_ns;        /* device time from the lane's first tick to its completion */
   int32_t error;            /* CCO_OK, or the code of a device failure that ended it */
   int32_t pad_;
+  int64_t n_evals_fp32;     /* evaluations done in FP32 (precision = 1) */
 } cco_request_result;
 
 typedef struct {

@@ -20,7 +20,10 @@ def test_settings_defaults_match_reference():
         step_init=1e-3, step_min=1e-15, shrink=0.5, grow=1.0, rel_tol=0.01, max_evals=10_000,
         energy_tol=0.0, record_every=0, max_records=0,
     )  # fmt: skip
-    assert dataclasses.asdict(LBFGSSettings()) == dict(
+    fields = dataclasses.asdict(LBFGSSettings())
+    # the one field the reference does not have: opt-in mixed precision, off by default
+    assert fields.pop("precision") == "fp64"
+    assert fields == dict(
         memory=100, rescales=(1e4, 1.0, 1e-2), max_evals_per_pass=500_000, energy_tol=0.0,
         grad_tol=0.0, stagnation_patience=50, max_linesearch_steps=30, record_every=0,
         max_records=0,

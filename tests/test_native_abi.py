@@ -40,7 +40,7 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts_match_header():
     assert ctypes.sizeof(_native.DescentSettingsC) == 9 * 8
     assert ctypes.sizeof(_native.LBFGSSettingsC) == 8 + 8 + 8 * 8 + 7 * 8
-    assert ctypes.sizeof(_native.RelaxOutC) == 15 * 8
+    assert ctypes.sizeof(_native.RelaxOutC) == 16 * 8
 
 
 def test_abi_version_and_errors():
@@ -86,5 +86,5 @@ def test_server_without_device_is_refused():
 
 def test_serving_structs_match_header():
     assert ctypes.sizeof(_native.ServerConfigC) == 3 * 8
-    assert ctypes.sizeof(_native.RequestResultC) == 11 * 8
+    assert ctypes.sizeof(_native.RequestResultC) == 12 * 8
     assert ctypes.sizeof(_native.ServerStatsC) == 13 * 8

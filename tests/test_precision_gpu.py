@@ -1,0 +1,104 @@
+"""Mixed precision: FP32 evaluations early, FP64 for the finish and the judgement.
+
+The reference is FP64 only, so these tests hold the mixed path to the FP64
+path and to the oracle: the FP32 evaluation stays within a stated error of
+the oracle's direct sum, mixed-precision relaxations reach Phi < 1e-20 on
+exactly the lanes where plain FP64 does (identical success masks on seeded
+ensembles), every mixed result's final energy is an FP64 value that the
+oracle confirms, and the lanes really ran FP32 evaluations first.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import RTOL_KERNEL_E, energy_atol
+from xla_cco import _native
+from xla_cco.box import cubic_box
+from xla_cco.energy import make_stealthy_energy
+from xla_cco.kvectors import enumerate_kvectors, k_outer_from_ka, ka_from_chi
+from xla_cco.minimize import relax, relax_device
+from xla_cco.minimize.lbfgs import LBFGSSettings
+from xla_cco.serve import RelaxServer
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-20
+# FP32 evaluation vs the FP64 oracle on uniform configurations: |rho_k| ~ sqrt(N),
+# each phase carries ~1e-6 relative error, so Phi is good to ~1e-5 relative and
+# the gradient to ~1e-4 of its largest component.
+RTOL_FP32_E = 1e-4
+RTOL_FP32_F = 1e-3
+
+
+def _system(n, d, chi):
+    box = cubic_box(n, d)
+    ks = enumerate_kvectors(box.basis, 0.0, k_outer_from_ka(ka_from_chi(chi, 0.05, d), 0.05, d))
+    return box, ks, make_stealthy_energy(box, ks)
+
+
+@pytest.mark.parametrize("n,d,chi,b", [(400, 1, 0.3, 3), (500, 2, 0.4, 3), (300, 3, 0.45, 3)])
+def test_fp32_evaluation_against_oracle(n, d, chi, b):
+    import torch
+
+    box, ks, en = _system(n, d, chi)
+    s = np.random.default_rng(n + d).uniform(size=(b, n, d))
+    st = torch.from_numpy(s).cuda()
+    phi = torch.empty(b, dtype=torch.float64, device="cuda")
+    g = torch.empty_like(st)
+    h = en.problem_handle(torch.cuda.current_device(), n)
+    code = _native.load().cco_energy_grad_fp32(h, None, b, st.data_ptr(), phi.data_ptr(), g.data_ptr())
+    assert code == _native.CCO_OK
+    torch.cuda.synchronize()
+    for i in range(b):
+        pr, gr = oracle.energy_grad(s[i], ks.n, ks.weights, box.volume)
+        np.testing.assert_allclose(phi[i].item(), pr, rtol=RTOL_FP32_E)
+        np.testing.assert_allclose(g[i].cpu().numpy(), gr, rtol=0, atol=RTOL_FP32_F * np.abs(gr).max())
+
+
+@pytest.mark.parametrize("n,d,chi,b", [(500, 2, 0.40, 24), (300, 3, 0.45, 16), (600, 1, 0.35, 8)])
+def test_mixed_precision_success_masks_match_plain(n, d, chi, b):
+    import torch
+
+    box, ks, en = _system(n, d, chi)
+    s0 = torch.from_numpy(np.random.default_rng(7 + n).uniform(size=(b, n, d))).cuda()
+    plain = relax_device(en, s0, LBFGSSettings(energy_tol=TOL))
+    mixed = relax_device(en, s0, LBFGSSettings(energy_tol=TOL, precision="mixed"))
+    ok_p = (plain["energy"] < TOL).cpu().numpy()
+    ok_m = (mixed["energy"] < TOL).cpu().numpy()
+    np.testing.assert_array_equal(ok_m, ok_p)
+    n32 = mixed["n_evals_fp32"].cpu().numpy()
+    assert (n32 > 0).all(), "every mixed lane starts in FP32"
+    assert (plain["n_evals_fp32"].cpu().numpy() == 0).all()
+    # the final energy of a mixed result is an FP64 evaluation: the oracle agrees
+    s_fin = mixed["s"].cpu().numpy()
+    e_fin = mixed["energy"].cpu().numpy()
+    for i in range(b):
+        e_ref, _ = oracle.energy_grad(s_fin[i], ks.n, ks.weights, box.volume)
+        np.testing.assert_allclose(e_fin[i], e_ref, rtol=RTOL_KERNEL_E,
+                                   atol=energy_atol(n, ks.n.shape[0], e_ref))  # fmt: skip
+
+
+def test_mixed_precision_served_equals_relaxed_alone():
+    _, _, en = _system(400, 2, 0.35)
+    rng = np.random.default_rng(3)
+    s0 = [rng.uniform(size=(400, 2)) for _ in range(4)]
+    st = LBFGSSettings(energy_tol=TOL, precision="mixed")
+    with RelaxServer(st) as srv:
+        results = [srv.result(t) for t in [srv.submit(en, s) for s in s0]]
+    for s, r in zip(s0, results):
+        alone = relax(en, s[None], st)
+        np.testing.assert_array_equal(r.s, alone.s[0])
+        assert r.energy == float(alone.energy[0]) and r.n_evals == int(alone.n_evals[0])
+        assert r.n_evals_fp32 > 0
+
+
+def test_precision_setting_is_validated():
+    _, _, en = _system(50, 2, 0.2)
+    with pytest.raises(ValueError):
+        relax(en, np.zeros((1, 50, 2)), LBFGSSettings(precision="fp16"))
+    assert ctypes.sizeof(_native.LBFGSSettingsC) == 17 * 8

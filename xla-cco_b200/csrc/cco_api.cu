@@ -367,7 +367,7 @@ __global__ void k_make_lanes(EvalLane* lanes, EvalItem* it1, EvalItem* it2, int 
                              int nt2, int total, const double* s, size_t s_stride, double* f,
                              size_t f_stride, double* g, size_t g_stride, double2* rho,
                              double2* rhow, double2* part, int M, const int64_t* status,
-                             size_t status_stride) {
+                             size_t status_stride, int prec) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
     if (i < B) {
       EvalLane L;
@@ -378,8 +378,9 @@ __global__ void k_make_lanes(EvalLane* lanes, EvalItem* it1, EvalItem* it2, int 
       L.rhow = rhow + (size_t)i * M;
       L.part = part + (size_t)i * nt1 * M;
       L.status = status ? status + (size_t)i * status_stride : nullptr;
+      L.prec = nullptr;
+      L.fixed_prec = prec;
       L.prob = 0;
-      L.pad_ = 0;
       lanes[i] = L;
     }
     const int j = i - B;
@@ -399,6 +400,7 @@ struct EvalWS {
   double2* rhow = nullptr;
   double2* part = nullptr;
   EvalPlan plan{};
+  int prec = PREC_FP64;   // arithmetic of every lane of this workspace
 
   // pass-2 threads per particle and tiles per configuration for a batch of B
   static int split_for(const cco_problem* p, int B) {
@@ -423,7 +425,7 @@ struct EvalWS {
     const int blocks = std::min(1024, (total + 255) / 256);
     k_make_lanes<<<blocks, 256, 0, st>>>(lanes, it1, it2, B, nt1, nt2, total, s, s_stride, f, f_stride,
                                          g, g_stride, rho, rhow, part, p->M, status,
-                                         status_stride);
+                                         status_stride, prec);
     plan.probs = p->dev;
     plan.lanes = lanes;
     plan.items1 = it1;
@@ -467,6 +469,25 @@ extern "C" int cco_energy_grad(cco_problem* p, void* stream, int batch, const do
   CCO_CUDA(eval_launch(ws.plan, st));
   if (rho_re || rho_im)
     CCO_CUDA(rho_scatter(ws.rho, p->run2ref, p->M, batch, p->M, rho_re, rho_im, st));
+  ws.release(st);
+  CCO_CUDA(cudaGetLastError());
+  return CCO_OK;
+}
+
+extern "C" int cco_energy_grad_fp32(cco_problem* p, void* stream, int batch, const double* s,
+                                    double* phi, double* grad) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (batch < 0) return fail(CCO_ERR_ARG, "batch must be >= 0");
+  if (batch == 0) return CCO_OK;
+  if (!s || !phi) return fail(CCO_ERR_ARG, "null s or phi");
+  DeviceGuard guard(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  EvalWS ws;
+  ws.prec = PREC_FP32;
+  CCO_CUDA(ws.alloc(p, batch, st));
+  const size_t nd = (size_t)p->N * p->d;
+  CCO_CUDA(ws.build(p, batch, s, nd, phi, 1, grad, nd, nullptr, 0, st));
+  CCO_CUDA(eval_launch(ws.plan, st));
   ws.release(st);
   CCO_CUDA(cudaGetLastError());
   return CCO_OK;

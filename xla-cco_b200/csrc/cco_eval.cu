@@ -56,9 +56,14 @@ __device__ __forceinline__ Levels<D> levels(const TabLayout& T) {
 // up to 8 entries, each seeded by FP64 sincospi of the exact exponent. Level 0
 // continues by products with z (error <= 8 eps), higher levels use one
 // sincospi per entry. Particles past nj get s = 0 and are never read back.
-template <int D>
+__device__ __forceinline__ void put(double2* p, double2 v) { *p = v; }
+__device__ __forceinline__ void put(float2* p, double2 v) {
+  *p = make_float2((float)v.x, (float)v.y);
+}
+
+template <int D, class C>
 __device__ void build_tables(const TabLayout& T, const double* __restrict__ s, int j0, int nj,
-                             int tj, int stride, double2* tab) {
+                             int tj, int stride, C* tab) {
   int units = 0;
 #pragma unroll
   for (int a = 0; a < D; ++a)
@@ -76,34 +81,34 @@ __device__ void build_tables(const TabLayout& T, const double* __restrict__ s, i
     const double sv = (j < nj) ? s[(size_t)(j0 + j) * D + a] : 0.0;
     const int e0 = q * 8, e1 = min(e0 + 8, T.nent[a][l]);
     double sn, cs;
-    double2* out = tab + (size_t)T.row[a][l] * stride + j;
+    C* out = tab + (size_t)T.row[a][l] * stride + j;
     if (l == 0) {
       sincospi(2.0 * sv, &sn, &cs);
       const double2 z = make_double2(cs, sn);
       sincospi(2.0 * ((double)e0 * sv), &sn, &cs);
       double2 p = make_double2(cs, sn);
       for (int e = e0; e < e1; ++e) {
-        out[(size_t)e * stride] = p;
+        put(out + (size_t)e * stride, p);
         p = cmul(p, z);
       }
     } else {
       for (int e = e0; e < e1; ++e) {
         sincospi(2.0 * ((double)(e * scale) * sv), &sn, &cs);
-        out[(size_t)e * stride] = make_double2(cs, sn);
+        put(out + (size_t)e * stride, make_double2(cs, sn));
       }
     }
   }
 }
 
 // exp(2 pi i n . s_j) at a segment start, from the tables.
-template <int D>
-__device__ __forceinline__ double2 start_phase(const Levels<D>& L, const SegHdr& h,
-                                               const double2* tab, int stride, int j) {
-  double2 ph = make_double2(1.0, 0.0);
+template <int D, class C>
+__device__ __forceinline__ C start_phase(const Levels<D>& L, const SegHdr& h, const C* tab,
+                                         int stride, int j) {
+  C ph = tab[j];   // replaced at a = 0
 #pragma unroll
   for (int a = 0; a < D; ++a) {
     const int dg = h.dig[a];
-    double2 f = tab[(dg & 255) * stride + j];
+    C f = tab[(dg & 255) * stride + j];
     if (L.n[a] > 1) f = cmul(f, tab[((dg >> 8) & 255) * stride + j]);
     if (L.n[a] > 2) f = cmul(f, tab[((dg >> 16) & 255) * stride + j]);
     if (dg >> 24) f.y = -f.y;
@@ -361,6 +366,237 @@ __device__ void pass2_body(const ProbDev& P, const EvalLane& ln, int tile, int s
   }
 }
 
+// ------------------------------------------------------------ FP32 bodies
+// Kahan-compensated FP32 complex accumulation: s holds the sum, c minus the
+// low-order part lost so far (value = s - c).
+__device__ __forceinline__ void kahan_add(float2& s, float2& c, float2 v) {
+  const float yx = v.x - c.x, yy = v.y - c.y;
+  const float tx = s.x + yx, ty = s.y + yy;
+  c.x = (tx - s.x) - yx;
+  c.y = (ty - s.y) - yy;
+  s.x = tx;
+  s.y = ty;
+}
+
+template <int D, bool FULL>
+__device__ __forceinline__ void seg_sum_f32(const Levels<D>& L, const SegHdr& h, const float2* tab,
+                                            int zrow, int j, int ns, int nj,
+                                            float2 (&acc)[kSeg1Len], float2 (&cmp)[kSeg1Len]) {
+  constexpr int S = kPass1Stride;
+  const int len = h.len;
+  for (; j + 3 * ns < nj; j += 4 * ns) {
+    float2 p0 = start_phase<D>(L, h, tab, S, j);
+    float2 p1 = start_phase<D>(L, h, tab, S, j + ns);
+    float2 p2 = start_phase<D>(L, h, tab, S, j + 2 * ns);
+    float2 p3 = start_phase<D>(L, h, tab, S, j + 3 * ns);
+    const float2 z0 = tab[zrow * S + j], z1 = tab[zrow * S + j + ns];
+    const float2 z2 = tab[zrow * S + j + 2 * ns], z3 = tab[zrow * S + j + 3 * ns];
+#pragma unroll
+    for (int i = 0; i < kSeg1Len; ++i) {
+      if (FULL || i < len) {
+        kahan_add(acc[i], cmp[i],
+                  make_float2((p0.x + p1.x) + (p2.x + p3.x), (p0.y + p1.y) + (p2.y + p3.y)));
+        p0 = cmul(p0, z0);
+        p1 = cmul(p1, z1);
+        p2 = cmul(p2, z2);
+        p3 = cmul(p3, z3);
+      }
+    }
+  }
+  for (; j < nj; j += ns) {
+    float2 p0 = start_phase<D>(L, h, tab, S, j);
+    const float2 z0 = tab[zrow * S + j];
+#pragma unroll
+    for (int i = 0; i < kSeg1Len; ++i) {
+      if (FULL || i < len) {
+        kahan_add(acc[i], cmp[i], p0);
+        p0 = cmul(p0, z0);
+      }
+    }
+  }
+}
+
+// Pass 1 in FP32 (same decomposition as pass1_body); partial rows leave in FP64.
+template <int D>
+__device__ void pass1_body_f32(const ProbDev& P, const EvalLane& ln, int tile, double2* smem) {
+  const TabLayout& T = P.t1;
+  float2* tab = reinterpret_cast<float2*>(smem);
+  const int j0 = tile * kPass1Tile;
+  const int nj = min(kPass1Tile, P.N - j0);
+  build_tables<D>(T, ln.s, j0, nj, kPass1Tile, kPass1Stride, tab);
+  const Levels<D> L = levels<D>(T);
+  const int zrow = T.zrow;
+  __syncthreads();
+  const int nseg = P.nseg1;
+  int ns = 1;
+  while (2 * ns * nseg <= (int)blockDim.x && 2 * ns <= nj) ns *= 2;
+  const int units = nseg * ns;
+  // slice partials after the tables, on a 16-byte boundary
+  double2* red = smem + ((size_t)T.nrows * kPass1Stride + 1) / 2;
+  double2* out = ln.part + (size_t)tile * P.M;
+  for (int u = threadIdx.x; u < units; u += blockDim.x) {
+    const int sg = u % nseg, slice = u / nseg;
+    const SegHdr h = P.seg1[sg];
+    float2 acc[kSeg1Len], cmp[kSeg1Len];
+#pragma unroll
+    for (int i = 0; i < kSeg1Len; ++i) {
+      acc[i] = make_float2(0.f, 0.f);
+      cmp[i] = make_float2(0.f, 0.f);
+    }
+    if (h.len == kSeg1Len)
+      seg_sum_f32<D, true>(L, h, tab, zrow, slice, ns, nj, acc, cmp);
+    else
+      seg_sum_f32<D, false>(L, h, tab, zrow, slice, ns, nj, acc, cmp);
+#pragma unroll
+    for (int i = 0; i < kSeg1Len; ++i) {
+      const double2 v = make_double2((double)acc[i].x - (double)cmp[i].x,
+                                     (double)acc[i].y - (double)cmp[i].y);
+      if (ns == 1) {
+        if (i < h.len) out[h.kstart + i] = v;
+      } else {
+        red[((size_t)slice * nseg + sg) * kSeg1Len + i] = v;
+      }
+    }
+  }
+  if (ns > 1) {
+    __syncthreads();
+    for (int v = threadIdx.x; v < nseg * kSeg1Len; v += blockDim.x) {
+      const int sg = v / kSeg1Len, i = v - sg * kSeg1Len;
+      const SegHdr h = P.seg1[sg];
+      if (i < h.len) {
+        double2 t = red[v];
+        for (int q = 1; q < ns; ++q) {
+          const double2 o = red[(size_t)q * nseg * kSeg1Len + v];
+          t.x += o.x;
+          t.y += o.y;
+        }
+        out[h.kstart + i] = t;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void bp_step_f32(float2 r, float2& ph, float2 z, float di, float& S,
+                                            float& Tn) {
+  const float c = r.y * ph.x - r.x * ph.y;
+  S += c;
+  Tn += c * di;
+  ph = cmul(ph, z);
+}
+
+// Slice q of pass 2 in FP32: each segment's sums S, T (<= 256 rows) in FP32,
+// folded into the FP64 gradient once per segment.
+template <int D>
+__device__ __forceinline__ void pass2_slice_f32(const ProbDev& P, const Levels<D>& L,
+                                                const float2* __restrict__ rw, const float2* tab,
+                                                int stride, int j, float2 z, int q, int sl,
+                                                double (&G)[D]) {
+  const int nseg = P.nseg2;
+#pragma unroll
+  for (int a = 0; a < D; ++a) G[a] = 0.0;
+  for (int sg = 2 * q; sg < nseg; sg += 2 * sl) {
+    const SegHdr hA = P.seg2[sg];
+    const SegHdr hB = P.seg2[min(sg + 1, nseg - 1)];
+    float2 pA = start_phase<D>(L, hA, tab, stride, j);
+    float2 pB = start_phase<D>(L, hB, tab, stride, j);
+    float SA = 0.f, TA = 0.f, SB = 0.f, TB = 0.f;
+    const float2* rA = rw + hA.kstart;
+    const float2* rB = rw + hB.kstart;
+    const int la = hA.len, lb = (sg + 1 < nseg) ? hB.len : 0;
+    int i = 0;
+    float di = 0.f;
+    for (; i + 2 <= lb; i += 2) {
+      const float2 a0 = rA[i], a1 = rA[i + 1];
+      const float2 b0 = rB[i], b1 = rB[i + 1];
+      bp_step_f32(a0, pA, z, di, SA, TA);
+      bp_step_f32(b0, pB, z, di, SB, TB);
+      bp_step_f32(a1, pA, z, di + 1.f, SA, TA);
+      bp_step_f32(b1, pB, z, di + 1.f, SB, TB);
+      di += 2.f;
+    }
+    if (i < lb) {
+      bp_step_f32(rA[i], pA, z, di, SA, TA);
+      bp_step_f32(rB[i], pB, z, di, SB, TB);
+      ++i;
+      di += 1.f;
+    }
+    for (; i + 2 <= la; i += 2) {
+      const float2 a0 = rA[i], a1 = rA[i + 1];
+      bp_step_f32(a0, pA, z, di, SA, TA);
+      bp_step_f32(a1, pA, z, di + 1.f, SA, TA);
+      di += 2.f;
+    }
+    if (i < la) bp_step_f32(rA[i], pA, z, di, SA, TA);
+#pragma unroll
+    for (int a = 0; a < D - 1; ++a) G[a] += (double)hA.n[a] * SA + (double)hB.n[a] * SB;
+    G[D - 1] += ((double)hA.n[D - 1] * SA + TA) + ((double)hB.n[D - 1] * SB + TB);
+  }
+}
+
+// Pass 2 in FP32 (decomposition of pass2_body). The weighted density of an
+// FP32 lane is an FP32 array (written by the reduction over the lane's FP64
+// w rho buffer).
+template <int D, bool STAGED>
+__device__ void pass2_body_f32(const ProbDev& P, const EvalLane& ln, int tile, int split,
+                               double2* smem) {
+  const TabLayout& T = P.t2;
+  float2* tab = reinterpret_cast<float2*>(smem);
+  const int tw = kPass2Tile / split;
+  const int j0 = tile * tw;
+  const int nj = min(tw, P.N - j0);
+  const float2* __restrict__ rw = reinterpret_cast<const float2*>(ln.rhow);
+  float2* after = tab + (size_t)T.nrows * tw;
+  if (STAGED) {
+    for (int k = threadIdx.x; k < P.M; k += blockDim.x) after[k] = rw[k];
+    rw = after;
+    after += P.M;
+  }
+  double* comb = reinterpret_cast<double*>(after + ((after - tab) & 1));   // 8-byte aligned
+  build_tables<D>(T, ln.s, j0, nj, tw, tw, tab);
+  const Levels<D> L = levels<D>(T);
+  __syncthreads();
+  const int j = threadIdx.x % tw, qp = threadIdx.x / tw;
+  const float2 z = tab[T.zrow * tw + j];
+  const int sl = P.sl2;
+  const int per = sl > split ? sl / split : 1;
+  const int nblk = sl / per;
+  if (qp < nblk) {
+    Pairwise<D> acc;
+    for (int q = qp * per; q < (qp + 1) * per; ++q) {
+      double G[D];
+      pass2_slice_f32<D>(P, L, rw, tab, tw, j, z, q, sl, G);
+      acc.push(G);
+    }
+    double G[D];
+    acc.total(G);
+    if (nblk > 1) {
+#pragma unroll
+      for (int a = 0; a < D; ++a) comb[((size_t)qp * tw + j) * D + a] = G[a];
+    } else if (j < nj) {
+      double* gj = ln.g + (size_t)(j0 + j) * D;
+#pragma unroll
+      for (int a = 0; a < D; ++a) gj[a] = P.gpref * G[a];
+    }
+  }
+  if (nblk > 1) {
+    __syncthreads();
+    if (qp == 0 && j < nj) {
+      Pairwise<D> acc;
+      for (int b = 0; b < nblk; ++b) {
+        double G[D];
+#pragma unroll
+        for (int a = 0; a < D; ++a) G[a] = comb[((size_t)b * tw + j) * D + a];
+        acc.push(G);
+      }
+      double G[D];
+      acc.total(G);
+      double* gj = ln.g + (size_t)(j0 + j) * D;
+#pragma unroll
+      for (int a = 0; a < D; ++a) gj[a] = P.gpref * G[a];
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kPass1Threads, 4) k_pass1(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
@@ -369,6 +605,14 @@ __global__ void __launch_bounds__(kPass1Threads, 4) k_pass1(EvalPlan plan) {
   if (!lane_active(ln.status)) return;
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
+  if (lane_prec(ln) == PREC_FP32) {
+    switch (sp.d) {
+      case 1: pass1_body_f32<1>(sp, ln, it.tile, smem); break;
+      case 2: pass1_body_f32<2>(sp, ln, it.tile, smem); break;
+      default: pass1_body_f32<3>(sp, ln, it.tile, smem); break;
+    }
+    return;
+  }
   switch (sp.d) {
     case 1: pass1_body<1>(sp, ln, it.tile, smem); break;
     case 2: pass1_body<2>(sp, ln, it.tile, smem); break;
@@ -399,7 +643,10 @@ __global__ void __launch_bounds__(kReduceChunk) k_reduce(EvalPlan plan) {
     }
     ln.rho[k] = t;
     const double wk = P.w_run[k];
-    ln.rhow[k] = make_double2(wk * t.x, wk * t.y);
+    if (lane_prec(ln) == PREC_FP32)
+      reinterpret_cast<float2*>(ln.rhow)[k] = make_float2((float)(wk * t.x), (float)(wk * t.y));
+    else
+      ln.rhow[k] = make_double2(wk * t.x, wk * t.y);
     e = wk * (t.x * t.x + t.y * t.y);
   }
   e = block_sum(e, red);
@@ -428,6 +675,22 @@ __global__ void __launch_bounds__(kPass2Threads, 4) k_pass2(EvalPlan plan) {
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
   const bool staged = (size_t)sp.M * sizeof(double2) <= kPass2RhoStage;
+  if (lane_prec(ln) == PREC_FP32) {
+    if (staged) {
+      switch (sp.d) {
+        case 1: pass2_body_f32<1, true>(sp, ln, it.tile, plan.split2, smem); break;
+        case 2: pass2_body_f32<2, true>(sp, ln, it.tile, plan.split2, smem); break;
+        default: pass2_body_f32<3, true>(sp, ln, it.tile, plan.split2, smem); break;
+      }
+    } else {
+      switch (sp.d) {
+        case 1: pass2_body_f32<1, false>(sp, ln, it.tile, plan.split2, smem); break;
+        case 2: pass2_body_f32<2, false>(sp, ln, it.tile, plan.split2, smem); break;
+        default: pass2_body_f32<3, false>(sp, ln, it.tile, plan.split2, smem); break;
+      }
+    }
+    return;
+  }
   if (staged) {
     switch (sp.d) {
       case 1: pass2_body<1, true>(sp, ln, it.tile, plan.split2, smem); break;

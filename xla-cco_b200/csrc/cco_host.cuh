@@ -99,6 +99,8 @@ inline EvalLane eval_lane(const RecordShape& R, const LaneRef& L, const cco_prob
                           int prob_index) {
   EvalLane e{};
   double2* dens;
+  e.prec = nullptr;
+  e.fixed_prec = PREC_FP64;
   if (R.method == Method::Descent) {
     const DsView v = ds_view(L.rec, L.ld);
     e.s = v.ps;
@@ -110,6 +112,7 @@ inline EvalLane eval_lane(const RecordShape& R, const LaneRef& L, const cco_prob
     e.s = v.ps;
     e.g = v.pg;
     e.f = v.pf;
+    e.prec = &v.st->prec;
     dens = v.dens;
   }
   e.rho = dens;
@@ -117,7 +120,6 @@ inline EvalLane eval_lane(const RecordShape& R, const LaneRef& L, const cco_prob
   e.part = dens + 2 * (size_t)p->M;
   e.status = rec_status(L.rec);
   e.prob = prob_index;
-  e.pad_ = 0;
   return e;
 }
 

@@ -76,9 +76,19 @@ struct EvalLane {
   double2* rhow;          // [M] weighted density (pass-2 input)
   double2* part;          // [ntile1][M]
   const int64_t* status;  // evaluate iff null or *status == RUNNING
+  const int32_t* prec;    // arithmetic of this evaluation: *prec, or `fixed_prec` when null
   int prob;
-  int pad_;
+  int fixed_prec;         // PREC_FP64 or PREC_FP32
 };
+
+// Evaluation arithmetic of a lane. PREC_FP32: phase tables seeded in FP64
+// and stored in FP32, phase recurrences, pass-1 accumulation (compensated)
+// and the back-projection in FP32; the tile reduction, rho, w rho and Phi in
+// FP64; pass-2 segment sums folded into FP64 gradients.
+enum : int32_t { PREC_FP64 = 0, PREC_FP32 = 1 };
+__device__ __forceinline__ int lane_prec(const EvalLane& ln) {
+  return ln.prec ? *ln.prec : ln.fixed_prec;
+}
 
 struct EvalItem {
   int lane;
@@ -88,6 +98,10 @@ struct EvalItem {
 // ---------------------------------------------------------------- complex
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
 __device__ __forceinline__ bool lane_active(const int64_t* status) {

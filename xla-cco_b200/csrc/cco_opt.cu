@@ -283,7 +283,7 @@ __device__ __forceinline__ int tri(int p, int q) { return q * (q + 1) / 2 + p; }
 struct LbShared {
   LbState L;
   double red[32];
-  int outcome, new_lo, advance;
+  int outcome, new_lo, advance, reeval;
 };
 
 // Lane vectors and history rows have a padded length ld (a multiple of 4
@@ -392,6 +392,17 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
     int local = L.pass_evals >= A.budget ? CCO_STATUS_BUDGET : CCO_STATUS_RUNNING;
     if (L.stag >= A.patience) local = CCO_STATUS_STAGNATED;
     if (fail) local = CCO_STATUS_LINESEARCH_FAIL;
+    // mixed precision: an FP32 lane switches to FP64 instead of ending its
+    // pass on a failed or stagnating line search, and once its energy is low
+    bool sw = false;
+    if (L.prec == PREC_FP32 && glob == CCO_STATUS_RUNNING) {
+      const bool low = L.f < kFp32SwitchPerParticle * (double)R.n;
+      const bool stuck = local == CCO_STATUS_LINESEARCH_FAIL || local == CCO_STATUS_STAGNATED;
+      if (low || stuck) {
+        sw = true;
+        local = CCO_STATUS_RUNNING;
+      }
+    }
     const bool last = L.pass_idx >= A.n_pass - 1;
     const bool pass_end = local != CCO_STATUS_RUNNING && glob == CCO_STATUS_RUNNING;
     const bool advance = pass_end && !last;
@@ -400,8 +411,21 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
     L.status = status;
     if (status != CCO_STATUS_RUNNING) L.t1 = gtimer();
     sh.advance = advance;
+    sh.reeval = sw;
+    if (sw) {
+      // fresh FP64 start at the current point: no history, one re-evaluation
+      L.prec = PREC_FP64;
+      L.phase = PH_REEVAL;
+      L.hk = 0;
+      L.hhead = 0;
+      L.newpair = 0;
+      L.stag = 0;
+    }
   }
   __syncthreads();
+  if (sh.reeval) {
+    for (int e = threadIdx.x; e < h2; e += blockDim.x) st2(v.ps, e, ld2(s, e));
+  }
   if (sh.advance) {
     const int nx = min(L.pass_idx + 1, A.n_pass - 1);
     const double rn = A.rescales[nx];
@@ -423,7 +447,8 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
   }
   __syncthreads();
   lb_record(A, lane, R, sh, s);
-  if (threadIdx.x == 0 && L.status == CCO_STATUS_RUNNING) L.need_dir = 1;
+  if (threadIdx.x == 0 && L.status == CCO_STATUS_RUNNING && L.phase != PH_REEVAL)
+    L.need_dir = 1;
 }
 
 // Lane start: probe positions = s0, every vector zero (padding included).
@@ -439,6 +464,7 @@ __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
     L.phase = PH_INIT;
     L.status = CCO_STATUS_RUNNING;
     L.R = A.rescales[0];
+    L.prec = A.prec0;
     L.t0 = gtimer();
     *v.st = L;
     if (A.traj_count) A.traj_count[R.idx] = 0;
@@ -458,7 +484,27 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
   if (sh.L.status != CCO_STATUS_RUNNING) return;
   LbState& L = sh.L;
   const int h2 = R.ld >> 1;
-  if (L.phase == PH_INIT) {
+  if (threadIdx.x == 0 && L.prec == PREC_FP32) L.n_fp32 += 1;   // this tick's evaluation
+  if (L.phase == PH_REEVAL) {
+    // the FP64 evaluation of the current point after a precision switch
+    const double Rs = L.R;
+    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+      const double2 gv = ld2(v.pg, e);
+      st2(v.g, e, make_double2(gv.x / Rs, gv.y / Rs));
+    }
+    if (threadIdx.x == 0) {
+      L.f = *v.pf;
+      L.n_evals += 1;
+      L.pass_evals += 1;
+      L.phase = PH_EXPAND;
+      if (L.f < A.energy_tol) {
+        L.status = CCO_STATUS_ENERGY_TOL;
+        L.t1 = gtimer();
+      } else {
+        L.need_dir = 1;
+      }
+    }
+  } else if (L.phase == PH_INIT) {
     // init_one (lbfgs.py:163-197): x = R0 s0, g_x = g_s / R0, one evaluation
     const double R0 = L.R;
     for (int e = threadIdx.x; e < h2; e += blockDim.x) {
@@ -813,7 +859,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passB(LbArgs A) {
 
 __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double* gn_out,
                                  int64_t* ne_out, int64_t* ni_out, int64_t* st_out,
-                                 int64_t* lat_out) {
+                                 int64_t* lat_out, int64_t* n32_out) {
   __shared__ double red[32];
   const int lane = blockIdx.x;
   const LaneRef R = A.lanes[lane];
@@ -833,6 +879,7 @@ __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double*
     ni_out[lane] = L.it;
     st_out[lane] = L.status;
     if (lat_out) lat_out[lane] = L.t1 - L.t0;
+    if (n32_out) n32_out[lane] = L.n_fp32;
   }
 }
 
@@ -898,9 +945,9 @@ cudaError_t lbfgs_update(const LbArgs& a, cudaStream_t st) {
 }
 cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double* gn_out,
                            int64_t* ne_out, int64_t* ni_out, int64_t* st_out, int64_t* lat_out,
-                           cudaStream_t st) {
+                           int64_t* n32_out, cudaStream_t st) {
   k_lbfgs_finalize<<<a.B, kUpdThreads, 0, st>>>(a, s_out, e_out, gn_out, ne_out, ni_out, st_out,
-                                                lat_out);
+                                                lat_out, n32_out);
   return cudaGetLastError();
 }
 cudaError_t count_running(const LaneRef* lanes, int B, int* out, cudaStream_t st) {

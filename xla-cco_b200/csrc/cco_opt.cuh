@@ -12,7 +12,15 @@
 
 namespace cco {
 
-enum : int { PH_INIT = 0, PH_ITER = 1, PH_EXPAND = 1, PH_ZOOM = 2 };
+enum : int { PH_INIT = 0, PH_ITER = 1, PH_EXPAND = 1, PH_ZOOM = 2, PH_REEVAL = 3 };
+
+// Mixed-precision L-BFGS: a lane starts with FP32 evaluations and switches to
+// FP64 for good once its energy falls below kFp32SwitchPerParticle * N, or
+// when an FP32 line search fails or stagnates (the FP32 energy is too coarse
+// to continue). At the switch the history is cleared and the current point is
+// evaluated again in FP64 before the next direction, so every energy the line
+// search compares and the final judgement come from FP64 evaluations.
+constexpr double kFp32SwitchPerParticle = 1e-6;
 
 // One lane of a launch.
 struct LaneRef {
@@ -21,7 +29,7 @@ struct LaneRef {
   int64_t soff;     // offset of the lane in the caller's packed positions
   int64_t toff;     // offset of the lane's trajectory rows in traj_s
   int32_t idx;      // the lane's index in the call: its row of traj_e/step/it/count
-  int32_t pad_;
+  int32_t n;        // particles N
 };
 
 __host__ __device__ __forceinline__ int pad4(int nd) { return (nd + 3) & ~3; }
@@ -86,8 +94,10 @@ struct LbState {
   double a_hi, f_hi, d_hi;
   double gamma, last_step;
   int32_t phase, ls_steps, pass_idx, hk, hhead, have_lo, newpair, need_dir;
+  int32_t prec;           // evaluation arithmetic (PREC_FP64 / PREC_FP32)
+  int32_t n_fp32;         // evaluations done in FP32
 };
-constexpr int kLbHead = 32;   // LbState (27 doubles) and pf at [31]
+constexpr int kLbHead = 32;   // LbState (28 doubles) and pf at [31]
 static_assert(sizeof(LbState) <= (kLbHead - 1) * sizeof(double), "LbState outgrew its slot");
 static_assert(sizeof(DsState) <= (kDsHead - 1) * sizeof(double), "DsState outgrew its slot");
 
@@ -148,6 +158,7 @@ struct LbArgs {
   double energy_tol, grad_tol;
   int64_t budget, patience, max_ls;
   int64_t rec_every, rec_cap;
+  int prec0;              // PREC_FP32: lanes start in FP32 (mixed precision)
   int nblkB;              // grid width of pass B (max over the lanes)
   size_t smem_tri;        // 0: triangles in the record (global memory)
   double *traj_s, *traj_e, *traj_step;
@@ -166,7 +177,7 @@ cudaError_t lbfgs_init(const LbArgs& a, const double* s0, cudaStream_t st);
 cudaError_t lbfgs_update(const LbArgs& a, cudaStream_t st);
 cudaError_t lbfgs_finalize(const LbArgs& a, double* s_out, double* e_out, double* gn_out,
                            int64_t* ne_out, int64_t* ni_out, int64_t* st_out, int64_t* lat_out,
-                           cudaStream_t st);
+                           int64_t* n32_out, cudaStream_t st);
 
 // Count lanes whose status is RUNNING.
 cudaError_t count_running(const LaneRef* lanes, int B, int* out, cudaStream_t st);

@@ -450,6 +450,7 @@ int make_table(cco_problem* const* probs, int B, const RecordShape& shape, int64
     r.soff = soff;
     r.toff = cap * soff;
     r.idx = i;
+    r.n = p->N;
     o += record_doubles(shape, p);
     soff += r.nd;
   }
@@ -525,6 +526,7 @@ int relax_lbfgs_set(cco_problem* const* probs, int B, cudaStream_t st, const dou
   if (cfg->memory < 1) return fail(CCO_ERR_ARG, "memory must be >= 1");
   if (cfg->memory > 256) return fail(CCO_ERR_ARG, "memory must be <= 256 on this build");
   if (cfg->max_linesearch_steps < 1) return fail(CCO_ERR_ARG, "max_linesearch_steps must be >= 1");
+  if (cfg->precision != 0 && cfg->precision != 1) return fail(CCO_ERR_ARG, "precision must be 0 or 1");
   if (B < 1 || !probs[0]) return fail(CCO_ERR_ARG, "need at least one configuration");
   const bool rec = cfg->record_every > 0 && cfg->max_records > 0;
   if (check_traj(out, rec) != CCO_OK) return CCO_ERR_ARG;
@@ -561,7 +563,8 @@ int relax_lbfgs_set(cco_problem* const* probs, int B, cudaStream_t st, const dou
   rc = run_lane_table(T, st, max_ticks, &rs);
   if (rc == CCO_OK) {
     cudaError_t e = lbfgs_finalize(A, out->s, out->energy, out->grad_norm, out->n_evals,
-                                   out->n_iters, out->status, out->latency_ns, st);
+                                   out->n_iters, out->status, out->latency_ns, out->n_evals_fp32,
+                                   st);
     if (e != cudaSuccess) rc = cuda_fail(e, "lbfgs_finalize");
   }
   out->ticks = rs.ticks;
@@ -595,6 +598,7 @@ int lbfgs_args(const cco_lbfgs_settings* cfg, LbArgs* A, RecordShape* shape) {
   A->max_ls = cfg->max_linesearch_steps;
   A->rec_every = 1;
   A->rec_cap = 0;
+  A->prec0 = cfg->precision == 1 ? PREC_FP32 : PREC_FP64;
   const size_t tri_bytes = lbfgs_update_smem(m);
   const bool in_smem = tri_bytes <= 200 * 1024;
   A->smem_tri = in_smem ? tri_bytes : 0;

@@ -44,7 +44,7 @@ struct Request {
   // results
   std::vector<double> s;
   double energy = 0.0, grad_norm = 0.0;
-  int64_t n_evals = 0, n_iters = 0, status = CCO_STATUS_RUNNING, device_ns = 0;
+  int64_t n_evals = 0, n_iters = 0, status = CCO_STATUS_RUNNING, device_ns = 0, n_fp32 = 0;
   int error = CCO_OK;
   bool done = false;
   bool cancel = false;      // asked by the client
@@ -320,6 +320,7 @@ class Driver {
       ref.rec = r->rec;
       ref.nd = r->p->N * r->p->d;
       ref.ld = pad4(ref.nd);
+      ref.n = r->p->N;
       ref.soff = (int64_t)s0.size();
       ref.toff = 0;
       s0.insert(s0.end(), r->s0.begin(), r->s0.end());
@@ -376,6 +377,7 @@ class Driver {
       ref.rec = r->rec;
       ref.nd = r->p->N * r->p->d;
       ref.ld = pad4(ref.nd);
+      ref.n = r->p->N;
       table_.probs.push_back(r->p);
       table_.refs.push_back(ref);
     }
@@ -471,14 +473,15 @@ class Driver {
       ref.rec = r->rec;
       ref.nd = r->p->N * r->p->d;
       ref.ld = pad4(ref.nd);
+      ref.n = r->p->N;
       ref.soff = total;
       R.soff.push_back(total);
       total += ref.nd;
       refs.push_back(ref);
     }
     // device outputs: s (total), energy, grad_norm (n each), then
-    // n_evals, n_iters, status, latency (n each, int64)
-    const size_t bytes = sizeof(double) * ((size_t)total + 6 * n);
+    // n_evals, n_iters, status, latency, FP32 evaluations (n each, int64)
+    const size_t bytes = sizeof(double) * ((size_t)total + 7 * n);
     double* d_out = nullptr;
     LaneRef* d_refs = nullptr;
     CCO_CUDA(upload(&d_refs, refs, st_));
@@ -492,7 +495,7 @@ class Driver {
     double* g_out = e_out + n;
     int64_t* i_out = reinterpret_cast<int64_t*>(g_out + n);
     CCO_CUDA(lbfgs_finalize(a, s_out, e_out, g_out, i_out, i_out + n, i_out + 2 * n,
-                            i_out + 3 * n, st_));
+                            i_out + 3 * n, i_out + 4 * n, st_));
     CCO_CUDA(cudaMemcpyAsync(R.host.ptr, d_out, bytes, cudaMemcpyDeviceToHost, st_));
     CCO_CUDA(cudaEventRecord(R.ev, st_));
     CCO_CUDA(cudaFreeAsync(d_out, st_));
@@ -543,6 +546,7 @@ class Driver {
           r->n_iters = hi[n + i];
           r->status = hi[2 * n + i];
           r->device_ns = hi[3 * n + i];
+          r->n_fp32 = hi[4 * n + i];
           complete_locked(S_, r);
         }
         std::vector<Request*> keep;
@@ -583,6 +587,8 @@ extern "C" int cco_server_create(int device, const cco_lbfgs_settings* settings,
     return fail(CCO_ERR_ARG, "memory must be in 1..256");
   if (settings->max_linesearch_steps < 1)
     return fail(CCO_ERR_ARG, "max_linesearch_steps must be >= 1");
+  if (settings->precision != 0 && settings->precision != 1)
+    return fail(CCO_ERR_ARG, "precision must be 0 or 1");
   if (settings->record_every > 0 && settings->max_records > 0)
     return fail(CCO_ERR_ARG, "the serving pool does not record trajectories");
   if (config && (config->max_lanes < 0 || config->graph_ticks < 0 || config->branches < 0 ||
@@ -680,6 +686,7 @@ extern "C" int cco_server_poll(cco_server* S, int64_t ticket, int timeout_ms,
   out->device_ns = r->device_ns;
   out->error = r->error;
   out->pad_ = 0;
+  out->n_evals_fp32 = r->n_fp32;
   if (s_dst && !r->s.empty()) std::memcpy(s_dst, r->s.data(), sizeof(double) * r->s.size());
   S->reqs.erase(it);
   return CCO_OK;

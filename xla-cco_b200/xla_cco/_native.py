@@ -47,7 +47,7 @@ class LBFGSSettingsC(ctypes.Structure):
     _fields_ = [
         ("memory", ctypes.c_int64),
         ("n_rescales", ctypes.c_int32),
-        ("pad_", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
         ("rescales", ctypes.c_double * MAX_RESCALES),
         ("max_evals_per_pass", ctypes.c_int64),
         ("energy_tol", ctypes.c_double),
@@ -73,6 +73,7 @@ class RelaxOutC(ctypes.Structure):
         ("traj_iteration", _vp),
         ("traj_count", _vp),
         ("latency_ns", _vp),
+        ("n_evals_fp32", _vp),
         ("ticks", ctypes.c_int64),
         ("launches", ctypes.c_int64),
         ("branches", ctypes.c_int32),
@@ -103,6 +104,7 @@ class RequestResultC(ctypes.Structure):
         ("device_ns", ctypes.c_int64),
         ("error", ctypes.c_int32),
         ("pad_", ctypes.c_int32),
+        ("n_evals_fp32", ctypes.c_int64),
     ]
 
 
@@ -128,6 +130,7 @@ SIGNATURES = {
     "cco_problem_info": (ctypes.c_int, [_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_int_p]),
     "cco_energy_grad": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
     "cco_energy_grad_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
+    "cco_energy_grad_fp32": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
     "cco_relax_descent": (
         ctypes.c_int,
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(DescentSettingsC), ctypes.c_int,

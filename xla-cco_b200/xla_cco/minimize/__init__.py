@@ -48,6 +48,9 @@ def _lbfgs_c(st: LBFGSSettings) -> _native.LBFGSSettingsC:
     c.max_linesearch_steps = int(st.max_linesearch_steps)
     c.record_every = int(st.record_every)
     c.max_records = int(st.max_records)
+    if st.precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', not {st.precision!r}")
+    c.precision = 1 if st.precision == "mixed" else 0
     return c
 
 
@@ -72,6 +75,7 @@ def _outputs(b: int, s_shape: tuple, traj_s_shape: tuple, settings: Any, dev: An
         "n_iters": torch.empty(b, dtype=i64, device=dev),
         "status": torch.empty(b, dtype=i64, device=dev),
         "latency_ns": torch.empty(b, dtype=i64, device=dev),
+        "n_evals_fp32": torch.zeros(b, dtype=i64, device=dev),
     }
     if settings.record_every > 0 and settings.max_records > 0:
         cap = int(settings.max_records)
@@ -89,7 +93,8 @@ def _call_relax(fn: str, first: Any, dev: Any, b: int, s0_ptr: int, cset: Any, c
 
     co = _native.RelaxOutC()
     for key in ("s", "energy", "grad_norm", "n_evals", "n_iters", "status", "latency_ns",
-                "traj_s", "traj_energy", "traj_step", "traj_iteration", "traj_count"):  # fmt: skip
+                "n_evals_fp32", "traj_s", "traj_energy", "traj_step", "traj_iteration",
+                "traj_count"):  # fmt: skip
         if key in out:
             setattr(co, key, out[key].data_ptr())
     with torch.cuda.device(dev):

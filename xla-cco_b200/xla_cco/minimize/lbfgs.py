@@ -55,6 +55,10 @@ class LBFGSSettings:
     max_linesearch_steps: int = 30
     record_every: int = 0
     max_records: int = 0
+    # Not in the reference: "mixed" evaluates in FP32 (FP64-seeded tables,
+    # compensated FP32 density sums, FP32 back-projection) while a lane's
+    # energy is above 1e-6 N, then switches that lane to FP64 for good.
+    precision: str = "fp64"
 
 
 def max_rounds(settings: LBFGSSettings, chunk_iters: int) -> int:

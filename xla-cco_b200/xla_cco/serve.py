@@ -45,6 +45,7 @@ class ServedResult:
     done_ns: int
     device_ns: int          # device time from the lane's first tick to its completion
     error: int              # CCO_OK, or the code of a device failure that ended it
+    n_evals_fp32: int = 0   # evaluations done in FP32 (settings.precision == "mixed")
 
     @property
     def latency_s(self) -> float:
@@ -136,7 +137,7 @@ class RelaxServer:
             s=s, energy=float(out.energy), grad_norm=float(out.grad_norm), n_evals=int(out.n_evals),
             n_iters=int(out.n_iters), status=int(out.status), submit_ns=int(out.submit_ns),
             admit_ns=int(out.admit_ns), done_ns=int(out.done_ns), device_ns=int(out.device_ns),
-            error=int(out.error),
+            error=int(out.error), n_evals_fp32=int(out.n_evals_fp32),
         )  # fmt: skip
 
     def result(self, ticket: int) -> ServedResult:
