@@ -362,6 +362,33 @@ def plain_dropin(inst, settings, sample: int) -> dict:
             "ms": ms, "how": "relax(energy_i, s0_i[None]) per instance, sequential, same device"}  # fmt: skip
 
 
+def served_mixed(inst, ok_plain) -> dict:
+    """The whole ensemble through the serving pool with mixed precision, all
+    requests submitted at once; success mask compared with the plain batch."""
+    from xla_cco import LBFGSSettings
+    from xla_cco.serve import RelaxServer
+
+    st = LBFGSSettings(energy_tol=TOL, precision="mixed")
+    with RelaxServer(st) as srv:
+        t0 = time.perf_counter()
+        tickets = [srv.submit(i.energy, i.s0) for i in inst]
+        res = [srv.result(t) for t in tickets]
+        wall = time.perf_counter() - t0
+        stats = srv.stats()
+    ok = np.array([r.energy < TOL for r in res])
+    lat = np.array([r.latency_s for r in res]) * 1e3
+    n32 = sum(r.n_evals_fp32 for r in res)
+    ev = sum(r.n_evals for r in res)
+    return {"value": float(ok.sum()) / wall, "unit": UNIT, "wall_s": wall,
+            "success": f"{int(ok.sum())}/{len(inst)}",
+            "success_mask_equals_plain_fp64": bool((ok == ok_plain).all()),
+            "mask_differences": int((ok != ok_plain).sum()),
+            "p50_latency_ms": float(np.percentile(lat, 50)),
+            "p99_latency_ms": float(np.percentile(lat, 99)),
+            "fp32_eval_fraction": n32 / max(ev, 1), "peak_lanes": stats.peak_lanes,
+            "timing": "host wall clock from the first submission to the last result"}  # fmt: skip
+
+
 def run_mixed(args) -> None:
     import torch
 
@@ -396,6 +423,7 @@ def run_mixed(args) -> None:
     flops = _flops(evals, inst) * args.steps
     value = succ / (ms / 1e3)
     plain = plain_dropin(inst, settings, args.plain_sample)
+    served = served_mixed(inst, outs[-1]["energy"].cpu().numpy() < TOL) if args.served else None
     peak = fp64_peak_tflops()
     achieved = flops / (ms * 1e-3) / 1e12
     line = {
@@ -415,6 +443,9 @@ def run_mixed(args) -> None:
         },
         "plain_fp64_dropin": plain,
         "speedup_vs_plain_dropin": value / plain["value"] if plain["value"] else None,
+        "served_mixed_precision": served,
+        "served_speedup_vs_plain_dropin": (served["value"] / plain["value"]
+                                           if served and plain["value"] else None),
         "roofline": {"kernel": "whole relaxation (evaluations + updates)", "bound": "fp64",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None,
@@ -599,6 +630,8 @@ def main() -> None:
                          "mixed-size ensemble; serve: a Poisson request stream")  # fmt: skip
     ap.add_argument("--mixed-count", type=int, default=512)
     ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--served", action="store_true",
+                    help="mixed workload: also serve the ensemble with mixed precision")  # fmt: skip
     ap.add_argument("--serve-count", type=int, default=200)
     ap.add_argument("--precision-batch", type=int, default=64)
     ap.add_argument("--serve-rate", type=float, default=200.0)

@@ -222,6 +222,59 @@ int cco_relax_lbfgs_mixed(cco_problem* const* problems, void* stream, int batch,
                           int chunk_iters, cco_relax_out* out);
 
 /*
+ * Gradient flow (adaptive Dormand-Prince 5(4)) of batch configurations,
+ * lane i relaxing configuration i of problems[i] (repeat one problem for a
+ * uniform batch). Replaces gradient_flow(energy, s0, basis, FlowSettings,
+ * dt0) with method "dopri5" (src/xla_cco/minimize/flow.py:258-364,401-451),
+ * vmapped over lanes. Same settings, stops, status precedence, clocks,
+ * recording and evaluation count (6 per attempted step, 1 at the start).
+ *   s0        device, packed as the mixed relaxations ([N_i][d_i] per lane)
+ *   bases     host [batch][d_i][d_i] cell bases (rows = lattice vectors), packed
+ *   dt0       host [batch] first step per lane (resume), or NULL for dt_init
+ * Outputs (device): s (packed like s0, not wrapped), and per lane energy, t,
+ * length, dt (next proposed step), n_steps, n_evals, status; with recording
+ * traj_s ([max_records][N_i d_i] per lane, packed), traj_t, traj_length,
+ * traj_energy ([batch][max_records]) and traj_count ([batch]).
+ */
+typedef struct {
+  double rtol;          /* 1e-6  */
+  double atol;          /* 1e-14 */
+  double dt_init;       /* 1e-3  */
+  double dt_min;        /* 1e-14 */
+  double dt_max;        /* inf   */
+  double t_max;         /* inf   */
+  int64_t max_steps;    /* 200000 */
+  double energy_tol;    /* 0 */
+  double grad_tol;      /* 0 */
+  int32_t arclength;    /* 0: parametrization "time", 1: "arclength" */
+  int32_t pad_;
+  int64_t record_every; /* 0 */
+  int64_t max_records;  /* 0 */
+} cco_flow_settings;
+
+typedef struct {
+  double* s;
+  double* energy;
+  double* t;
+  double* length;
+  double* dt;
+  int64_t* n_steps;
+  int64_t* n_evals;
+  int64_t* status;
+  double* traj_s;
+  double* traj_t;
+  double* traj_length;
+  double* traj_energy;
+  int64_t* traj_count;
+  int64_t ticks;        /* out */
+  int64_t launches;     /* out */
+} cco_flow_out;
+
+int cco_gradient_flow(cco_problem* const* problems, void* stream, int batch, const double* s0,
+                      const double* bases, const double* dt0, const cco_flow_settings* settings,
+                      cco_flow_out* out);
+
+/*
  * Tick schedules (graph branches, ticks per graph) are tuned online on the
  * first relaxation of each shape class (minimizer, lane count and total
  * N M bucketed by powers of two, largest d) and cached for the process;

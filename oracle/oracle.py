@@ -240,3 +240,99 @@ def energy_direct(s: np.ndarray, n: np.ndarray, w: np.ndarray, volume: float):
     coef = w[:, None] * (im[:, None] * c - re[:, None] * si)  # (M, N)
     grad = (2.0 * 2.0 * math.pi / volume) * (coef.T @ n.astype(np.float64))
     return phi, grad
+
+
+# ------------------------------------------------------------------ gradient flow
+# Dormand & Prince (1980) 5(4) tableau, the published coefficients.
+_DP_A = (
+    (),
+    (1 / 5,),
+    (3 / 40, 9 / 40),
+    (44 / 45, -56 / 15, 32 / 9),
+    (19372 / 6561, -25360 / 2187, 64448 / 6561, -212 / 729),
+    (9017 / 3168, -355 / 33, 46732 / 5247, 49 / 176, -5103 / 18656),
+)
+_DP_B5 = (35 / 384, 0.0, 500 / 1113, 125 / 192, -2187 / 6784, 11 / 84, 0.0)
+_DP_B4 = (5179 / 57600, 0.0, 7571 / 16695, 393 / 640, -92097 / 339200, 187 / 2100, 1 / 40)
+_DP_E = tuple(b5 - b4 for b5, b4 in zip(_DP_B5, _DP_B4))
+
+
+def gradient_flow_dopri5(s0: np.ndarray, n: np.ndarray, w: np.ndarray, volume: float,
+                         basis: np.ndarray, st, dt0: float | None = None) -> dict:  # fmt: skip
+    """Restatement of the reference's DoPri5 gradient flow for one lane
+    (``src/xla_cco/minimize/flow.py:258-364,401-451``), energies and gradients
+    from the C direct sum. ``st`` carries the FlowSettings fields. Returns the
+    final state and, when recording, the trajectory rows."""
+    basis = np.asarray(basis, dtype=np.float64)
+    metric_inv = np.linalg.inv(basis @ basis.T)
+    binv_t = np.linalg.inv(basis).T
+    arc = st.parametrization == "arclength"
+
+    def velocity(s):
+        f, g = energy_grad(s, n, w, volume)
+        v = -g @ metric_inv
+        gn = float(np.sqrt(np.sum((g @ binv_t) ** 2)))
+        if not arc:
+            return f, g, v, np.array([1.0, gn]), gn
+        inv = 1.0 / gn if gn > 0.0 else 0.0
+        return f, g, v * inv, np.array([inv, 1.0]), gn
+
+    def status(f, g, gn, t, dt, steps, tries):
+        code = 2 if dt < st.dt_min else 0
+        if t >= st.t_max or steps >= st.max_steps or tries >= 4 * st.max_steps:
+            code = 3
+        if np.all(g == 0.0) or gn < st.grad_tol:
+            code = 6
+        return 1 if f < st.energy_tol else code
+
+    s = np.array(s0, dtype=np.float64)
+    f, g, v, rate, gn = velocity(s)
+    dt = min(st.dt_init if dt0 is None else dt0, st.dt_max)
+    t = length = 0.0
+    steps = tries = 0
+    evals = 1
+    rows = [(s.copy(), 0.0, 0.0, f)]
+    code = status(f, g, gn, 0.0, dt, 0, 0)
+    while code == 0:
+        h = dt if arc else min(dt, st.t_max - t)
+        ks, rates = [v], [rate]
+        for i in range(1, 6):
+            incr = sum(a * k for a, k in zip(_DP_A[i], ks))
+            _, _, vi, ri, _ = velocity(s + h * incr)
+            ks.append(vi)
+            rates.append(ri)
+        s_new = s + h * sum(b * k for b, k in zip(_DP_B5[:6], ks))
+        tl = h * sum(b * r for b, r in zip(_DP_B5[:6], rates))
+        f_new, g_new, v_new, r_new, gn_new = velocity(s_new)
+        err_s = h * sum(e * k for e, k in zip(_DP_E, ks + [v_new]))
+        err_tl = h * sum(e * r for e, r in zip(_DP_E, rates + [r_new]))
+        move = np.sqrt(np.mean(((s_new - s) @ basis) ** 2))
+        err = np.sqrt(np.mean((err_s @ basis) ** 2)) / (st.atol + st.rtol * move)
+        err = max(err, float(np.max(np.abs(err_tl) / (st.atol + st.rtol * np.abs(tl)))))
+        accept = err <= 1.0
+        with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
+            factor = float(np.clip(0.9 * err ** (-1.0 / 5.0), 0.2, 5.0))
+        if not math.isfinite(factor):
+            factor = 0.2
+        dt = min(h * factor, st.dt_max)
+        if accept:
+            s, f, g, v, rate, gn = s_new, f_new, g_new, v_new, r_new, gn_new
+            t += tl[0]
+            length += tl[1]
+            steps += 1
+        tries += 1
+        evals += 6
+        code = status(f, g, gn, t, dt, steps, tries)
+        if (accept and st.record_every > 0 and steps % st.record_every == 0
+                and len(rows) < st.max_records):  # fmt: skip
+            rows.append((s.copy(), t, length, f))
+    out = dict(s=s, energy=f, t=t, length=length, dt=dt, n_steps=steps, n_evals=evals,
+               status=code)  # fmt: skip
+    if st.record_every > 0:
+        if not (rows[-1][2] == length and rows[-1][1] == t):
+            if len(rows) >= st.max_records:
+                rows[-1] = (s.copy(), t, length, f)
+            else:
+                rows.append((s.copy(), t, length, f))
+        out["trajectory"] = rows
+    return out

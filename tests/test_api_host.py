@@ -82,3 +82,29 @@ def test_relax_validates_before_device_work():
         relax(en, np.zeros((2, 8, 2), np.float32), DescentSettings())
     with pytest.raises(TypeError):
         relax(en, np.zeros((2, 8, 2)), object())
+
+
+def test_flow_settings_defaults_and_validation():
+    import math
+
+    import numpy as np
+
+    from xla_cco.minimize.flow import FlowSettings, gradient_flow
+
+    assert dataclasses.asdict(FlowSettings()) == dict(
+        rtol=1e-6, atol=1e-14, parametrization="time", method="dopri5", dt_init=1e-3,
+        dt_min=1e-14, dt_max=math.inf, t_max=math.inf, max_steps=200_000, energy_tol=0.0,
+        grad_tol=0.0, record_every=0, max_records=0,
+    )  # fmt: skip
+    s0, basis = np.zeros((4, 2)), np.eye(2)
+    bad = [FlowSettings(atol=0.0), FlowSettings(parametrization="x"), FlowSettings(method="x"),
+           FlowSettings(method="rosenbrock", parametrization="arclength"),
+           FlowSettings(parametrization="arclength", t_max=1.0),
+           FlowSettings(record_every=1, max_records=1)]  # fmt: skip
+    for st in bad:
+        with pytest.raises(ValueError):
+            gradient_flow(None, s0, basis, st)
+    with pytest.raises(TypeError):
+        gradient_flow(None, np.zeros((4, 2), np.float32), basis, FlowSettings())
+    with pytest.raises(ValueError):
+        gradient_flow(None, s0, np.eye(3), FlowSettings())

@@ -12,6 +12,7 @@
 
 #include "cco.h"
 #include "cco_internal.cuh"
+#include "cco_flow.cuh"
 #include "cco_opt.cuh"
 
 struct cco_problem {
@@ -72,7 +73,7 @@ struct DeviceGuard {
 };
 
 // ------------------------------------------------------------ lane records
-enum class Method { Descent, Lbfgs };
+enum class Method { Descent, Lbfgs, Flow };
 
 // What every record of one launch shares: the minimizer and, for L-BFGS,
 // the memory m and whether the scalar kernel's triangles live in the record.
@@ -83,9 +84,10 @@ struct RecordShape {
 
 inline size_t record_doubles(const RecordShape& R, const cco_problem* p) {
   const int ld = pad4(p->N * p->d);
-  const size_t n = R.method == Method::Descent
-                       ? ds_record_doubles(ld, p->M, p->host.ntile1)
-                       : lb_record_doubles(R.m, R.tri_len, ld, p->M, p->host.ntile1);
+  size_t n = 0;
+  if (R.method == Method::Descent) n = ds_record_doubles(ld, p->M, p->host.ntile1);
+  else if (R.method == Method::Flow) n = fl_record_doubles(ld, p->M, p->host.ntile1);
+  else n = lb_record_doubles(R.m, R.tri_len, ld, p->M, p->host.ntile1);
   return (n + 31) & ~(size_t)31;   // records start on 256-byte boundaries
 }
 
@@ -103,6 +105,12 @@ inline EvalLane eval_lane(const RecordShape& R, const LaneRef& L, const cco_prob
   e.fixed_prec = PREC_FP64;
   if (R.method == Method::Descent) {
     const DsView v = ds_view(L.rec, L.ld);
+    e.s = v.ps;
+    e.g = v.pg;
+    e.f = v.pf;
+    dens = v.dens;
+  } else if (R.method == Method::Flow) {
+    const FlView v = fl_view(L.rec, L.ld);
     e.s = v.ps;
     e.g = v.pg;
     e.f = v.pf;
@@ -223,6 +231,7 @@ struct LaneTable {
   LaneRef* d_refs = nullptr;
   DescentArgs ds{};
   LbArgs lb{};
+  FlArgs fl{};
   int upload_refs(cudaStream_t st);
   void release(cudaStream_t st);
 };
@@ -237,6 +246,7 @@ struct TickPlan {
   EvalSet ev[kMaxBranches];
   DescentArgs ds[kMaxBranches];
   LbArgs lb[kMaxBranches];
+  FlArgs fl[kMaxBranches];
   cudaGraphExec_t exec = nullptr;
   int build(const LaneTable& T, const Schedule& sch, cudaStream_t st);
   cudaError_t tick(cudaStream_t s, int b) const;

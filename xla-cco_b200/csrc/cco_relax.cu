@@ -98,7 +98,12 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
     CCO_CUDA(ev[b].build(T.shape, T.refs, T.probs, lo, hi, st));
     int nblk = 1;
     for (int i = lo; i < hi; ++i) nblk = std::max(nblk, lb_nblk(T.refs[i].ld));
-    if (T.shape.method == Method::Descent) {
+    if (T.shape.method == Method::Flow) {
+      FlArgs a = T.fl;
+      a.B = hi - lo;
+      a.lanes = T.d_refs + lo;
+      fl[b] = a;
+    } else if (T.shape.method == Method::Descent) {
       DescentArgs a = T.ds;
       a.B = hi - lo;
       a.lanes = T.d_refs + lo;
@@ -155,11 +160,13 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
 cudaError_t TickPlan::tick(cudaStream_t s, int b) const {
   cudaError_t e = eval_launch(ev[b].plan, s);
   if (e != cudaSuccess) return e;
+  if (method == Method::Flow) return flow_update(fl[b], s);
   return method == Method::Descent ? descent_update(ds[b], s) : lbfgs_update(lb[b], s);
 }
 
 int TickPlan::launches_per_tick() const {
-  return nbr * (method == Method::Descent ? 5 : 8);  // 4 evaluation kernels + the update
+  // 4 evaluation kernels + the update kernels
+  return nbr * (method == Method::Lbfgs ? 8 : 5);
 }
 
 void TickPlan::release(cudaStream_t st) {
@@ -296,6 +303,7 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
   C.shape = T.shape;
   C.ds = T.ds;
   C.lb = T.lb;
+  C.fl = T.fl;
   C.refs = T.refs;
   C.probs = T.probs;
   Schedule chosen, first;
@@ -312,6 +320,8 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
     C.ds.B = (int)C.refs.size();
     C.lb.lanes = C.d_refs;
     C.lb.B = (int)C.refs.size();
+    C.fl.lanes = C.d_refs;
+    C.fl.B = (int)C.refs.size();
     Schedule s;
     if (force_br > 0 || force_gt > 0) {
       if (force_br > 0) s.branches = force_br;
@@ -654,6 +664,140 @@ extern "C" int cco_relax_lbfgs_mixed(cco_problem* const* problems, void* stream,
   if (chunk_iters < 1) return fail(CCO_ERR_ARG, "chunk_iters must be positive");
   if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
   return relax_lbfgs_set(problems, batch, (cudaStream_t)stream, s0, cfg, out);
+}
+
+namespace {
+
+// B, B^-T and (B B^T)^-1 of a d x d basis into 3x3 row-major slots (Gauss-
+// Jordan with partial pivoting). False if the basis is singular.
+bool basis_mats(const double* basis, int d, double* out27) {
+  double a[3][6] = {};
+  for (int i = 0; i < d; ++i)
+    for (int j = 0; j < d; ++j) {
+      a[i][j] = basis[i * d + j];
+      a[i][d + j] = i == j ? 1.0 : 0.0;
+    }
+  for (int c = 0; c < d; ++c) {
+    int piv = c;
+    for (int i = c + 1; i < d; ++i)
+      if (std::fabs(a[i][c]) > std::fabs(a[piv][c])) piv = i;
+    if (a[piv][c] == 0.0 || !std::isfinite(a[piv][c])) return false;
+    if (piv != c)
+      for (int j = 0; j < 2 * d; ++j) std::swap(a[c][j], a[piv][j]);
+    const double inv = 1.0 / a[c][c];
+    for (int j = 0; j < 2 * d; ++j) a[c][j] *= inv;
+    for (int i = 0; i < d; ++i)
+      if (i != c) {
+        const double f = a[i][c];
+        for (int j = 0; j < 2 * d; ++j) a[i][j] -= f * a[c][j];
+      }
+  }
+  for (int q = 0; q < 27; ++q) out27[q] = 0.0;
+  for (int i = 0; i < d; ++i)
+    for (int j = 0; j < d; ++j) {
+      out27[i * 3 + j] = basis[i * d + j];
+      out27[9 + i * 3 + j] = a[j][d + i];  // (B^-1)^T
+    }
+  // (B B^T)^-1 = B^-T B^-1
+  for (int i = 0; i < d; ++i)
+    for (int j = 0; j < d; ++j) {
+      double acc = 0.0;
+      for (int k = 0; k < d; ++k) acc += a[k][d + i] * a[k][d + j];
+      out27[18 + i * 3 + j] = acc;
+    }
+  return true;
+}
+
+}  // namespace
+
+extern "C" int cco_gradient_flow(cco_problem* const* problems, void* stream, int batch,
+                                 const double* s0, const double* bases, const double* dt0,
+                                 const cco_flow_settings* cfg, cco_flow_out* out) {
+  if (!problems || !s0 || !bases || !cfg || !out) return fail(CCO_ERR_ARG, "null argument");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  if (!out->s || !out->energy || !out->t || !out->length || !out->dt || !out->n_steps ||
+      !out->n_evals || !out->status)
+    return fail(CCO_ERR_ARG, "incomplete output struct");
+  if (!(cfg->atol > 0.0) || !(cfg->rtol > 0.0) || !(cfg->dt_init > 0.0) || cfg->max_steps <= 0)
+    return fail(CCO_ERR_ARG, "atol, rtol, dt_init and max_steps must be positive");
+  if (cfg->arclength && std::isfinite(cfg->t_max))
+    return fail(CCO_ERR_ARG, "t_max is supported only with parametrization='time'");
+  if (cfg->record_every < 0 || cfg->max_records < 0)
+    return fail(CCO_ERR_ARG, "record_every and max_records must be >= 0");
+  if ((cfg->record_every > 0) != (cfg->max_records > 1))
+    return fail(CCO_ERR_ARG, "recording needs record_every > 0 and max_records >= 2");
+  const bool rec = cfg->record_every > 0;
+  if (rec && (!out->traj_s || !out->traj_t || !out->traj_length || !out->traj_energy ||
+              !out->traj_count))
+    return fail(CCO_ERR_ARG, "trajectory recording needs the traj_* outputs");
+  for (int i = 0; i < batch; ++i)
+    if (!problems[i]) return fail(CCO_ERR_ARG, "null problem for lane %d", i);
+  std::vector<double> mats((size_t)batch * 27);
+  size_t bo = 0;
+  for (int i = 0; i < batch; ++i) {
+    const int d = problems[i]->d;
+    if (!basis_mats(bases + bo, d, mats.data() + (size_t)i * 27))
+      return fail(CCO_ERR_ARG, "singular basis for lane %d", i);
+    bo += (size_t)d * d;
+  }
+  DeviceGuard guard(problems[0]->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  RecordShape shape;
+  shape.method = Method::Flow;
+  LaneTable T;
+  FlArgs& a = T.fl;
+  a.rtol = cfg->rtol;
+  a.atol = cfg->atol;
+  a.dt_init = cfg->dt_init;
+  a.dt_min = cfg->dt_min;
+  a.dt_max = cfg->dt_max;
+  a.t_max = cfg->t_max;
+  a.energy_tol = cfg->energy_tol;
+  a.grad_tol = cfg->grad_tol;
+  a.max_steps = cfg->max_steps;
+  a.arclength = cfg->arclength ? 1 : 0;
+  a.rec_every = rec ? cfg->record_every : 0;
+  a.rec_cap = rec ? cfg->max_records : 0;
+  if (rec) {
+    a.traj_s = out->traj_s;
+    a.traj_t = out->traj_t;
+    a.traj_len = out->traj_length;
+    a.traj_e = out->traj_energy;
+    a.traj_count = out->traj_count;
+  }
+  double* records = nullptr;
+  int rc = make_table(problems, batch, shape, a.rec_cap, st, &T, &records);
+  if (rc != CCO_OK) {
+    if (records) cudaFreeAsync(records, st);
+    return rc;
+  }
+  a.B = batch;
+  a.lanes = T.d_refs;
+  double* d_mats = nullptr;
+  double* d_dt0 = nullptr;
+  CCO_CUDA(upload(&d_mats, mats, st));
+  if (dt0) {
+    std::vector<double> v(dt0, dt0 + batch);
+    CCO_CUDA(upload(&d_dt0, v, st));
+  }
+  CCO_CUDA(flow_init(a, s0, d_mats, d_dt0, st));
+  const int64_t max_ticks = 2 + 6 * 4 * cfg->max_steps + 4 * (kInflight + 1) * 32;
+  RunStats rs;
+  rc = run_lane_table(T, st, max_ticks, &rs);
+  if (rc == CCO_OK) {
+    cudaError_t e = flow_finalize(a, out->s, out->energy, out->t, out->length, out->dt,
+                                  out->n_steps, out->n_evals, out->status, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "flow_finalize");
+  }
+  out->ticks = rs.ticks;
+  out->launches = rs.launches + 3;
+  T.release(st);
+  cudaFreeAsync(d_mats, st);
+  if (d_dt0) cudaFreeAsync(d_dt0, st);
+  cudaFreeAsync(records, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "gradient flow");
+  return rc;
 }
 
 extern "C" int cco_schedule_reset(void) {

@@ -115,6 +115,25 @@ class ServerStatsC(ctypes.Structure):
     )]  # fmt: skip
 
 
+class FlowSettingsC(ctypes.Structure):
+    _fields_ = [
+        ("rtol", ctypes.c_double), ("atol", ctypes.c_double),
+        ("dt_init", ctypes.c_double), ("dt_min", ctypes.c_double),
+        ("dt_max", ctypes.c_double), ("t_max", ctypes.c_double),
+        ("max_steps", ctypes.c_int64), ("energy_tol", ctypes.c_double),
+        ("grad_tol", ctypes.c_double), ("arclength", ctypes.c_int32),
+        ("pad_", ctypes.c_int32), ("record_every", ctypes.c_int64),
+        ("max_records", ctypes.c_int64),
+    ]  # fmt: skip
+
+
+class FlowOutC(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in (
+        "s", "energy", "t", "length", "dt", "n_steps", "n_evals", "status", "traj_s", "traj_t",
+        "traj_length", "traj_energy", "traj_count",
+    )] + [("ticks", ctypes.c_int64), ("launches", ctypes.c_int64)]  # fmt: skip
+
+
 # (name, restype, argtypes) for every symbol include/cco.h declares
 SIGNATURES = {
     "cco_abi_version": (ctypes.c_int, []),
@@ -142,6 +161,11 @@ SIGNATURES = {
          ctypes.POINTER(RelaxOutC)],
     ),  # fmt: skip
     "cco_schedule_reset": (ctypes.c_int, []),
+    "cco_gradient_flow": (
+        ctypes.c_int,
+        [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, ctypes.POINTER(FlowSettingsC),
+         ctypes.POINTER(FlowOutC)],
+    ),  # fmt: skip
     "cco_server_create": (
         ctypes.c_int,
         [ctypes.c_int, ctypes.POINTER(LBFGSSettingsC), ctypes.POINTER(ServerConfigC),
