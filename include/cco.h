@@ -275,6 +275,54 @@ int cco_gradient_flow(cco_problem* const* problems, void* stream, int batch, con
                       cco_flow_out* out);
 
 /*
+ * Molecular-dynamics steps of batch lanes, lane i a configuration of
+ * problems[i] in Cartesian coordinates r = s B (mass 1). Replaces repeated
+ * verlet_step / andersen_reset / baoab_step (src/xla_cco/dynamics/
+ * integrators.py:83-176) with the force F = -dPhi/ds B^-T of
+ * value_grad_density(r B^-1) (dynamics/run.py:219-244); one force evaluation
+ * per step, all steps on the device. Random draws (BAOAB noise, Andersen
+ * coin, particle and velocity row) come from Philox4x32-10 keyed per lane and
+ * counted by step, not from JAX's threefry streams.
+ *   r0, v0   device, packed [N_i][d_i] per lane
+ *   bases    host [batch][d_i][d_i] packed; keys host [batch][2] uint32
+ *   acc0     host [batch] Andersen "count" accumulators, or NULL for 0
+ * Outputs (device): r, v, f packed like r0, and per lane the energy Phi and
+ * kinetic energy of the final state, the largest |E - E0| over the steps,
+ * the Andersen reset count and accumulator, the next key, the status
+ * (CCO_STATUS_BUDGET when the steps are done, CCO_STATUS_DRIFT if
+ * drift_tol > 0 and |E - E0| exceeded it).
+ */
+typedef struct {
+  double dt;
+  int64_t n_steps;
+  int32_t scheme;        /* 0: velocity Verlet, 1: BAOAB */
+  int32_t andersen;      /* 0: off, 1: "count", 2: "bernoulli" (Verlet only) */
+  double andersen_p;
+  double gamma;          /* BAOAB friction */
+  double temperature;
+  double drift_tol;      /* 0: no drift stop */
+} cco_md_settings;
+
+typedef struct {
+  double* r;
+  double* v;
+  double* f;             /* may be NULL */
+  double* energy;
+  double* kinetic;
+  double* max_drift;
+  int64_t* n_resets;
+  double* reset_acc;
+  uint32_t* keys;        /* [batch][2] */
+  int64_t* status;
+  int64_t ticks;         /* out */
+  int64_t launches;      /* out */
+} cco_md_out;
+
+int cco_md_run(cco_problem* const* problems, void* stream, int batch, const double* r0,
+               const double* v0, const double* bases, const uint32_t* keys, const double* acc0,
+               const cco_md_settings* settings, cco_md_out* out);
+
+/*
  * Tick schedules (graph branches, ticks per graph) are tuned online on the
  * first relaxation of each shape class (minimizer, lane count and total
  * N M bucketed by powers of two, largest d) and cached for the process;

@@ -13,6 +13,7 @@
 #include "cco.h"
 #include "cco_internal.cuh"
 #include "cco_flow.cuh"
+#include "cco_md.cuh"
 #include "cco_opt.cuh"
 
 struct cco_problem {
@@ -73,7 +74,7 @@ struct DeviceGuard {
 };
 
 // ------------------------------------------------------------ lane records
-enum class Method { Descent, Lbfgs, Flow };
+enum class Method { Descent, Lbfgs, Flow, Md };
 
 // What every record of one launch shares: the minimizer and, for L-BFGS,
 // the memory m and whether the scalar kernel's triangles live in the record.
@@ -87,6 +88,7 @@ inline size_t record_doubles(const RecordShape& R, const cco_problem* p) {
   size_t n = 0;
   if (R.method == Method::Descent) n = ds_record_doubles(ld, p->M, p->host.ntile1);
   else if (R.method == Method::Flow) n = fl_record_doubles(ld, p->M, p->host.ntile1);
+  else if (R.method == Method::Md) n = md_record_doubles(ld, p->M, p->host.ntile1);
   else n = lb_record_doubles(R.m, R.tri_len, ld, p->M, p->host.ntile1);
   return (n + 31) & ~(size_t)31;   // records start on 256-byte boundaries
 }
@@ -111,6 +113,12 @@ inline EvalLane eval_lane(const RecordShape& R, const LaneRef& L, const cco_prob
     dens = v.dens;
   } else if (R.method == Method::Flow) {
     const FlView v = fl_view(L.rec, L.ld);
+    e.s = v.ps;
+    e.g = v.pg;
+    e.f = v.pf;
+    dens = v.dens;
+  } else if (R.method == Method::Md) {
+    const MdView v = md_view(L.rec, L.ld);
     e.s = v.ps;
     e.g = v.pg;
     e.f = v.pf;
@@ -232,6 +240,7 @@ struct LaneTable {
   DescentArgs ds{};
   LbArgs lb{};
   FlArgs fl{};
+  MdArgs md{};
   int upload_refs(cudaStream_t st);
   void release(cudaStream_t st);
 };
@@ -247,6 +256,7 @@ struct TickPlan {
   DescentArgs ds[kMaxBranches];
   LbArgs lb[kMaxBranches];
   FlArgs fl[kMaxBranches];
+  MdArgs md[kMaxBranches];
   cudaGraphExec_t exec = nullptr;
   int build(const LaneTable& T, const Schedule& sch, cudaStream_t st);
   cudaError_t tick(cudaStream_t s, int b) const;

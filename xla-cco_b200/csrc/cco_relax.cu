@@ -103,6 +103,11 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
       a.B = hi - lo;
       a.lanes = T.d_refs + lo;
       fl[b] = a;
+    } else if (T.shape.method == Method::Md) {
+      MdArgs a = T.md;
+      a.B = hi - lo;
+      a.lanes = T.d_refs + lo;
+      md[b] = a;
     } else if (T.shape.method == Method::Descent) {
       DescentArgs a = T.ds;
       a.B = hi - lo;
@@ -161,6 +166,7 @@ cudaError_t TickPlan::tick(cudaStream_t s, int b) const {
   cudaError_t e = eval_launch(ev[b].plan, s);
   if (e != cudaSuccess) return e;
   if (method == Method::Flow) return flow_update(fl[b], s);
+  if (method == Method::Md) return md_update(md[b], s);
   return method == Method::Descent ? descent_update(ds[b], s) : lbfgs_update(lb[b], s);
 }
 
@@ -304,6 +310,7 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
   C.ds = T.ds;
   C.lb = T.lb;
   C.fl = T.fl;
+  C.md = T.md;
   C.refs = T.refs;
   C.probs = T.probs;
   Schedule chosen, first;
@@ -322,6 +329,8 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
     C.lb.B = (int)C.refs.size();
     C.fl.lanes = C.d_refs;
     C.fl.B = (int)C.refs.size();
+    C.md.lanes = C.d_refs;
+    C.md.B = (int)C.refs.size();
     Schedule s;
     if (force_br > 0 || force_gt > 0) {
       if (force_br > 0) s.branches = force_br;
@@ -797,6 +806,93 @@ extern "C" int cco_gradient_flow(cco_problem* const* problems, void* stream, int
   cudaFreeAsync(records, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "gradient flow");
+  return rc;
+}
+
+extern "C" int cco_md_run(cco_problem* const* problems, void* stream, int batch,
+                          const double* r0, const double* v0, const double* bases,
+                          const uint32_t* keys, const double* acc0, const cco_md_settings* cfg,
+                          cco_md_out* out) {
+  if (!problems || !r0 || !v0 || !bases || !keys || !cfg || !out)
+    return fail(CCO_ERR_ARG, "null argument");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one configuration");
+  if (!out->r || !out->v || !out->energy || !out->kinetic || !out->max_drift || !out->n_resets ||
+      !out->reset_acc || !out->keys || !out->status)
+    return fail(CCO_ERR_ARG, "incomplete output struct");
+  if (!(std::isfinite(cfg->dt) && cfg->dt > 0.0))
+    return fail(CCO_ERR_ARG, "dt must be finite and positive, got %g", cfg->dt);
+  if (cfg->n_steps < 0) return fail(CCO_ERR_ARG, "n_steps must be >= 0");
+  if (cfg->scheme != MD_VERLET && cfg->scheme != MD_BAOAB) return fail(CCO_ERR_ARG, "unknown scheme");
+  if (cfg->andersen < 0 || cfg->andersen > 2) return fail(CCO_ERR_ARG, "unknown Andersen mode");
+  if (cfg->andersen != ANDERSEN_OFF && !(cfg->andersen_p >= 0.0 && cfg->andersen_p <= 1.0))
+    return fail(CCO_ERR_ARG, "p must lie in [0, 1], got %g", cfg->andersen_p);
+  if (cfg->scheme == MD_BAOAB && !(std::isfinite(cfg->gamma) && cfg->gamma >= 0.0))
+    return fail(CCO_ERR_ARG, "gamma must be finite and >= 0, got %g", cfg->gamma);
+  if (!(cfg->temperature >= 0.0)) return fail(CCO_ERR_ARG, "temperature must be >= 0");
+  for (int i = 0; i < batch; ++i)
+    if (!problems[i]) return fail(CCO_ERR_ARG, "null problem for lane %d", i);
+  std::vector<double> mats((size_t)batch * 27);
+  size_t bo = 0;
+  for (int i = 0; i < batch; ++i) {
+    const int d = problems[i]->d;
+    double m27[27];
+    if (!basis_mats(bases + bo, d, m27)) return fail(CCO_ERR_ARG, "singular basis for lane %d", i);
+    // B, B^-1 (= (B^-T)^T), B^-T
+    for (int q = 0; q < 9; ++q) mats[(size_t)i * 27 + q] = m27[q];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        mats[(size_t)i * 27 + 9 + a * 3 + b] = m27[9 + b * 3 + a];
+        mats[(size_t)i * 27 + 18 + a * 3 + b] = m27[9 + a * 3 + b];
+      }
+    bo += (size_t)d * d;
+  }
+  DeviceGuard guard(problems[0]->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  RecordShape shape;
+  shape.method = Method::Md;
+  LaneTable T;
+  MdArgs& a = T.md;
+  a.dt = cfg->dt;
+  a.gamma = cfg->gamma;
+  a.temperature = cfg->temperature;
+  a.andersen_p = cfg->andersen_p;
+  a.drift_tol = cfg->drift_tol;
+  a.n_steps = cfg->n_steps;
+  a.scheme = cfg->scheme;
+  a.andersen = cfg->scheme == MD_VERLET ? cfg->andersen : ANDERSEN_OFF;
+  double* records = nullptr;
+  int rc = make_table(problems, batch, shape, 0, st, &T, &records);
+  if (rc != CCO_OK) {
+    if (records) cudaFreeAsync(records, st);
+    return rc;
+  }
+  a.B = batch;
+  a.lanes = T.d_refs;
+  double* d_mats = nullptr;
+  uint32_t* d_keys = nullptr;
+  double* d_acc = nullptr;
+  CCO_CUDA(upload(&d_mats, mats, st));
+  CCO_CUDA(upload(&d_keys, std::vector<uint32_t>(keys, keys + 2 * (size_t)batch), st));
+  if (acc0) CCO_CUDA(upload(&d_acc, std::vector<double>(acc0, acc0 + batch), st));
+  CCO_CUDA(md_init(a, r0, v0, d_mats, d_keys, d_acc, st));
+  const int64_t max_ticks = 2 + cfg->n_steps + 4 * (kInflight + 1) * 32;
+  RunStats rs;
+  rc = run_lane_table(T, st, max_ticks, &rs);
+  if (rc == CCO_OK) {
+    cudaError_t e = md_finalize(a, out->r, out->v, out->f, out->energy, out->kinetic,
+                                out->max_drift, out->n_resets, out->reset_acc, out->keys,
+                                out->status, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "md_finalize");
+  }
+  out->ticks = rs.ticks;
+  out->launches = rs.launches + 3;
+  T.release(st);
+  cudaFreeAsync(d_mats, st);
+  cudaFreeAsync(d_keys, st);
+  if (d_acc) cudaFreeAsync(d_acc, st);
+  cudaFreeAsync(records, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "md run");
   return rc;
 }
 

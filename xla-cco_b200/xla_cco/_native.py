@@ -134,6 +134,20 @@ class FlowOutC(ctypes.Structure):
     )] + [("ticks", ctypes.c_int64), ("launches", ctypes.c_int64)]  # fmt: skip
 
 
+class MdSettingsC(ctypes.Structure):
+    _fields_ = [
+        ("dt", ctypes.c_double), ("n_steps", ctypes.c_int64), ("scheme", ctypes.c_int32),
+        ("andersen", ctypes.c_int32), ("andersen_p", ctypes.c_double), ("gamma", ctypes.c_double),
+        ("temperature", ctypes.c_double), ("drift_tol", ctypes.c_double),
+    ]  # fmt: skip
+
+
+class MdOutC(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in (
+        "r", "v", "f", "energy", "kinetic", "max_drift", "n_resets", "reset_acc", "keys", "status",
+    )] + [("ticks", ctypes.c_int64), ("launches", ctypes.c_int64)]  # fmt: skip
+
+
 # (name, restype, argtypes) for every symbol include/cco.h declares
 SIGNATURES = {
     "cco_abi_version": (ctypes.c_int, []),
@@ -161,6 +175,11 @@ SIGNATURES = {
          ctypes.POINTER(RelaxOutC)],
     ),  # fmt: skip
     "cco_schedule_reset": (ctypes.c_int, []),
+    "cco_md_run": (
+        ctypes.c_int,
+        [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(MdSettingsC),
+         ctypes.POINTER(MdOutC)],
+    ),  # fmt: skip
     "cco_gradient_flow": (
         ctypes.c_int,
         [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, ctypes.POINTER(FlowSettingsC),
