@@ -539,7 +539,7 @@ def run_serve(args) -> None:
     reqs = request_stream(args.serve_count, seed=SEED, rate=args.serve_rate)
     for r in reqs:
         r.energy.problem_handle(0, r.n)
-    settings = LBFGSSettings(energy_tol=TOL)
+    settings = LBFGSSettings(energy_tol=TOL, precision=args.serve_precision)
     sampler = ClockSampler(0)
     with RelaxServer(settings, hbm_budget_bytes=150 << 30) as srv:
         # warm-up: a few requests through the pool before the stream starts
@@ -567,7 +567,8 @@ def run_serve(args) -> None:
     flops = _flops(evals, reqs)
     peak = fp64_peak_tflops()
     line = {
-        "metric": "served relaxations/s to Phi<1e-20 + p50/p99 latency (Poisson stream, plain FP64)",
+        "metric": "served relaxations/s to Phi<1e-20 + p50/p99 latency (Poisson stream)",
+        "precision": args.serve_precision,
         "value": succ / span, "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": args.warmup,
         "ms_per_step": span * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -634,6 +635,7 @@ def main() -> None:
                     help="mixed workload: also serve the ensemble with mixed precision")  # fmt: skip
     ap.add_argument("--serve-count", type=int, default=200)
     ap.add_argument("--precision-batch", type=int, default=64)
+    ap.add_argument("--serve-precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     args = ap.parse_args()
     if args.profile:
