@@ -660,10 +660,12 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
 
 // Scalar kernel (one CTA per lane): gamma and the coefficients of the
 // direction from the inner products. The lower triangles of SY (s_older .
-// y_newer) and YY are copied row by row into shared memory from the slot
-// matrices (rows are contiguous: SY row = newer slot), then loop 1 runs
-// column-oriented (one shuffle per step) and loop 2 row-oriented (one warp
-// reduction per step); both read contiguous shared-memory rows.
+// y_newer) and YY are gathered from the slot matrices into shared memory in
+// logical (oldest-first) order with every thread keeping eight loads in
+// flight - the slot matrices are usually L2 misses by now, so the gather is
+// latency-bound and needs the parallelism. Loop 1 then runs column-oriented
+// (one shuffle per step) and loop 2 row-oriented; both read contiguous
+// shared-memory rows.
 __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
   extern __shared__ double dsm[];
   __shared__ double av[kScalarMaxPairs], bv[kScalarMaxPairs], alp[kScalarMaxPairs],
@@ -679,28 +681,51 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
   const int k = Lp->hk, m = A.m, head = Lp->hhead;
   double* sc = v.scal;
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
-  // two packings of SY[p][q] = s_p . y_q (p older than q): triSY by newer
-  // rows (tri(p, q) = q (q + 1) / 2 + p) for loop 1, triSO by older rows
-  // (off(p) + q - p, off(p) = p k - p (p - 1) / 2) for loop 2
+  // three packings: triSY (SY[p][q] = s_p . y_q, p older than q) by newer rows
+  // (tri(p, q) = q (q + 1) / 2 + p) for loop 1, triSO by older rows
+  // (off(p) + q - p, off(p) = p k - p (p - 1) / 2) for loop 2, triYY (the
+  // symmetric YY) by newer rows
+  const size_t tri_n = (size_t)m * (m + 1) / 2;
   double* triSY = A.smem_tri ? dsm : v.tri;
-  double* triSO = triSY + (size_t)m * (m + 1) / 2;
-  const double* YYs = v.YY;
+  double* triSO = triSY + tri_n;
+  double* triYY = triSO + tri_n;
   if (k > 0) {
     const double* SYt = v.SY;
+    const double* YYs = v.YY;
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
       sl[p] = (head - k + p + m) % m;
       av[p] = sc[p];
       bv[p] = sc[m + p];
     }
     __syncthreads();
-    for (int q = warp; q < k; q += nwarps) {
-      const double* rs = SYt + (size_t)sl[q] * m;
-      const int base = q * (q + 1) / 2;
-      for (int p = wl; p <= q; p += 32) {
-        const double x = rs[sl[p]];
-        triSY[base + p] = x;
-        triSO[p * k - p * (p - 1) / 2 + (q - p)] = x;
+    const int total = k * (k + 1) / 2;
+    constexpr int U = 8;
+    for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
+      double xs[U], xy[U];
+      int qs[U], ps[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int t = t0 + u * blockDim.x;
+        int q = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+        while (q * (q + 1) / 2 > t) --q;
+        while ((q + 1) * (q + 2) / 2 <= t) ++q;
+        const int p = t - q * (q + 1) / 2;
+        qs[u] = q;
+        ps[u] = p;
+        if (t < total) {
+          xs[u] = SYt[(size_t)sl[q] * m + sl[p]];
+          xy[u] = YYs[(size_t)sl[q] * m + sl[p]];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int t = t0 + u * blockDim.x;
+        if (t < total) {
+          const int q = qs[u], p = ps[u];
+          triSY[t] = xs[u];
+          triYY[t] = xy[u];
+          triSO[p * k - p * (p - 1) / 2 + (q - p)] = xs[u];
+        }
       }
     }
     __syncthreads();
@@ -710,7 +735,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
     }
     if (threadIdx.x == 0) {
       const int n = k - 1;
-      const double num = triSY[tri(n, n)], den = YYs[(size_t)sl[n] * m + sl[n]];
+      const double num = triSY[tri(n, n)], den = triYY[tri(n, n)];
       gam_s = den > 0.0 ? num / den : 1.0;
     }
   } else {
@@ -728,61 +753,68 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
   if (threadIdx.x == 0) sc[2 * m] = gam;
   if (k == 0) return;
   constexpr int R8 = kScalarMaxPairs / 32;
+  // Loops 1 and 2 run on warp 0 with lane l holding the entries p = 32 i + l
+  // in register i. Both are unrolled over i so that every register index is
+  // a compile-time constant: the step's critical path is one multiply, one
+  // shuffle and one FMA.
   if (warp == 0) {
     // loop 1 (newest first): alpha_q = rho_q t_q, then t_p -= alpha_q SY[p][q], p < q
-    double t[R8];
+    double tv[R8];
 #pragma unroll
-    for (int i = 0; i < R8; ++i) t[i] = (32 * i + wl < k) ? av[32 * i + wl] : 0.0;
-    for (int q = k - 1; q >= 0; --q) {
-      const double* row = triSY + q * (q + 1) / 2;
-      const int own = q & 31, oi = q >> 5;
-      double tq = 0.0;
+    for (int i = 0; i < R8; ++i) tv[i] = (32 * i + wl < k) ? av[32 * i + wl] : 0.0;
 #pragma unroll
-      for (int i = 0; i < R8; ++i) tq = (i == oi) ? t[i] : tq;
-      const double aq = __shfl_sync(0xffffffffu, rh[q] * tq, own);
-      if (wl == 0) alp[q] = aq;
+    for (int oi = R8 - 1; oi >= 0; --oi) {
+      if (32 * oi < k) {
+        const int top = min(31, k - 1 - 32 * oi);
+        for (int own = top; own >= 0; --own) {
+          const int q = 32 * oi + own;
+          const double* row = triSY + q * (q + 1) / 2;
+          const double aq = __shfl_sync(0xffffffffu, rh[q] * tv[oi], own);
+          if (wl == 0) alp[q] = aq;
 #pragma unroll
-      for (int i = 0; i < R8; ++i) {
-        const int p = 32 * i + wl;
-        if (p < q) t[i] -= aq * row[p];
+          for (int i = 0; i <= oi; ++i) {
+            const int p = 32 * i + wl;
+            if (p < q) tv[i] -= aq * row[p];
+          }
+        }
       }
     }
   }
   __syncthreads();
-  // t2_p = b_p - sum_q alpha_q YY[p][q] (independent rows: one warp each)
-  // (YY rows are read in place: contiguous in slot order, L2-resident)
-  for (int p = warp; p < k; p += nwarps) {
-    const double* row = YYs + (size_t)sl[p] * m;
+  // t2_p = b_p - sum_q alpha_q YY[p][q] (a thread per p; triYY row r holds
+  // YY[p][r] for p <= r, so q < p reads row p and q >= p reads column p)
+  for (int p = threadIdx.x; p < k; p += blockDim.x) {
+    const double* rp = triYY + p * (p + 1) / 2;
     double acc = 0.0;
-    for (int q = wl; q < k; q += 32) acc += alp[q] * row[sl[q]];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (wl == 0) bet[p] = bv[p] - acc;  // holds t2_p until loop 2 overwrites it
+    for (int q = 0; q < p; ++q) acc += alp[q] * rp[q];
+    for (int q = p; q < k; ++q) acc += alp[q] * triYY[q * (q + 1) / 2 + p];
+    bet[p] = bv[p] - acc;   // holds t2_p until loop 2 overwrites it
   }
   __syncthreads();
   if (warp == 0) {
     // loop 2 (oldest first, column-oriented): beta_p = rho_p (gamma t2_p + u_p),
-    // then u_q += (alpha_p - beta_p) SY[p][q] for every newer q
+    // then u_q += (alpha_p - beta_p) SY[p][q] for every newer q. Every lane
+    // forms the candidate from its own u and the owner's is shuffled out, as
+    // in loop 1 (no divergent owner branch).
     double u[R8];
 #pragma unroll
     for (int i = 0; i < R8; ++i) u[i] = 0.0;
-    for (int p = 0; p < k; ++p) {
-      const double* row = triSO + (p * k - p * (p - 1) / 2) - p;  // row[q] = SY[p][q]
-      const int own = p & 31, oi = p >> 5;
-      double up = 0.0;
 #pragma unroll
-      for (int i = 0; i < R8; ++i) up = (i == oi) ? u[i] : up;
-      double dq = 0.0;
-      if (wl == own) {
-        const double bp = rh[p] * (gam * bet[p] + up);
-        bet[p] = bp;
-        dq = alp[p] - bp;
-      }
-      dq = __shfl_sync(0xffffffffu, dq, own);
+    for (int oi = 0; oi < R8; ++oi) {
+      if (32 * oi < k) {
+        const int top = min(31, k - 1 - 32 * oi);
+        for (int own = 0; own <= top; ++own) {
+          const int p = 32 * oi + own;
+          const double* row = triSO + (p * k - p * (p - 1) / 2) - p;  // row[q] = SY[p][q]
+          const double bp = __shfl_sync(0xffffffffu, rh[p] * (gam * bet[p] + u[oi]), own);
+          const double dq = alp[p] - bp;
+          if (wl == 0) bet[p] = bp;
 #pragma unroll
-      for (int i = 0; i < R8; ++i) {
-        const int q = 32 * i + wl;
-        if (q > p && q < k) u[i] += dq * row[q];
+          for (int i = oi; i < R8; ++i) {
+            const int q = 32 * i + wl;
+            if (q > p && q < k) u[i] += dq * row[q];
+          }
+        }
       }
     }
     __syncwarp();
@@ -923,7 +955,7 @@ cudaError_t descent_finalize(const DescentArgs& a, double* s_out, double* e_out,
   return cudaGetLastError();
 }
 
-size_t lbfgs_update_smem(int m) { return (size_t)m * (m + 1) * sizeof(double); }
+size_t lbfgs_update_smem(int m) { return 3 * ((size_t)m * (m + 1) / 2) * sizeof(double); }
 cudaError_t lbfgs_configure(size_t smem) {
   return cudaFuncSetAttribute(k_lbfgs_scalar, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem);
