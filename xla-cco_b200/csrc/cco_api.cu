@@ -433,6 +433,11 @@ struct EvalWS {
     plan.n_lanes = B;
     plan.n_items1 = B * nt1;
     plan.n_items2 = B * nt2;
+    for (int D = 0; D <= 3; ++D) {
+      plan.d_off1[D] = D >= p->d ? plan.n_items1 : 0;
+      plan.d_off2[D] = D >= p->d ? plan.n_items2 : 0;
+    }
+    plan.dyn_prec = prec == PREC_FP32 ? 1 : 0;
     plan.max_d = p->d;
     plan.smem1 = p->smem1;
     plan.smem2 = eval_smem2(p->host, split);

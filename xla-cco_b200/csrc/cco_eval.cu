@@ -597,27 +597,21 @@ __device__ void pass2_body_f32(const ProbDev& P, const EvalLane& ln, int tile, i
   }
 }
 
+// One kernel per dimension D (and per precision mode) keeps each kernel's
+// code small: the instruction cache holds one body instead of all of them.
+template <int D, bool DYN>
 __global__ void __launch_bounds__(kPass1Threads, 4) k_pass1(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
-  const EvalItem it = plan.items1[blockIdx.x];
+  const EvalItem it = plan.items1[plan.d_off1[D - 1] + blockIdx.x];
   const EvalLane ln = plan.lanes[it.lane];
   if (!lane_active(ln.status)) return;
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
-  if (lane_prec(ln) == PREC_FP32) {
-    switch (sp.d) {
-      case 1: pass1_body_f32<1>(sp, ln, it.tile, smem); break;
-      case 2: pass1_body_f32<2>(sp, ln, it.tile, smem); break;
-      default: pass1_body_f32<3>(sp, ln, it.tile, smem); break;
-    }
-    return;
-  }
-  switch (sp.d) {
-    case 1: pass1_body<1>(sp, ln, it.tile, smem); break;
-    case 2: pass1_body<2>(sp, ln, it.tile, smem); break;
-    default: pass1_body<3>(sp, ln, it.tile, smem); break;
-  }
+  if (DYN && lane_prec(ln) == PREC_FP32)
+    pass1_body_f32<D>(sp, ln, it.tile, smem);
+  else
+    pass1_body<D>(sp, ln, it.tile, smem);
 }
 
 // Reduction (grid: k-chunks x lanes): rho_k = sum over tiles of the pass-1
@@ -666,44 +660,27 @@ __global__ void k_energy(EvalPlan plan) {
   if (threadIdx.x == 0) *ln.f = e / P.vol;
 }
 
+template <int D, bool DYN>
 __global__ void __launch_bounds__(kPass2Threads, 4) k_pass2(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
-  const EvalItem it = plan.items2[blockIdx.x];
+  const EvalItem it = plan.items2[plan.d_off2[D - 1] + blockIdx.x];
   const EvalLane ln = plan.lanes[it.lane];
   if (!lane_active(ln.status) || ln.g == nullptr) return;
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
   const bool staged = (size_t)sp.M * sizeof(double2) <= kPass2RhoStage;
-  if (lane_prec(ln) == PREC_FP32) {
-    if (staged) {
-      switch (sp.d) {
-        case 1: pass2_body_f32<1, true>(sp, ln, it.tile, plan.split2, smem); break;
-        case 2: pass2_body_f32<2, true>(sp, ln, it.tile, plan.split2, smem); break;
-        default: pass2_body_f32<3, true>(sp, ln, it.tile, plan.split2, smem); break;
-      }
-    } else {
-      switch (sp.d) {
-        case 1: pass2_body_f32<1, false>(sp, ln, it.tile, plan.split2, smem); break;
-        case 2: pass2_body_f32<2, false>(sp, ln, it.tile, plan.split2, smem); break;
-        default: pass2_body_f32<3, false>(sp, ln, it.tile, plan.split2, smem); break;
-      }
-    }
+  if (DYN && lane_prec(ln) == PREC_FP32) {
+    if (staged)
+      pass2_body_f32<D, true>(sp, ln, it.tile, plan.split2, smem);
+    else
+      pass2_body_f32<D, false>(sp, ln, it.tile, plan.split2, smem);
     return;
   }
-  if (staged) {
-    switch (sp.d) {
-      case 1: pass2_body<1, true>(sp, ln, it.tile, plan.split2, smem); break;
-      case 2: pass2_body<2, true>(sp, ln, it.tile, plan.split2, smem); break;
-      default: pass2_body<3, true>(sp, ln, it.tile, plan.split2, smem); break;
-    }
-  } else {
-    switch (sp.d) {
-      case 1: pass2_body<1, false>(sp, ln, it.tile, plan.split2, smem); break;
-      case 2: pass2_body<2, false>(sp, ln, it.tile, plan.split2, smem); break;
-      default: pass2_body<3, false>(sp, ln, it.tile, plan.split2, smem); break;
-    }
-  }
+  if (staged)
+    pass2_body<D, true>(sp, ln, it.tile, plan.split2, smem);
+  else
+    pass2_body<D, false>(sp, ln, it.tile, plan.split2, smem);
 }
 
 __global__ void k_rho_scatter(const double2* __restrict__ rho, const int* __restrict__ run2ref,
@@ -755,22 +732,59 @@ int pass2_split(long long tiles_at_split1) {
   return split;
 }
 
-cudaError_t eval_configure() {
-  cudaError_t e = cudaFuncSetAttribute(k_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       227 * 1024 - 1024);
+namespace {
+
+template <int D, bool DYN>
+cudaError_t configure_d() {
+  cudaError_t e = cudaFuncSetAttribute(k_pass1<D, DYN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_pass2<D, DYN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               227 * 1024 - 1024);
 }
 
+template <int D, bool DYN>
+void launch_d(const EvalPlan& plan, bool pass2, cudaStream_t stream) {
+  if (!pass2) {
+    const int n = plan.d_off1[D] - plan.d_off1[D - 1];
+    if (n > 0) k_pass1<D, DYN><<<n, kPass1Threads, plan.smem1, stream>>>(plan);
+  } else {
+    const int n = plan.d_off2[D] - plan.d_off2[D - 1];
+    if (n > 0) k_pass2<D, DYN><<<n, kPass2Threads, plan.smem2, stream>>>(plan);
+  }
+}
+
+void launch_pass(const EvalPlan& plan, bool pass2, cudaStream_t stream) {
+  if (plan.dyn_prec) {
+    launch_d<1, true>(plan, pass2, stream);
+    launch_d<2, true>(plan, pass2, stream);
+    launch_d<3, true>(plan, pass2, stream);
+  } else {
+    launch_d<1, false>(plan, pass2, stream);
+    launch_d<2, false>(plan, pass2, stream);
+    launch_d<3, false>(plan, pass2, stream);
+  }
+}
+
+}  // namespace
+
+cudaError_t eval_configure() {
+  cudaError_t e = configure_d<1, false>();
+  if (e == cudaSuccess) e = configure_d<2, false>();
+  if (e == cudaSuccess) e = configure_d<3, false>();
+  if (e == cudaSuccess) e = configure_d<1, true>();
+  if (e == cudaSuccess) e = configure_d<2, true>();
+  if (e == cudaSuccess) e = configure_d<3, true>();
+  return e;
+}
+
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream) {
-  if (plan.n_items1 > 0) k_pass1<<<plan.n_items1, kPass1Threads, plan.smem1, stream>>>(plan);
+  launch_pass(plan, false, stream);
   if (plan.n_lanes > 0) {
     k_reduce<<<dim3(plan.red_chunks, plan.n_lanes), kReduceChunk, 0, stream>>>(plan);
     k_energy<<<plan.n_lanes, 32, 0, stream>>>(plan);
   }
-  if (plan.want_grad && plan.n_items2 > 0)
-    k_pass2<<<plan.n_items2, kPass2Threads, plan.smem2, stream>>>(plan);
+  if (plan.want_grad) launch_pass(plan, true, stream);
   return cudaGetLastError();
 }
 

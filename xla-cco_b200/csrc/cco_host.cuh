@@ -149,14 +149,14 @@ struct EvalSet {
 
   cudaError_t build(const RecordShape& R, const std::vector<LaneRef>& refs,
                     const std::vector<const cco_problem*>& probs_of, int lo, int hi,
-                    cudaStream_t st) {
+                    cudaStream_t st, bool may_fp32 = false) {
     long long tiles1 = 0;
     for (int i = lo; i < hi; ++i) tiles1 += probs_of[i]->host.ntile2;
     const int split = pass2_split(tiles1);
     std::vector<const cco_problem*> uniq;
     std::vector<ProbDev> pv;
     std::vector<EvalLane> lv;
-    std::vector<EvalItem> i1, i2;
+    std::vector<EvalItem> g1[3], g2[3];   // items grouped by d
     size_t smem1 = 0, smem2 = 0;
     int max_d = 1, max_m = 1;
     for (int i = lo; i < hi; ++i) {
@@ -173,10 +173,19 @@ struct EvalSet {
       }
       const int j = i - lo;
       lv.push_back(eval_lane(R, refs[i], p, u));
-      for (int t = 0; t < p->host.ntile1; ++t) i1.push_back(EvalItem{j, t});
+      for (int t = 0; t < p->host.ntile1; ++t) g1[p->d - 1].push_back(EvalItem{j, t});
       const int nt2 = pass2_tiles(p->host, split);
-      for (int t = 0; t < nt2; ++t) i2.push_back(EvalItem{j, t});
+      for (int t = 0; t < nt2; ++t) g2[p->d - 1].push_back(EvalItem{j, t});
     }
+    std::vector<EvalItem> i1, i2;
+    plan.d_off1[0] = plan.d_off2[0] = 0;
+    for (int D = 0; D < 3; ++D) {
+      i1.insert(i1.end(), g1[D].begin(), g1[D].end());
+      i2.insert(i2.end(), g2[D].begin(), g2[D].end());
+      plan.d_off1[D + 1] = (int)i1.size();
+      plan.d_off2[D + 1] = (int)i2.size();
+    }
+    plan.dyn_prec = may_fp32 ? 1 : 0;
     cudaError_t e = upload(&probs, pv, st);
     if (e == cudaSuccess) e = upload(&lanes, lv, st);
     if (e == cudaSuccess) e = upload(&it1, i1, st);

@@ -129,9 +129,11 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 struct EvalPlan {
   const ProbDev* probs;     // device
   const EvalLane* lanes;    // device
-  const EvalItem* items1;   // device
-  const EvalItem* items2;   // device
+  const EvalItem* items1;   // device, grouped by d: d = D items at [d_off1[D-1], d_off1[D])
+  const EvalItem* items2;   // device, grouped the same way (d_off2)
   int n_lanes, n_items1, n_items2;
+  int d_off1[4], d_off2[4];
+  int dyn_prec;             // 1: lanes may be FP32 (per-lane dispatch), 0: FP64 kernels only
   int max_d;                // largest d in the plan (template dispatch)
   int red_chunks;           // k-chunks of the reduction: ceil(max M / kReduceChunk)
   int split2;               // pass-2 threads per particle (1, 2, 4 or 8)

@@ -95,7 +95,8 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
   bounds = branch_bounds(T.probs, nbr);
   for (int b = 0; b < nbr; ++b) {
     const int lo = bounds[b], hi = bounds[b + 1];
-    CCO_CUDA(ev[b].build(T.shape, T.refs, T.probs, lo, hi, st));
+    const bool may_fp32 = T.shape.method == Method::Lbfgs && T.lb.prec0 == PREC_FP32;
+    CCO_CUDA(ev[b].build(T.shape, T.refs, T.probs, lo, hi, st, may_fp32));
     int nblk = 1;
     for (int i = lo; i < hi; ++i) nblk = std::max(nblk, lb_nblk(T.refs[i].ld));
     if (T.shape.method == Method::Flow) {
