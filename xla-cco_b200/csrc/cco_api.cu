@@ -243,6 +243,7 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
 
   // runs -> segments (headers carry each pass's absolute table rows)
   std::vector<SegHdr> s1, s2;
+  std::vector<GemmRun> runs;
   auto emit = [&](std::vector<SegHdr>& dst, const TabLayout& T, int kstart, int len, int maxlen) {
     for (int off = 0; off < len; off += maxlen) {
       SegHdr h{};
@@ -268,8 +269,63 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     if (brk) {
       emit(s1, P.t1, start, k - start, kSeg1Len);
       emit(s2, P.t2, start, k - start, kSeg2Len);
+      const int* nv = n_vectors + (size_t)order[start] * d;
+      GemmRun g{};
+      g.n0 = d >= 2 ? nv[0] : 0;
+      g.n1 = d >= 3 ? nv[1] : 0;
+      g.a = nv[d - 1];
+      g.b = nv[d - 1] + (k - start) - 1;
+      g.kstart = start;
+      runs.push_back(g);
       start = k;
     }
+  }
+  // GEMM pass 1: runs grouped kGemmRows at a time by length, each group's
+  // last-axis range cut into kGemmCols windows. Used when at least half of
+  // the computed grid cells are k-set rows (CCO_PASS1_GEMM=0 turns it off).
+  std::vector<GemmRun> grun;
+  std::vector<GemmBlock> gblk;
+  {
+    const char* env = getenv("CCO_PASS1_GEMM");
+    const bool allow = d >= 2 && !(env && atoi(env) == 0);
+    int m0 = 1 << 30, M0 = -(1 << 30), m1 = 1 << 30, M1 = -(1 << 30);
+    for (const GemmRun& g : runs) {
+      m0 = std::min(m0, g.n0);
+      M0 = std::max(M0, g.n0);
+      m1 = std::min(m1, g.n1);
+      M1 = std::max(M1, g.n1);
+    }
+    std::vector<GemmRun> sorted = runs;
+    std::stable_sort(sorted.begin(), sorted.end(), [](const GemmRun& x, const GemmRun& y) {
+      return (x.b - x.a) > (y.b - y.a);
+    });
+    for (size_t r0 = 0; r0 < sorted.size(); r0 += kGemmRows) {
+      const int nrun = (int)std::min<size_t>(kGemmRows, sorted.size() - r0);
+      int lo = 1 << 30, hi = -(1 << 30);
+      for (int r = 0; r < nrun; ++r) {
+        lo = std::min(lo, sorted[r0 + r].a);
+        hi = std::max(hi, sorted[r0 + r].b);
+      }
+      const int run0 = (int)grun.size();
+      for (int r = 0; r < nrun; ++r) grun.push_back(sorted[r0 + r]);
+      for (int w = lo; w <= hi; w += kGemmCols) {
+        GemmBlock b{};
+        b.run0 = run0;
+        b.nrun = nrun;
+        b.lo = w;
+        b.nb = std::min(kGemmCols, hi - w + 1);
+        gblk.push_back(b);
+      }
+    }
+    const double cells = (double)gblk.size() * kGemmRows * kGemmCols;
+    const int c0 = M0 - m0 + 1, c1 = d >= 3 ? M1 - m1 + 1 : 0;
+    P.gemm = allow && !runs.empty() && c0 <= kGemmMaxPrefix && c1 <= kGemmMaxPrefix &&
+             (double)m >= 0.5 * cells;
+    P.ngblk = (int)gblk.size();
+    P.gm0 = m0;
+    P.gc0 = c0;
+    P.gm1 = d >= 3 ? m1 : 0;
+    P.gc1 = c1;
   }
   // longest segments first: pass-1 warps share trip counts, pass 2 pairs
   // segments of similar length
@@ -318,6 +374,14 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   if (e == cudaSuccess) e = cudaMemcpy(pr->seg2, s2.data(), s2.size() * sizeof(SegHdr), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(pr->w_run, w_run.data(), m * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(pr->run2ref, r2r.data(), m * sizeof(int), cudaMemcpyHostToDevice);
+  if (P.gemm) {
+    if (e == cudaSuccess) e = cudaMalloc(&pr->grun, grun.size() * sizeof(GemmRun));
+    if (e == cudaSuccess) e = cudaMalloc(&pr->gblk, gblk.size() * sizeof(GemmBlock));
+    if (e == cudaSuccess) e = cudaMemcpy(pr->grun, grun.data(), grun.size() * sizeof(GemmRun), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(pr->gblk, gblk.data(), gblk.size() * sizeof(GemmBlock), cudaMemcpyHostToDevice);
+  }
+  P.grun = pr->grun;
+  P.gblk = pr->gblk;
   P.seg1 = pr->seg1;
   P.seg2 = pr->seg2;
   P.w_run = pr->w_run;
@@ -326,6 +390,7 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   pr->host = P;
   pr->smem1 = smem1;
   pr->smem2 = smem2;
+  pr->smemG = eval_smemG(P);
   if (e != cudaSuccess) {
     cco_problem_destroy(pr);
     return cuda_fail(e, "cco_problem_create upload");
@@ -341,6 +406,8 @@ int cco_problem_destroy(cco_problem* p) {
   cudaFree(p->seg2);
   cudaFree(p->w_run);
   cudaFree(p->run2ref);
+  if (p->grun) cudaFree(p->grun);
+  if (p->gblk) cudaFree(p->gblk);
   cudaFree(p->dev);
   delete p;
   return CCO_OK;
@@ -363,8 +430,9 @@ int cco_problem_info(const cco_problem* p, int* d, int* n_particles, int* m, int
 // ------------------------------------------------------------ eval workspace
 namespace {
 
-__global__ void k_make_lanes(EvalLane* lanes, EvalItem* it1, EvalItem* it2, int B, int nt1,
-                             int nt2, int total, const double* s, size_t s_stride, double* f,
+__global__ void k_make_lanes(EvalLane* lanes, EvalItem* it1, EvalItem* it2, EvalItem* itG,
+                             int B, int nt1, int nt2, int ntG, int total, const double* s,
+                             size_t s_stride, double* f,
                              size_t f_stride, double* g, size_t g_stride, double2* rho,
                              double2* rhow, double2* part, int M, const int64_t* status,
                              size_t status_stride, int prec) {
@@ -387,6 +455,7 @@ __global__ void k_make_lanes(EvalLane* lanes, EvalItem* it1, EvalItem* it2, int 
     if (j >= 0) {
       if (j < B * nt1) it1[j] = EvalItem{j / nt1, j % nt1};
       if (j < B * nt2) it2[j] = EvalItem{j / nt2, j % nt2};
+      if (itG && j < B * ntG) itG[j] = EvalItem{j / ntG, j % ntG};
     }
   }
 }
@@ -396,11 +465,16 @@ struct EvalWS {
   EvalLane* lanes = nullptr;
   EvalItem* it1 = nullptr;
   EvalItem* it2 = nullptr;
+  EvalItem* itG = nullptr;   // GEMM pass-1 items (problems with p->host.gemm)
   double2* rho = nullptr;
   double2* rhow = nullptr;
   double2* part = nullptr;
   EvalPlan plan{};
   int prec = PREC_FP64;   // arithmetic of every lane of this workspace
+
+  static int gemm_tiles(const cco_problem* p) {
+    return p->host.gemm ? p->host.ntile1 * p->host.ngblk : 0;
+  }
 
   // pass-2 threads per particle and tiles per configuration for a batch of B
   static int split_for(const cco_problem* p, int B) {
@@ -411,6 +485,8 @@ struct EvalWS {
     cudaError_t e = pool_alloc(&lanes, sizeof(EvalLane) * B, st);
     if (e == cudaSuccess) e = pool_alloc(&it1, sizeof(EvalItem) * (size_t)B * nt1, st);
     if (e == cudaSuccess) e = pool_alloc(&it2, sizeof(EvalItem) * (size_t)B * nt2, st);
+    if (e == cudaSuccess && gemm_tiles(p) > 0)
+      e = pool_alloc(&itG, sizeof(EvalItem) * (size_t)B * gemm_tiles(p), st);
     if (e == cudaSuccess) e = pool_alloc(&rho, sizeof(double2) * (size_t)B * M, st);
     if (e == cudaSuccess) e = pool_alloc(&rhow, sizeof(double2) * (size_t)B * M, st);
     if (e == cudaSuccess) e = pool_alloc(&part, sizeof(double2) * (size_t)B * nt1 * M, st);
@@ -421,22 +497,29 @@ struct EvalWS {
                     size_t status_stride, cudaStream_t st) {
     const int split = split_for(p, B);
     const int nt1 = p->host.ntile1, nt2 = pass2_tiles(p->host, split);
-    const int total = B * std::max(nt1, nt2) + B;
+    const int ntG = itG ? gemm_tiles(p) : 0;
+    const int total = B * std::max(std::max(nt1, nt2), ntG) + B;
     const int blocks = std::min(1024, (total + 255) / 256);
-    k_make_lanes<<<blocks, 256, 0, st>>>(lanes, it1, it2, B, nt1, nt2, total, s, s_stride, f, f_stride,
-                                         g, g_stride, rho, rhow, part, p->M, status,
-                                         status_stride, prec);
+    k_make_lanes<<<blocks, 256, 0, st>>>(lanes, it1, it2, itG, B, nt1, nt2, ntG, total, s,
+                                         s_stride, f, f_stride, g, g_stride, rho, rhow, part,
+                                         p->M, status, status_stride, prec);
     plan.probs = p->dev;
     plan.lanes = lanes;
     plan.items1 = it1;
     plan.items2 = it2;
+    plan.itemsG = itG;
     plan.n_lanes = B;
-    plan.n_items1 = B * nt1;
+    // the per-segment pass 1 covers FP32 lanes, and FP64 lanes of problems
+    // without the GEMM form
+    plan.n_items1 = (ntG > 0 && prec == PREC_FP64) ? 0 : B * nt1;
     plan.n_items2 = B * nt2;
+    plan.n_itemsG = (prec == PREC_FP64) ? B * ntG : 0;
     for (int D = 0; D <= 3; ++D) {
       plan.d_off1[D] = D >= p->d ? plan.n_items1 : 0;
       plan.d_off2[D] = D >= p->d ? plan.n_items2 : 0;
+      plan.d_offG[D] = D >= p->d ? plan.n_itemsG : 0;
     }
+    plan.smemG = p->smemG;
     plan.dyn_prec = prec == PREC_FP32 ? 1 : 0;
     plan.max_d = p->d;
     plan.smem1 = p->smem1;
@@ -450,10 +533,12 @@ struct EvalWS {
     cudaFreeAsync(lanes, st);
     cudaFreeAsync(it1, st);
     cudaFreeAsync(it2, st);
+    if (itG) cudaFreeAsync(itG, st);
     cudaFreeAsync(rho, st);
     cudaFreeAsync(rhow, st);
     cudaFreeAsync(part, st);
     lanes = nullptr;
+    itG = nullptr;
   }
 };
 
@@ -543,9 +628,10 @@ extern "C" int cco_energy_grad_noalloc(cco_problem* p, void* stream, int batch, 
   const size_t b_lanes = round256(sizeof(EvalLane) * B);
   const size_t b_it1 = round256(sizeof(EvalItem) * B * nt1);
   const size_t b_it2 = round256(sizeof(EvalItem) * B * nt2);
+  const size_t b_itG = round256(sizeof(EvalItem) * B * (size_t)EvalWS::gemm_tiles(p));
   const size_t b_rho = round256(sizeof(double2) * B * M);
   const size_t b_part = round256(sizeof(double2) * B * nt1 * M);
-  const size_t need = b_lanes + b_it1 + b_it2 + 2 * b_rho + b_part;
+  const size_t need = b_lanes + b_it1 + b_it2 + 2 * b_rho + b_part + b_itG;
   if (need > CCO_NOALLOC_SCRATCH_BYTES)
     return fail(CCO_ERR_ARG,
                 "batch %d needs %zu bytes of fixed scratch, the limit is %zu: split the batch",
@@ -562,6 +648,8 @@ extern "C" int cco_energy_grad_noalloc(cco_problem* p, void* stream, int batch, 
   ws.rho = reinterpret_cast<double2*>(base + b_lanes + b_it1 + b_it2);
   ws.rhow = reinterpret_cast<double2*>(base + b_lanes + b_it1 + b_it2 + b_rho);
   ws.part = reinterpret_cast<double2*>(base + b_lanes + b_it1 + b_it2 + 2 * b_rho);
+  ws.itG = b_itG > 0 ? reinterpret_cast<EvalItem*>(base + b_lanes + b_it1 + b_it2 + 2 * b_rho + b_part)
+                     : nullptr;
   const size_t nd = (size_t)p->N * p->d;
   CCO_CUDA(ws.build(p, batch, s, nd, phi, 1, grad, nd, nullptr, 0, st));
   CCO_CUDA(eval_launch(ws.plan, st));

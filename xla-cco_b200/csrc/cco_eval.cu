@@ -597,6 +597,121 @@ __device__ void pass2_body_f32(const ProbDev& P, const EvalLane& ln, int tile, i
   }
 }
 
+// ------------------------------------------------------------ GEMM pass 1
+// Powers dst[e] = exp(2 pi i (base + e) s) for e in [e0, e0 + cnt), cnt <= 8:
+// FP64 sincospi of the exact exponent at e0, products with z after it.
+__device__ __forceinline__ void fill_powers8(double2* dst, int e0, int cnt, int base, double s) {
+  double sn, cs;
+  sincospi(2.0 * s, &sn, &cs);
+  const double2 z = make_double2(cs, sn);
+  sincospi(2.0 * ((double)(base + e0) * s), &sn, &cs);
+  double2 p = make_double2(cs, sn);
+  for (int e = 0; e < cnt; ++e) {
+    dst[e0 + e] = p;
+    p = cmul(p, z);
+  }
+}
+
+// Pass 1 of one (lane, tile, block) as a complex GEMM over the tile's
+// particles, kGemmChunk at a time: the tables of the chunk (prefix powers
+// per axis, last-axis powers for the block's window) and the A rows are
+// built in shared memory, then every thread accumulates a 3 x 3 tile of
+// C[run][n] (runs 3 tr .. 3 tr + 2, columns tn, tn + 16, tn + 32) with four
+// FMAs per complex product. Each grid cell of the k-set is written once.
+template <int D>
+__device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, int blk,
+                                double2* smem) {
+  constexpr int KC = kGemmChunk;
+  const GemmBlock B = P.gblk[blk];
+  const int j0 = tile * kPass1Tile;
+  const int nj = min(kPass1Tile, P.N - j0);
+  const int c0 = P.gc0, c1 = D == 3 ? P.gc1 : 0;
+  double2* T0 = smem;                       // [KC][c0]
+  double2* T1 = T0 + KC * c0;               // [KC][c1]
+  double2* Z = T1 + KC * c1;                // [KC][kGemmCols]
+  double2* A = Z + KC * kGemmCols;          // [KC][kGemmRows]
+  const int tr = threadIdx.x >> 4, tn = threadIdx.x & 15;
+  double2 acc[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[i][c] = make_double2(0.0, 0.0);
+  const int u0 = (c0 + 7) >> 3, u1 = (c1 + 7) >> 3, uz = kGemmCols >> 3;
+  for (int jc = 0; jc < nj; jc += KC) {
+    const int kc = min(KC, nj - jc);
+    __syncthreads();   // the previous chunk's products are done
+    for (int u = threadIdx.x; u < KC * (u0 + u1 + uz); u += blockDim.x) {
+      const int j = u % KC, q = u / KC;
+      const double* sj = ln.s + (size_t)(j0 + jc + j) * D;
+      const bool live = j < kc;
+      if (q < u0) {
+        fill_powers8(T0 + j * c0, 8 * q, min(8, c0 - 8 * q), P.gm0, live ? sj[0] : 0.0);
+      } else if (q < u0 + u1) {
+        const int qq = q - u0;
+        fill_powers8(T1 + j * c1, 8 * qq, min(8, c1 - 8 * qq), P.gm1, live ? sj[1] : 0.0);
+      } else {
+        const int qq = q - u0 - u1;
+        fill_powers8(Z + j * kGemmCols, 8 * qq, 8, B.lo, live ? sj[D - 1] : 0.0);
+      }
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < KC * kGemmRows; u += blockDim.x) {
+      const int j = u / kGemmRows, r = u - j * kGemmRows;
+      double2 v = make_double2(0.0, 0.0);
+      if (j < kc && r < B.nrun) {
+        const GemmRun g = P.grun[B.run0 + r];
+        v = T0[j * c0 + (g.n0 - P.gm0)];
+        if (D == 3) v = cmul(v, T1[j * c1 + (g.n1 - P.gm1)]);
+      }
+      A[j * kGemmRows + r] = v;
+    }
+    __syncthreads();
+    for (int j = 0; j < kc; ++j) {
+      double2 a[3], z[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) a[i] = A[j * kGemmRows + 3 * tr + i];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) z[c] = Z[j * kGemmCols + tn + 16 * c];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          acc[i][c].x = fma(a[i].x, z[c].x, acc[i][c].x);
+          acc[i][c].x = fma(-a[i].y, z[c].y, acc[i][c].x);
+          acc[i][c].y = fma(a[i].x, z[c].y, acc[i][c].y);
+          acc[i][c].y = fma(a[i].y, z[c].x, acc[i][c].y);
+        }
+    }
+  }
+  double2* out = ln.part + (size_t)tile * P.M;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int r = 3 * tr + i;
+    if (r < B.nrun) {
+      const GemmRun g = P.grun[B.run0 + r];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int col = tn + 16 * c;
+        const int n = B.lo + col;
+        if (col < B.nb && n >= g.a && n <= g.b) out[g.kstart + (n - g.a)] = acc[i][c];
+      }
+    }
+  }
+}
+
+template <int D>
+__global__ void __launch_bounds__(kGemmThreads, 4) k_pass1_gemm(EvalPlan plan) {
+  extern __shared__ double2 smem[];
+  __shared__ ProbDev sp;
+  const EvalItem it = plan.itemsG[plan.d_offG[D - 1] + blockIdx.x];
+  const EvalLane ln = plan.lanes[it.lane];
+  if (!lane_active(ln.status)) return;
+  if (plan.dyn_prec && lane_prec(ln) == PREC_FP32) return;   // the FP32 body handles it
+  if (threadIdx.x == 0) sp = plan.probs[ln.prob];
+  __syncthreads();
+  pass1_gemm_body<D>(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
+}
+
 // One kernel per dimension D (and per precision mode) keeps each kernel's
 // code small: the instruction cache holds one body instead of all of them.
 template <int D, bool DYN>
@@ -610,8 +725,8 @@ __global__ void __launch_bounds__(kPass1Threads, 4) k_pass1(EvalPlan plan) {
   __syncthreads();
   if (DYN && lane_prec(ln) == PREC_FP32)
     pass1_body_f32<D>(sp, ln, it.tile, smem);
-  else
-    pass1_body<D>(sp, ln, it.tile, smem);
+  else if (!sp.gemm)
+    pass1_body<D>(sp, ln, it.tile, smem);   // GEMM problems: k_pass1_gemm
 }
 
 // Reduction (grid: k-chunks x lanes): rho_k = sum over tiles of the pass-1
@@ -710,6 +825,12 @@ size_t eval_smem1(const ProbDev& p) {
   return ((size_t)p.t1.nrows * kPass1Stride + red) * sizeof(double2);
 }
 
+size_t eval_smemG(const ProbDev& p) {
+  if (!p.gemm) return 0;
+  const int c1 = p.d == 3 ? p.gc1 : 0;
+  return (size_t)kGemmChunk * (p.gc0 + c1 + kGemmCols + kGemmRows) * sizeof(double2);
+}
+
 size_t eval_smem2(const ProbDev& p, int split) {
   const size_t rho = (size_t)p.M * sizeof(double2);
   const size_t comb = split > 1 ? (size_t)kPass2Tile * p.d * sizeof(double) : 0;
@@ -769,7 +890,12 @@ void launch_pass(const EvalPlan& plan, bool pass2, cudaStream_t stream) {
 }  // namespace
 
 cudaError_t eval_configure() {
-  cudaError_t e = configure_d<1, false>();
+  cudaError_t e = cudaFuncSetAttribute(k_pass1_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       227 * 1024 - 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_pass1_gemm<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024 - 1024);
+  if (e == cudaSuccess) e = configure_d<1, false>();
   if (e == cudaSuccess) e = configure_d<2, false>();
   if (e == cudaSuccess) e = configure_d<3, false>();
   if (e == cudaSuccess) e = configure_d<1, true>();
@@ -780,6 +906,11 @@ cudaError_t eval_configure() {
 
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream) {
   launch_pass(plan, false, stream);
+  {
+    const int n2 = plan.d_offG[2] - plan.d_offG[1], n3 = plan.d_offG[3] - plan.d_offG[2];
+    if (n2 > 0) k_pass1_gemm<2><<<n2, kGemmThreads, plan.smemG, stream>>>(plan);
+    if (n3 > 0) k_pass1_gemm<3><<<n3, kGemmThreads, plan.smemG, stream>>>(plan);
+  }
   if (plan.n_lanes > 0) {
     k_reduce<<<dim3(plan.red_chunks, plan.n_lanes), kReduceChunk, 0, stream>>>(plan);
     k_energy<<<plan.n_lanes, 32, 0, stream>>>(plan);

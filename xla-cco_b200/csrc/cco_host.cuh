@@ -25,7 +25,9 @@ struct cco_problem {
   cco::SegHdr* seg2 = nullptr;
   double* w_run = nullptr;
   int* run2ref = nullptr;
-  size_t smem1 = 0, smem2 = 0;
+  cco::GemmRun* grun = nullptr;
+  cco::GemmBlock* gblk = nullptr;
+  size_t smem1 = 0, smem2 = 0, smemG = 0;
 };
 
 namespace cco {
@@ -145,6 +147,7 @@ struct EvalSet {
   EvalLane* lanes = nullptr;
   EvalItem* it1 = nullptr;
   EvalItem* it2 = nullptr;
+  EvalItem* itG = nullptr;
   EvalPlan plan{};
 
   cudaError_t build(const RecordShape& R, const std::vector<LaneRef>& refs,
@@ -156,8 +159,8 @@ struct EvalSet {
     std::vector<const cco_problem*> uniq;
     std::vector<ProbDev> pv;
     std::vector<EvalLane> lv;
-    std::vector<EvalItem> g1[3], g2[3];   // items grouped by d
-    size_t smem1 = 0, smem2 = 0;
+    std::vector<EvalItem> g1[3], g2[3], gG[3];   // items grouped by d
+    size_t smem1 = 0, smem2 = 0, smemG = 0;
     int max_d = 1, max_m = 1;
     for (int i = lo; i < hi; ++i) {
       const cco_problem* p = probs_of[i];
@@ -168,32 +171,45 @@ struct EvalSet {
         pv.push_back(p->host);
         smem1 = std::max(smem1, p->smem1);
         smem2 = std::max(smem2, eval_smem2(p->host, split));
+        smemG = std::max(smemG, p->smemG);
         max_d = std::max(max_d, p->d);
         max_m = std::max(max_m, p->M);
       }
       const int j = i - lo;
       lv.push_back(eval_lane(R, refs[i], p, u));
-      for (int t = 0; t < p->host.ntile1; ++t) g1[p->d - 1].push_back(EvalItem{j, t});
+      if (p->host.gemm) {
+        const int ntG = p->host.ntile1 * p->host.ngblk;
+        for (int t = 0; t < ntG; ++t) gG[p->d - 1].push_back(EvalItem{j, t});
+      }
+      // the per-segment pass 1: FP32 lanes, and problems without the GEMM form
+      if (!p->host.gemm || may_fp32)
+        for (int t = 0; t < p->host.ntile1; ++t) g1[p->d - 1].push_back(EvalItem{j, t});
       const int nt2 = pass2_tiles(p->host, split);
       for (int t = 0; t < nt2; ++t) g2[p->d - 1].push_back(EvalItem{j, t});
     }
-    std::vector<EvalItem> i1, i2;
-    plan.d_off1[0] = plan.d_off2[0] = 0;
+    std::vector<EvalItem> i1, i2, iG;
+    plan.d_off1[0] = plan.d_off2[0] = plan.d_offG[0] = 0;
     for (int D = 0; D < 3; ++D) {
       i1.insert(i1.end(), g1[D].begin(), g1[D].end());
       i2.insert(i2.end(), g2[D].begin(), g2[D].end());
+      iG.insert(iG.end(), gG[D].begin(), gG[D].end());
       plan.d_off1[D + 1] = (int)i1.size();
       plan.d_off2[D + 1] = (int)i2.size();
+      plan.d_offG[D + 1] = (int)iG.size();
     }
     plan.dyn_prec = may_fp32 ? 1 : 0;
     cudaError_t e = upload(&probs, pv, st);
     if (e == cudaSuccess) e = upload(&lanes, lv, st);
     if (e == cudaSuccess) e = upload(&it1, i1, st);
     if (e == cudaSuccess) e = upload(&it2, i2, st);
+    if (e == cudaSuccess) e = upload(&itG, iG, st);
     plan.probs = probs;
     plan.lanes = lanes;
     plan.items1 = it1;
     plan.items2 = it2;
+    plan.itemsG = itG;
+    plan.n_itemsG = (int)iG.size();
+    plan.smemG = smemG;
     plan.n_lanes = hi - lo;
     plan.n_items1 = (int)i1.size();
     plan.n_items2 = (int)i2.size();
@@ -210,6 +226,8 @@ struct EvalSet {
     if (lanes) cudaFreeAsync(lanes, st);
     if (it1) cudaFreeAsync(it1, st);
     if (it2) cudaFreeAsync(it2, st);
+    if (itG) cudaFreeAsync(itG, st);
+    itG = nullptr;
     probs = nullptr;
     lanes = nullptr;
     it1 = it2 = nullptr;

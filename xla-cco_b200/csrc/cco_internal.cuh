@@ -42,6 +42,21 @@ struct SegHdr {
 };
 static_assert(sizeof(SegHdr) == 32, "segment header is two 16-byte loads");
 
+// Pass 1 as a complex GEMM (problems where it is efficient, FP64 lanes): the
+// density of a particle tile on the grid (run r, last-axis n) is
+// C[r][n] = sum_j A[r][j] Z[n][j] with A the run's prefix phase and Z the
+// last-axis power z_j^n. Runs are grouped kGemmRows at a time (sorted by
+// length) and each group's last-axis range is cut into windows of kGemmCols;
+// a (group, window) is a block, one CTA per (lane, tile, block).
+constexpr int kGemmRows = 24, kGemmCols = 48, kGemmChunk = 16, kGemmThreads = 128;
+constexpr int kGemmMaxPrefix = 128;   // table entries per prefix axis
+struct GemmRun {
+  int n0, n1, a, b, kstart, pad_;   // prefix (n0[, n1]), last-axis range [a, b]
+};
+struct GemmBlock {
+  int run0, nrun, lo, nb;            // runs [run0, run0 + nrun), columns lo .. lo + nb - 1
+};
+
 // Per-particle phase tables of one pass: row r holds z_a^(e * base^l) for one
 // (axis a, level l, entry e); level 0 always holds z^0 .. z^(base-1).
 struct TabLayout {
@@ -59,6 +74,10 @@ struct ProbDev {
   TabLayout t1, t2;          // pass-1 / pass-2 table layouts
   int ntile1, ntile2;        // particle tiles of pass 1 / pass 2 (pass 2 at split 1)
   int sl2;                   // logical slices of the pass-2 segment pairs (power of 2, <= 8)
+  int gemm;                  // 1: FP64 pass 1 runs as the GEMM below
+  int ngblk, gm0, gc0, gm1, gc1;   // GEMM blocks; prefix tables [gm, gm + gc) per axis
+  const GemmBlock* gblk;
+  const GemmRun* grun;
   double vol;                // V
   double gpref;              // 2 (2 pi) / V
   const SegHdr* seg1;
@@ -133,6 +152,10 @@ struct EvalPlan {
   const EvalItem* items2;   // device, grouped the same way (d_off2)
   int n_lanes, n_items1, n_items2;
   int d_off1[4], d_off2[4];
+  const EvalItem* itemsG;   // GEMM pass-1 items (lane, tile * ngblk + block), grouped by d
+  int n_itemsG;
+  int d_offG[4];
+  size_t smemG;
   int dyn_prec;             // 1: lanes may be FP32 (per-lane dispatch), 0: FP64 kernels only
   int max_d;                // largest d in the plan (template dispatch)
   int red_chunks;           // k-chunks of the reduction: ceil(max M / kReduceChunk)
@@ -151,6 +174,7 @@ __host__ __device__ __forceinline__ int reduce_chunks(int M) {
 
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream);
 size_t eval_smem1(const ProbDev& p);
+size_t eval_smemG(const ProbDev& p);   // GEMM pass 1 (0 when the problem has none)
 size_t eval_smem2(const ProbDev& p, int split);
 // Pass-2 tiles of one configuration when `split` threads share a particle.
 int pass2_tiles(const ProbDev& p, int split);
