@@ -389,6 +389,25 @@ int cco_server_poll(cco_server* server, int64_t ticket, int timeout_ms, cco_requ
 int cco_server_cancel(cco_server* server, int64_t ticket);
 int cco_server_get_stats(cco_server* server, cco_server_stats* out);
 
+/*
+ * Minimum-image pair statistics of a batch (the g2 and Hp inputs of the
+ * ground-state driver), on the device.
+ *   cco_pair_histogram   <- pair_distance_histogram   src/xla_cco/analysis/pairs.py:66-110
+ *   cco_nearest_neighbor <- nearest_neighbor_distances src/xla_cco/analysis/pairs.py:41-63
+ * s: device [batch][n][d] fractional positions wrapped to [0, 1); basis: host
+ * [d][d], rows = lattice vectors. Distances use ds - round(ds) and the 3^d
+ * image shifts (exact for reduced cells, as the reference). edges: host,
+ * n_edges >= 2, finite, non-negative, strictly increasing; counts: device
+ * int64 [n_edges - 1], overwritten with the counts of all pairs i < j summed
+ * over the batch (np.histogram bins: left-closed, the last one closed).
+ * out: device [batch][n] nearest-neighbour distances (a lone particle sees
+ * its own images). batch <= 65535.
+ */
+int cco_pair_histogram(int device, void* stream, int batch, int n, int d, const double* s,
+                       const double* basis, int n_edges, const double* edges, int64_t* counts);
+int cco_nearest_neighbor(int device, void* stream, int batch, int n, int d, const double* s,
+                         const double* basis, double* out);
+
 #ifdef __cplusplus
 }
 #endif

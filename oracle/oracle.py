@@ -8,7 +8,17 @@ path. Wraps ``cco_oracle.c`` (built by ``oracle/build.py`` into
 * ``halfspace_kvectors``: brute-force k scan (``tests/oracle.py:114-150`` of
   the reference), independent of the product's vectorized enumeration;
 * ``energy_direct``: NumPy direct sum of the trig path
-  (``src/xla_cco/energy.py:45-50,301-324``), for small cases.
+  (``src/xla_cco/energy.py:45-50,301-324``), for small cases;
+* ``structure_factor_direct``, ``isotropic_kset``, ``bin_moments``: S(k)
+  by direct sums, the C++ ``GetKs`` k-set by brute force and the C++ S(k)
+  binning in plain Python (``src/xla_cco/analysis/structure.py:44-201``);
+* ``min_image_distances``: minimum-image pair and nearest-neighbour
+  distances (``src/xla_cco/analysis/pairs.py:41-188``).
+
+Parity pins (tests/golden/io_golden.*, generated from the reference by
+``tests/golden/make_io_golden.py``): the reference's own ``_isotropic_kset``
+and ``_bin_moments`` outputs, its oracle's pair distances and S(k), and its
+ConfigPack and table writers' bytes.
 
 Parity pins (tests/golden/, generated from the reference by
 ``tests/golden/make_golden.py``): C++ golden energies of
@@ -336,3 +346,97 @@ def gradient_flow_dopri5(s0: np.ndarray, n: np.ndarray, w: np.ndarray, volume: f
                 rows.append((s.copy(), t, length, f))
         out["trajectory"] = rows
     return out
+
+
+# ------------------------------------------------------------------ analysis
+
+
+def structure_factor_direct(s: np.ndarray, n: np.ndarray) -> np.ndarray:
+    """S(n) = |sum_j exp(2 pi i n . s_j)|^2 / N by direct NumPy sums (small cases)."""
+    theta = 2.0 * math.pi * (np.asarray(n, dtype=np.float64) @ s.T)
+    re, im = np.cos(theta).sum(1), np.sin(theta).sum(1)
+    return (re * re + im * im) / s.shape[0]
+
+
+def isotropic_kset(basis: np.ndarray, k_dir: float, k_max: float):
+    """C++ ``GetKs`` by brute force: primitive half-space vectors with |k| < k_dir
+    ordered by (|k|^2, n_0, n_1, ...), each followed by its multiples i n while
+    |i k|^2 <= k_max^2 (summed component by component). d = 1: the one
+    direction n = 1 whatever k_dir."""
+    dim = basis.shape[0]
+    recip = reciprocal_basis(basis)
+    if dim == 1:
+        prim = [np.array([1], dtype=np.int64)]
+    else:
+        found, ksq = halfspace_kvectors(basis, 0.0, k_dir)
+        order = sorted(range(len(ksq)), key=lambda i: (ksq[i], tuple(found[i])))
+        prim = []
+        for i in order:
+            g = 0
+            for c in found[i]:
+                g = math.gcd(g, abs(int(c)))
+            if g == 1:
+                prim.append(found[i])
+    rows, sq = [], []
+    for nv in prim:
+        kv = nv.astype(np.float64) @ recip if dim > 1 else np.array([recip[0, 0]])
+        i = 1
+        while True:
+            q = 0.0
+            for c in range(dim):
+                comp = float(i) * float(kv[c])
+                q += comp * comp
+            if q > k_max * k_max:
+                break
+            rows.append([float(i) * float(x) for x in nv])
+            sq.append(q)
+            i += 1
+    return np.array(rows, dtype=np.float64), np.array(sq, dtype=np.float64)
+
+
+def bin_moments(k: np.ndarray, s_mean: np.ndarray, s2_mean: np.ndarray, n_cfg: int,
+                width: float):
+    """C++ S(k) binning in plain Python: per bin floor(|k| / width), totals over k
+    and configurations, mean |k|, mean S, SEM of |k| (0 unless the variance is
+    positive) and SEM of S (NaN for a negative variance)."""
+    acc: dict[int, list[float]] = {}
+    for kk, sm, s2 in zip(k.tolist(), s_mean.tolist(), s2_mean.tolist()):
+        b = int(math.floor(kk / width))
+        a = acc.setdefault(b, [0.0, 0.0, 0.0, 0.0, 0.0])
+        a[0] += 1.0
+        a[1] += kk
+        a[2] += sm
+        a[3] += kk * kk
+        a[4] += s2
+    cols: list[list[float]] = [[], [], [], []]
+    for b in sorted(acc):
+        a = acc[b]
+        cnt = a[0] * float(n_cfg)
+        mk, ms = a[1] * n_cfg / cnt, a[2] * n_cfg / cnt
+        vk = (a[3] * n_cfg / cnt - mk * mk) / cnt
+        vs = (a[4] * n_cfg / cnt - ms * ms) / cnt
+        cols[0].append(mk)
+        cols[1].append(ms)
+        cols[2].append(math.sqrt(vk) if vk > 0.0 else 0.0)
+        cols[3].append(math.sqrt(vs) if vs >= 0.0 else math.nan)
+    return tuple(np.array(c) for c in cols)
+
+
+def min_image_distances(s: np.ndarray, basis: np.ndarray):
+    """(nearest-neighbour distance per particle (N,), distances of pairs i < j
+    in row order) with ds - round(ds) and the 3^d image shifts; a particle's
+    own zero shift is excluded (a lone particle sees its images)."""
+    n, dim = s.shape
+    shifts = np.array(list(itertools.product((-1.0, 0.0, 1.0), repeat=dim)))
+    ds = s[None, :, :] - s[:, None, :]
+    ds = ds - np.round(ds)
+    best = np.full((n, n), np.inf)
+    for sh in shifts:
+        v = (ds + sh) @ basis
+        r2 = (v * v).sum(-1)
+        if not sh.any():
+            r2 = np.where(np.eye(n, dtype=bool), np.inf, r2)
+        best = np.minimum(best, r2)
+    dist = np.sqrt(best)
+    iu = np.triu_indices(n, 1)
+    return dist.min(axis=1), dist[iu]

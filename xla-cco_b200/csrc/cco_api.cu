@@ -326,6 +326,23 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     P.gc0 = c0;
     P.gm1 = d >= 3 ? m1 : 0;
     P.gc1 = c1;
+    P.gs0 = c0 | 1;
+    P.gs1 = c1 > 0 ? (c1 | 1) : 0;
+    // fill units: the fewest rounds of one unit per thread, then the
+    // shortest chains (each unit seeds with sincospi, then multiplies)
+    const int per_round = kGemmThreads / kGemmChunk;
+    bool found = false;
+    for (int rounds = 1; !found; ++rounds)
+      for (int L = 8; L <= kGemmMaxRun && !found; ++L) {
+        const int u0 = (c0 + L - 1) / L, u1 = (c1 + L - 1) / L, uz = (kGemmCols + L - 1) / L;
+        if (u0 + u1 + uz <= per_round * rounds) {
+          P.gL = L;
+          P.gu0 = u0;
+          P.gu1 = u1;
+          P.guz = uz;
+          found = true;
+        }
+      }
   }
   // longest segments first: pass-1 warps share trip counts, pass 2 pairs
   // segments of similar length

@@ -598,17 +598,27 @@ __device__ void pass2_body_f32(const ProbDev& P, const EvalLane& ln, int tile, i
 }
 
 // ------------------------------------------------------------ GEMM pass 1
-// Powers dst[e] = exp(2 pi i (base + e) s) for e in [e0, e0 + cnt), cnt <= 8:
-// FP64 sincospi of the exact exponent at e0, products with z after it.
-__device__ __forceinline__ void fill_powers8(double2* dst, int e0, int cnt, int base, double s) {
+// Powers dst[e] = exp(2 pi i (base + e) s) for e in [e0, e0 + cnt): FP64
+// sincospi of the exact exponent at e0, products with z = exp(2 pi i s) after it.
+__device__ __forceinline__ void fill_powers(double2* dst, int e0, int cnt, int base, double s,
+                                            double2 z) {
   double sn, cs;
-  sincospi(2.0 * s, &sn, &cs);
-  const double2 z = make_double2(cs, sn);
   sincospi(2.0 * ((double)(base + e0) * s), &sn, &cs);
   double2 p = make_double2(cs, sn);
   for (int e = 0; e < cnt; ++e) {
     dst[e0 + e] = p;
     p = cmul(p, z);
+  }
+}
+
+// z = exp(2 pi i s) per (particle, axis) of the chunk starting at particle jb.
+template <int D>
+__device__ __forceinline__ void chunk_roots(double2* zs, const double* s, int jb, int kc) {
+  for (int u = threadIdx.x; u < kGemmChunk * D; u += blockDim.x) {
+    const int j = u / D;
+    double sn = 0.0, cs = 1.0;
+    if (j < kc) sincospi(2.0 * s[(size_t)jb * D + u], &sn, &cs);
+    zs[u] = make_double2(cs, sn);
   }
 }
 
@@ -618,6 +628,7 @@ __device__ __forceinline__ void fill_powers8(double2* dst, int e0, int cnt, int 
 // built in shared memory, then every thread accumulates a 3 x 3 tile of
 // C[run][n] (runs 3 tr .. 3 tr + 2, columns tn, tn + 16, tn + 32) with four
 // FMAs per complex product. Each grid cell of the k-set is written once.
+// The roots z of the next chunk are formed while the A rows are built.
 template <int D>
 __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, int blk,
                                 double2* smem) {
@@ -626,32 +637,40 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
   const int j0 = tile * kPass1Tile;
   const int nj = min(kPass1Tile, P.N - j0);
   const int c0 = P.gc0, c1 = D == 3 ? P.gc1 : 0;
-  double2* T0 = smem;                       // [KC][c0]
-  double2* T1 = T0 + KC * c0;               // [KC][c1]
-  double2* Z = T1 + KC * c1;                // [KC][kGemmCols]
-  double2* A = Z + KC * kGemmCols;          // [KC][kGemmRows]
+  const int s0 = P.gs0, s1 = D == 3 ? P.gs1 : 0;
+  double2* T0 = smem;                       // [KC][s0]
+  double2* T1 = T0 + KC * s0;               // [KC][s1]
+  double2* Z = T1 + KC * s1;                // [KC][kGemmZStride]
+  double2* A = Z + KC * kGemmZStride;       // [KC][kGemmRows]
+  double2* R = A + KC * kGemmRows;          // [2][KC * D] roots, double-buffered
   const int tr = threadIdx.x >> 4, tn = threadIdx.x & 15;
   double2 acc[3][3];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[i][c] = make_double2(0.0, 0.0);
-  const int u0 = (c0 + 7) >> 3, u1 = (c1 + 7) >> 3, uz = kGemmCols >> 3;
+  const int L = P.gL, u0 = P.gu0, u1 = D == 3 ? P.gu1 : 0, uz = P.guz;
+  chunk_roots<D>(R, ln.s, j0, min(KC, nj));
+  int buf = 0;
   for (int jc = 0; jc < nj; jc += KC) {
     const int kc = min(KC, nj - jc);
-    __syncthreads();   // the previous chunk's products are done
+    const double2* zs = R + buf * KC * D;
+    __syncthreads();   // the previous chunk's products and this chunk's roots are done
     for (int u = threadIdx.x; u < KC * (u0 + u1 + uz); u += blockDim.x) {
       const int j = u % KC, q = u / KC;
       const double* sj = ln.s + (size_t)(j0 + jc + j) * D;
       const bool live = j < kc;
       if (q < u0) {
-        fill_powers8(T0 + j * c0, 8 * q, min(8, c0 - 8 * q), P.gm0, live ? sj[0] : 0.0);
+        fill_powers(T0 + j * s0, L * q, min(L, c0 - L * q), P.gm0, live ? sj[0] : 0.0,
+                    zs[j * D]);
       } else if (q < u0 + u1) {
         const int qq = q - u0;
-        fill_powers8(T1 + j * c1, 8 * qq, min(8, c1 - 8 * qq), P.gm1, live ? sj[1] : 0.0);
+        fill_powers(T1 + j * s1, L * qq, min(L, c1 - L * qq), P.gm1, live ? sj[1] : 0.0,
+                    zs[j * D + 1]);
       } else {
         const int qq = q - u0 - u1;
-        fill_powers8(Z + j * kGemmCols, 8 * qq, 8, B.lo, live ? sj[D - 1] : 0.0);
+        fill_powers(Z + j * kGemmZStride, L * qq, min(L, kGemmCols - L * qq), B.lo,
+                    live ? sj[D - 1] : 0.0, zs[j * D + D - 1]);
       }
     }
     __syncthreads();
@@ -660,18 +679,20 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
       double2 v = make_double2(0.0, 0.0);
       if (j < kc && r < B.nrun) {
         const GemmRun g = P.grun[B.run0 + r];
-        v = T0[j * c0 + (g.n0 - P.gm0)];
-        if (D == 3) v = cmul(v, T1[j * c1 + (g.n1 - P.gm1)]);
+        v = T0[j * s0 + (g.n0 - P.gm0)];
+        if (D == 3) v = cmul(v, T1[j * s1 + (g.n1 - P.gm1)]);
       }
       A[j * kGemmRows + r] = v;
     }
+    if (jc + KC < nj) chunk_roots<D>(R + (buf ^ 1) * KC * D, ln.s, j0 + jc + KC, min(KC, nj - jc - KC));
+    buf ^= 1;
     __syncthreads();
     for (int j = 0; j < kc; ++j) {
       double2 a[3], z[3];
 #pragma unroll
       for (int i = 0; i < 3; ++i) a[i] = A[j * kGemmRows + 3 * tr + i];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) z[c] = Z[j * kGemmCols + tn + 16 * c];
+      for (int c = 0; c < 3; ++c) z[c] = Z[j * kGemmZStride + tn + 16 * c];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -827,8 +848,9 @@ size_t eval_smem1(const ProbDev& p) {
 
 size_t eval_smemG(const ProbDev& p) {
   if (!p.gemm) return 0;
-  const int c1 = p.d == 3 ? p.gc1 : 0;
-  return (size_t)kGemmChunk * (p.gc0 + c1 + kGemmCols + kGemmRows) * sizeof(double2);
+  const int s1 = p.d == 3 ? p.gs1 : 0;
+  return (size_t)kGemmChunk * (p.gs0 + s1 + kGemmZStride + kGemmRows + 2 * p.d) *
+         sizeof(double2);
 }
 
 size_t eval_smem2(const ProbDev& p, int split) {

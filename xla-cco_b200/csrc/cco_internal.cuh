@@ -49,7 +49,9 @@ static_assert(sizeof(SegHdr) == 32, "segment header is two 16-byte loads");
 // length) and each group's last-axis range is cut into windows of kGemmCols;
 // a (group, window) is a block, one CTA per (lane, tile, block).
 constexpr int kGemmRows = 24, kGemmCols = 48, kGemmChunk = 16, kGemmThreads = 128;
+constexpr int kGemmZStride = kGemmCols + 1;   // odd row stride: table writes spread over banks
 constexpr int kGemmMaxPrefix = 128;   // table entries per prefix axis
+constexpr int kGemmMaxRun = 16;       // longest power chain between FP64 sincospi seeds
 struct GemmRun {
   int n0, n1, a, b, kstart, pad_;   // prefix (n0[, n1]), last-axis range [a, b]
 };
@@ -76,6 +78,8 @@ struct ProbDev {
   int sl2;                   // logical slices of the pass-2 segment pairs (power of 2, <= 8)
   int gemm;                  // 1: FP64 pass 1 runs as the GEMM below
   int ngblk, gm0, gc0, gm1, gc1;   // GEMM blocks; prefix tables [gm, gm + gc) per axis
+  int gs0, gs1;              // their shared-memory row strides (odd)
+  int gL, gu0, gu1, guz;     // table fill: gL entries per unit; units per particle per table
   const GemmBlock* gblk;
   const GemmRun* grun;
   double vol;                // V

@@ -190,6 +190,15 @@ SIGNATURES = {
         [ctypes.c_int, ctypes.POINTER(LBFGSSettingsC), ctypes.POINTER(ServerConfigC),
          ctypes.POINTER(_vp)],
     ),  # fmt: skip
+    "cco_pair_histogram": (
+        ctypes.c_int,
+        [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp,
+         _vp],
+    ),  # fmt: skip
+    "cco_nearest_neighbor": (
+        ctypes.c_int,
+        [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp],
+    ),  # fmt: skip
     "cco_server_destroy": (ctypes.c_int, [_vp]),
     "cco_server_submit": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_int64)]),
     "cco_server_poll": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(RequestResultC)]),
