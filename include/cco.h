@@ -323,6 +323,65 @@ int cco_md_run(cco_problem* const* problems, void* stream, int batch, const doub
                const cco_md_settings* settings, cco_md_out* out);
 
 /*
+ * MD segments with observables  <- simulate / md_chunk / init_state
+ *                                  src/xla_cco/dynamics/run.py:300-640
+ * Advances `batch` lanes of one problem (one basis) by n_steps steps from
+ * the batched state in `state` and writes the state back in place. Per step,
+ * besides the integrator of cco_md_run: densities of the tracked waves (the
+ * first n_constrained are the problem's rows `constrained_rows`, taken from
+ * the force pass; the others are summed fresh on steps divisible by
+ * wind_every), multiplied by exp(-i k . R_cm) unless the scheme is plain
+ * Verlet; the winding update (phase_floor on |rho|^2 / N); running sums;
+ * snapshots at record_steps; the rho trace every record_rho_every steps; the
+ * drift guard of plain Verlet (|E - e0| <= drift_tol * d (N - 1) T / 2; inf:
+ * none). Lanes whose status is not RUNNING are left as they are; a lane whose
+ * rho_prev row is NaN gets that row recomputed first; a lane whose e0 is NaN
+ * gets e0 = Phi + KE. n_steps = 0 only does those two. Status on return:
+ * RUNNING or DRIFT.
+ */
+typedef struct {
+  double dt, gamma, andersen_p, drift_tol, phase_floor;
+  int64_t n_steps;
+  int32_t scheme;            /* 0: velocity Verlet, 1: BAOAB */
+  int32_t andersen;          /* Verlet only: 0 off, 1 "count", 2 "bernoulli" */
+  int32_t wind_every;        /* >= 1 */
+  int32_t n_record_steps;    /* <= 256 */
+  const int64_t* record_steps;   /* host, strictly ascending, >= 1 */
+  int32_t record_rho_every, max_rho_records;
+} cco_md_segment_settings;
+
+typedef struct {
+  int32_t n_waves, n_constrained;
+  const double* n_vectors;        /* host [w][d] reciprocal-basis coefficients */
+  const double* kvec;             /* host [w][d] Cartesian wavevectors */
+  const int32_t* constrained_rows;/* host [n_constrained] problem rows of the constrained waves */
+} cco_md_waves;
+
+/* Device arrays, [batch] leading; w waves, R = n_record_steps, Q = max_rho_records. */
+typedef struct {
+  double *r, *v, *f;                      /* [B][N][d] Cartesian */
+  double *phi, *temperature, *time, *reset_acc, *e0, *max_drift;
+  double *sum_kinetic, *sum_phi, *sum_phi2;
+  uint32_t* keys;                         /* [B][2] */
+  int64_t *step, *status, *n_sum;
+  double* rho_prev;                       /* [B][w][2] */
+  double *wind_abs, *wind_net, *sum_s;    /* [B][w] */
+  int64_t* n_valid;                       /* [B][w] */
+  int64_t *snap_step, *snap_count;        /* [B][R], [B] */
+  double *snap_time, *snap_phi, *snap_kinetic;        /* [B][R] */
+  double *snap_wind_abs, *snap_wind_net;  /* [B][R][w] */
+  double* snap_rho;                       /* [B][R][w][2] */
+  double* snap_r;                         /* [B][R][N][d] */
+  double* trace_rho;                      /* [B][Q][w][2] */
+  double* trace_time;                     /* [B][Q] */
+  int64_t* trace_count;                   /* [B] */
+} cco_md_state;
+
+int cco_md_segment(cco_problem* p, void* stream, int batch, const double* basis,
+                   const cco_md_segment_settings* settings, const cco_md_waves* waves,
+                   cco_md_state* state, int64_t* ticks);
+
+/*
  * Tick schedules (graph branches, ticks per graph) are tuned online on the
  * first relaxation of each shape class (minimizer, lane count and total
  * N M bucketed by powers of two, largest d) and cached for the process;

@@ -440,3 +440,49 @@ def min_image_distances(s: np.ndarray, basis: np.ndarray):
     dist = np.sqrt(best)
     iu = np.triu_indices(n, 1)
     return dist.min(axis=1), dist[iu]
+
+
+# ------------------------------------------------------------------ MD observables
+# Restates src/xla_cco/dynamics/observables.py:56-125 and the per-step
+# bookkeeping of src/xla_cco/dynamics/run.py:247-280,415-496 in NumPy.
+
+
+def density_direct(s: np.ndarray, n: np.ndarray):
+    """(Re rho, Im rho) = sum_j (cos, sin)(2 pi n . s_j) by direct NumPy sums."""
+    theta = 2.0 * math.pi * (np.asarray(n, dtype=np.float64) @ s.T)
+    return np.cos(theta).sum(1), np.sin(theta).sum(1)
+
+
+def md_observe(r: np.ndarray, basis: np.ndarray, waves_n: np.ndarray, kvec: np.ndarray, nc: int,
+               rho_prev: np.ndarray, wind: bool, corrected: bool) -> tuple:
+    """(rho (w, 2), active (w,)) of one step: every constrained wave and, when
+    ``wind``, the others from direct sums at s = r B^-1; exp(-i k . R_cm) when
+    ``corrected``; inactive rows keep rho_prev."""
+    w = waves_n.shape[0]
+    s = r @ np.linalg.inv(basis)
+    rcm = r.mean(axis=0)
+    rows = np.arange(w) if wind else np.arange(nc)
+    re, im = density_direct(s, waves_n[rows])
+    rho = rho_prev.copy()
+    new = np.stack([re, im], axis=-1)
+    if corrected:
+        ph = kvec[rows] @ rcm
+        c, sn = np.cos(ph), np.sin(ph)
+        new = np.stack([new[:, 0] * c + new[:, 1] * sn, new[:, 1] * c - new[:, 0] * sn], axis=-1)
+    active = np.zeros(w, dtype=bool)
+    active[rows] = True
+    rho[rows] = new
+    return rho, active
+
+
+def md_winding(rho_prev, rho_new, wind_abs, wind_net, n_valid, active, n, floor):
+    """One winding update: phase change atan2 of rho_new conj(rho_old), counted
+    for active waves with |rho|^2 / n above ``floor`` at both ends."""
+    o, q = rho_prev, rho_new
+    delta = np.arctan2(q[:, 1] * o[:, 0] - q[:, 0] * o[:, 1], q[:, 0] * o[:, 0] + q[:, 1] * o[:, 1])
+    s_old = (o ** 2).sum(1) / n
+    s_new = (q ** 2).sum(1) / n
+    ok = active & (s_old > floor) & (s_new > floor)
+    keep = np.where(active[:, None], q, o)
+    return keep, wind_abs + np.where(ok, np.abs(delta), 0.0), wind_net + np.where(ok, delta, 0.0), \
+        n_valid + ok.astype(np.int64)

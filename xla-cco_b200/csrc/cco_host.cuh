@@ -83,6 +83,7 @@ enum class Method { Descent, Lbfgs, Flow, Md };
 struct RecordShape {
   Method method = Method::Lbfgs;
   int m = 0, tri_len = 0;
+  int waves = 0;   // MD segment runs: tracked waves per lane
 };
 
 inline size_t record_doubles(const RecordShape& R, const cco_problem* p) {
@@ -90,7 +91,7 @@ inline size_t record_doubles(const RecordShape& R, const cco_problem* p) {
   size_t n = 0;
   if (R.method == Method::Descent) n = ds_record_doubles(ld, p->M, p->host.ntile1);
   else if (R.method == Method::Flow) n = fl_record_doubles(ld, p->M, p->host.ntile1);
-  else if (R.method == Method::Md) n = md_record_doubles(ld, p->M, p->host.ntile1);
+  else if (R.method == Method::Md) n = md_record_doubles(ld, p->M, p->host.ntile1, R.waves);
   else n = lb_record_doubles(R.m, R.tri_len, ld, p->M, p->host.ntile1);
   return (n + 31) & ~(size_t)31;   // records start on 256-byte boundaries
 }
@@ -120,7 +121,7 @@ inline EvalLane eval_lane(const RecordShape& R, const LaneRef& L, const cco_prob
     e.f = v.pf;
     dens = v.dens;
   } else if (R.method == Method::Md) {
-    const MdView v = md_view(L.rec, L.ld);
+    const MdView v = md_view(L.rec, L.ld, R.waves);
     e.s = v.ps;
     e.g = v.pg;
     e.f = v.pf;

@@ -17,6 +17,15 @@
 // depends on launch shapes. Normals by Box-Muller on two 53-bit uniforms.
 // JAX's threefry streams are not reproduced: the reference's draws differ,
 // their distributions do not.
+//
+// Segment runs (the reference's simulate, dynamics/run.py:398-540) add the
+// per-step observables of w tracked waves: the constrained waves' densities
+// are the force evaluation's own (rho in run order, cpos maps them), the
+// others are summed fresh by k_md_waves on wind steps; both are multiplied
+// by exp(-i k . R_cm) unless the scheme is plain Verlet; then the winding
+// update, running sums, the drift guard (plain Verlet), snapshots at the
+// recorded steps and the dense rho trace (_step, _record, winding_update in
+// dynamics/run.py and dynamics/observables.py:98-125).
 #include <cmath>
 
 #include "cco_md.cuh"
@@ -120,7 +129,7 @@ __global__ void k_md_init(MdArgs a, const double* __restrict__ r0, const double*
                           const double* __restrict__ acc0) {
   const int lane = blockIdx.x;
   const LaneRef R = a.lanes[lane];
-  const MdView w = md_view(R.rec, R.ld);
+  const MdView w = md_view(R.rec, R.ld, a.w);
   for (int e = threadIdx.x; e < 5 * R.ld; e += blockDim.x) w.r[e] = 0.0;
   __shared__ MdState S;
   if (threadIdx.x == 0) {
@@ -134,6 +143,10 @@ __global__ void k_md_init(MdArgs a, const double* __restrict__ r0, const double*
     x.key[0] = keys[2 * R.idx];
     x.key[1] = keys[2 * R.idx + 1];
     x.acc = acc0 ? acc0[R.idx] : 0.0;
+    x.step_end = a.n_steps;
+    x.temperature = a.temperature;
+    x.drift_limit = a.drift_tol > 0.0 ? a.drift_tol : -1.0;
+    x.e0 = NAN;
     x.t0 = gtimer();
     S = x;
   }
@@ -147,12 +160,140 @@ __global__ void k_md_init(MdArgs a, const double* __restrict__ r0, const double*
   if (threadIdx.x == 0) *w.st = S;
 }
 
-__global__ void __launch_bounds__(kUpdThreads) k_md_update(MdArgs a, double c, double noise) {
+// NaN-propagating maximum (jnp.maximum).
+__device__ __forceinline__ double max_nan(double a, double b) {
+  return (a != a || b != b) ? NAN : fmax(a, b);
+}
+
+// Mean Cartesian position (unwrapped r, mass 1) into rcm[0..d).
+__device__ void center_of_mass(const LaneRef& R, const MdView& w, int d, double* rcm,
+                               double* red) {
+  for (int c = 0; c < d; ++c) {
+    double s = 0.0;
+    for (int j = threadIdx.x; j < R.n; j += blockDim.x) s += w.r[(size_t)j * d + c];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) rcm[c] = s / R.n;
+    __syncthreads();
+  }
+}
+
+// Density of wave c as the observables see it: the force pass's rho for a
+// constrained wave, the fresh sum otherwise; times exp(-i k . R_cm) when
+// the scheme corrects the centre of mass.
+__device__ __forceinline__ double2 wave_rho(const MdArgs& a, const MdView& w, int c, int d,
+                                            const double* rcm) {
+  double2 r;
+  if (c < a.nc) r = w.dens[a.cpos[c]];
+  else r = make_double2(w.fresh[2 * c], w.fresh[2 * c + 1]);
+  if (a.corrected) {
+    double ph = 0.0;
+    for (int q = 0; q < d; ++q) ph += a.wave_k[(size_t)c * d + q] * rcm[q];
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    r = make_double2(r.x * cs + r.y * sn, r.y * cs - r.x * sn);
+  }
+  return r;
+}
+
+// Index of `step` among the ascending recorded steps, or -1.
+__device__ __forceinline__ int record_slot(const MdArgs& a, int64_t step) {
+  int lo = 0, hi = a.n_rec - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int64_t v = a.rec_steps[mid];
+    if (v == step) return mid;
+    if (v < step) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+// Observables after a finished step of a segment run (S holds the new step,
+// time, phi, ke; running sums and counters are advanced here).
+__device__ void observe_step(const MdArgs& a, const LaneRef& R, const MdView& w, MdState& S,
+                             int d, double* red) {
+  __shared__ double rcm[3];
+  __shared__ int snap_slot, trace_row;
+  if (a.corrected) center_of_mass(R, w, d, rcm, red);
+  const bool wind = S.step % a.wind_every == 0;
+  if (threadIdx.x == 0) {
+    snap_slot = a.n_rec > 0 ? record_slot(a, S.step) : -1;
+    trace_row = (a.trace_every > 0 && a.trace_cap > 0 && S.step % a.trace_every == 0 &&
+                 S.trace_count < a.trace_cap) ? (int)S.trace_count : -1;
+  }
+  __syncthreads();
+  const int js = snap_slot, jt = trace_row;
+  const size_t lane = (size_t)R.idx;
+  for (int c = threadIdx.x; c < a.w; c += blockDim.x) {
+    const double2 old = make_double2(w.rho_prev[2 * c], w.rho_prev[2 * c + 1]);
+    const bool active = c < a.nc || wind;
+    double2 nw = old;
+    if (active) nw = wave_rho(a, w, c, d, rcm);
+    const double delta = atan2(nw.y * old.x - nw.x * old.y, nw.x * old.x + nw.y * old.y);
+    const double s_old = (old.x * old.x + old.y * old.y) / R.n;
+    const double s_new = (nw.x * nw.x + nw.y * nw.y) / R.n;
+    const bool ok = active && s_old > a.phase_floor && s_new > a.phase_floor;
+    const double2 rp = active ? nw : old;
+    w.rho_prev[2 * c] = rp.x;
+    w.rho_prev[2 * c + 1] = rp.y;
+    if (ok) {
+      w.wind_abs[c] += fabs(delta);
+      w.wind_net[c] += delta;
+      w.n_valid[c] += 1.0;
+    }
+    w.sum_s[c] += (rp.x * rp.x + rp.y * rp.y) / R.n;
+    if (js >= 0) {
+      const size_t o = (lane * a.n_rec + js) * a.w + c;
+      a.io.snap_wind_abs[o] = w.wind_abs[c];
+      a.io.snap_wind_net[o] = w.wind_net[c];
+      a.io.snap_rho[2 * o] = rp.x;
+      a.io.snap_rho[2 * o + 1] = rp.y;
+    }
+    if (jt >= 0) {
+      const size_t o = (lane * a.trace_cap + jt) * a.w + c;
+      a.io.trace_rho[2 * o] = rp.x;
+      a.io.trace_rho[2 * o + 1] = rp.y;
+    }
+  }
+  if (js >= 0)
+    for (int e = threadIdx.x; e < R.nd; e += blockDim.x)
+      a.io.snap_r[(lane * a.n_rec + js) * R.nd + e] = w.r[e];
+  if (threadIdx.x == 0) {
+    if (js >= 0) {
+      const size_t o = lane * a.n_rec + js;
+      a.io.snap_step[o] = S.step;
+      a.io.snap_time[o] = S.time;
+      a.io.snap_phi[o] = S.phi;
+      a.io.snap_kinetic[o] = S.ke;
+      S.snap_count += 1;
+    }
+    if (jt >= 0) {
+      a.io.trace_time[lane * a.trace_cap + jt] = S.time;
+      S.trace_count += 1;
+    }
+  }
+}
+
+// Rows of rho_prev marked pending (NaN) get the current densities (the first
+// tick of a segment run evaluated the force at the current positions).
+__device__ void repair_pending(const MdArgs& a, const LaneRef& R, const MdView& w, int d,
+                               double* red) {
+  __shared__ double rcm[3];
+  if (a.corrected) center_of_mass(R, w, d, rcm, red);
+  for (int c = threadIdx.x; c < a.w; c += blockDim.x)
+    if (w.rho_prev[2 * c] != w.rho_prev[2 * c]) {
+      const double2 r = wave_rho(a, w, c, d, rcm);
+      w.rho_prev[2 * c] = r.x;
+      w.rho_prev[2 * c + 1] = r.y;
+    }
+}
+
+__global__ void __launch_bounds__(kUpdThreads) k_md_update(MdArgs a, double c, double noise_var) {
   __shared__ MdState S;
   __shared__ double red[32];
   const int lane = blockIdx.x;
   const LaneRef R = a.lanes[lane];
-  const MdView w = md_view(R.rec, R.ld);
+  const MdView w = md_view(R.rec, R.ld, a.w);
   if (threadIdx.x == 0) S = *w.st;
   __syncthreads();
   if (S.status != CCO_STATUS_RUNNING) return;
@@ -160,15 +301,17 @@ __global__ void __launch_bounds__(kUpdThreads) k_md_update(MdArgs a, double c, d
   forces(R, w, S, d);
   __syncthreads();
   if (S.phase == 0) {
-    // forces at the start: energy reference for the drift
+    // forces at the start: energy reference for the drift (kept when the
+    // segment already has one), pending densities of a segment run
     const double ke = kinetic(R, w, red);
+    if (a.w > 0) repair_pending(a, R, w, d, red);
     if (threadIdx.x == 0) {
       S.phi = *w.pf;
       S.ke = ke;
-      S.e0 = S.phi + ke;
-      S.max_drift = 0.0;
+      if (a.w == 0 || S.e0 != S.e0) S.e0 = S.phi + ke;
+      if (a.w == 0) S.max_drift = 0.0;
       S.phase = 1;
-      if (a.n_steps <= 0) {
+      if (S.step >= S.step_end) {
         S.status = CCO_STATUS_BUDGET;
         S.t1 = gtimer();
       }
@@ -180,6 +323,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_md_update(MdArgs a, double c, d
     __shared__ int fire, pick;
     if (threadIdx.x == 0) {
       S.step += 1;
+      S.time += a.dt;
       fire = 0;
       pick = 0;
       if (a.scheme == MD_VERLET && a.andersen != ANDERSEN_OFF) {
@@ -199,7 +343,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_md_update(MdArgs a, double c, d
     __syncthreads();
     if (fire && threadIdx.x < d)
       w.v[(size_t)pick * d + threadIdx.x] =
-          sqrt(a.temperature) * normal(draw(S, RNG_ROW, threadIdx.x));
+          sqrt(S.temperature) * normal(draw(S, RNG_ROW, threadIdx.x));
     __syncthreads();
     const double ke = kinetic(R, w, red);
     if (threadIdx.x == 0) {
@@ -212,16 +356,162 @@ __global__ void __launch_bounds__(kUpdThreads) k_md_update(MdArgs a, double c, d
       S.phi = *w.pf;
       S.ke = ke;
       const double drift = fabs(S.phi + ke - S.e0);
-      S.max_drift = fmax(S.max_drift, drift);
-      if (a.drift_tol > 0.0 && !(drift <= a.drift_tol)) S.status = CCO_STATUS_DRIFT;
-      else if (S.step >= a.n_steps) S.status = CCO_STATUS_BUDGET;
+      S.max_drift = max_nan(S.max_drift, drift);
+      if (S.drift_limit >= 0.0 && !(drift <= S.drift_limit)) S.status = CCO_STATUS_DRIFT;
+      if (a.w > 0) {
+        S.sum_kinetic += ke;
+        S.sum_phi += S.phi;
+        S.sum_phi2 += S.phi * S.phi;
+        S.n_sum += 1;
+      }
+    }
+    __syncthreads();
+    if (a.w > 0) observe_step(a, R, w, S, d, red);
+    if (threadIdx.x == 0) {
+      if (S.status == CCO_STATUS_RUNNING && S.step >= S.step_end) S.status = CCO_STATUS_BUDGET;
       if (S.status != CCO_STATUS_RUNNING) S.t1 = gtimer();
     }
   }
   __syncthreads();
-  if (S.status == CCO_STATUS_RUNNING) begin_step(a, R, w, S, d, c, noise);
+  if (S.status == CCO_STATUS_RUNNING) {
+    const double noise = sqrt(noise_var * S.temperature);
+    begin_step(a, R, w, S, d, c, noise);
+  }
   __syncthreads();
   if (threadIdx.x == 0) *w.st = S;
+}
+
+// Fresh densities of the unconstrained waves at the probe positions (the
+// positions the tick's force pass evaluated) on wind steps and on the first
+// tick. Grid: (lanes, wave chunks of blockDim.x); particles staged in tiles.
+__global__ void __launch_bounds__(kUpdThreads) k_md_waves(MdArgs a) {
+  __shared__ double tile[kUpdThreads * 3];
+  const LaneRef R = a.lanes[blockIdx.x];
+  const MdView w = md_view(R.rec, R.ld, a.w);
+  const MdState* S = w.st;
+  if (S->status != CCO_STATUS_RUNNING) return;
+  if (S->phase != 0 && (S->step + 1) % a.wind_every != 0) return;
+  const int d = R.nd / R.n;
+  const int u = a.nc + blockIdx.y * blockDim.x + threadIdx.x;
+  double nv[3] = {0.0, 0.0, 0.0};
+  if (u < a.w)
+    for (int q = 0; q < d; ++q) nv[q] = a.wave_n[(size_t)u * d + q];
+  double re = 0.0, im = 0.0;
+  for (int j0 = 0; j0 < R.n; j0 += blockDim.x) {
+    const int nj = min((int)blockDim.x, R.n - j0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < nj * d; e += blockDim.x) tile[e] = w.ps[(size_t)j0 * d + e];
+    __syncthreads();
+    if (u < a.w)
+      for (int jj = 0; jj < nj; ++jj) {
+        double dot = 0.0;
+        for (int q = 0; q < d; ++q) dot += nv[q] * tile[jj * d + q];
+        double sn, cs;
+        sincospi(2.0 * dot, &sn, &cs);
+        re += cs;
+        im += sn;
+      }
+  }
+  if (u < a.w) {
+    w.fresh[2 * u] = re;
+    w.fresh[2 * u + 1] = im;
+  }
+}
+
+// Segment runs: each lane's record from the batched state.
+__global__ void k_md_seg_init(MdArgs a, const double* __restrict__ mats) {
+  const LaneRef R = a.lanes[blockIdx.x];
+  const MdView w = md_view(R.rec, R.ld, a.w);
+  const MdSegIO& io = a.io;
+  const size_t i = (size_t)R.idx;
+  __shared__ MdState S;
+  if (threadIdx.x == 0) {
+    MdState x = {};
+    x.status = io.status[i];
+    for (int q = 0; q < 9; ++q) {
+      x.B[q] = mats[q];
+      x.Binv[q] = mats[9 + q];
+      x.BinvT[q] = mats[18 + q];
+    }
+    x.key[0] = io.keys[2 * i];
+    x.key[1] = io.keys[2 * i + 1];
+    x.acc = io.reset_acc[i];
+    x.step = io.step[i];
+    x.step_end = x.step + a.n_steps;
+    x.time = io.time[i];
+    x.temperature = io.temperature[i];
+    x.phi = io.phi[i];
+    x.e0 = io.e0[i];
+    x.max_drift = io.max_drift[i];
+    x.sum_kinetic = io.sum_kinetic[i];
+    x.sum_phi = io.sum_phi[i];
+    x.sum_phi2 = io.sum_phi2[i];
+    x.n_sum = io.n_sum[i];
+    x.snap_count = io.snap_count[i];
+    x.trace_count = io.trace_count[i];
+    x.drift_limit = a.drift_coef >= 0.0 ? a.drift_coef * x.temperature : -1.0;
+    x.t0 = gtimer();
+    S = x;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < R.nd; e += blockDim.x) {
+    w.r[e] = io.r[R.soff + e];
+    w.v[e] = io.v[R.soff + e];
+    w.f[e] = io.f[R.soff + e];
+  }
+  for (int c = threadIdx.x; c < a.w; c += blockDim.x) {
+    const size_t o = i * a.w + c;
+    w.rho_prev[2 * c] = io.rho_prev[2 * o];
+    w.rho_prev[2 * c + 1] = io.rho_prev[2 * o + 1];
+    w.wind_abs[c] = io.wind_abs[o];
+    w.wind_net[c] = io.wind_net[o];
+    w.n_valid[c] = (double)io.n_valid[o];
+    w.sum_s[c] = io.sum_s[o];
+  }
+  __syncthreads();
+  to_fractional(R, w, S, R.nd / R.n);
+  if (threadIdx.x == 0) *w.st = S;
+}
+
+// Segment runs: the batched state from each lane's record. A lane that
+// finished its steps is STATUS_RUNNING again (only a drift stops a lane).
+__global__ void k_md_seg_finalize(MdArgs a) {
+  const LaneRef R = a.lanes[blockIdx.x];
+  const MdView w = md_view(R.rec, R.ld, a.w);
+  const MdSegIO& io = a.io;
+  const size_t i = (size_t)R.idx;
+  const MdState S = *w.st;
+  for (int e = threadIdx.x; e < R.nd; e += blockDim.x) {
+    io.r[R.soff + e] = w.r[e];
+    io.v[R.soff + e] = w.v[e];
+    io.f[R.soff + e] = w.f[e];
+  }
+  for (int c = threadIdx.x; c < a.w; c += blockDim.x) {
+    const size_t o = i * a.w + c;
+    io.rho_prev[2 * o] = w.rho_prev[2 * c];
+    io.rho_prev[2 * o + 1] = w.rho_prev[2 * c + 1];
+    io.wind_abs[o] = w.wind_abs[c];
+    io.wind_net[o] = w.wind_net[c];
+    io.n_valid[o] = (int64_t)w.n_valid[c];
+    io.sum_s[o] = w.sum_s[c];
+  }
+  if (threadIdx.x == 0) {
+    io.status[i] = S.status == CCO_STATUS_BUDGET ? CCO_STATUS_RUNNING : S.status;
+    io.keys[2 * i] = S.key[0];
+    io.keys[2 * i + 1] = S.key[1];
+    io.reset_acc[i] = S.acc;
+    io.step[i] = S.step;
+    io.time[i] = S.time;
+    io.phi[i] = S.phi;
+    io.e0[i] = S.e0;
+    io.max_drift[i] = S.max_drift;
+    io.sum_kinetic[i] = S.sum_kinetic;
+    io.sum_phi[i] = S.sum_phi;
+    io.sum_phi2[i] = S.sum_phi2;
+    io.n_sum[i] = S.n_sum;
+    io.snap_count[i] = S.snap_count;
+    io.trace_count[i] = S.trace_count;
+  }
 }
 
 __global__ void k_md_finalize(MdArgs a, double* r_out, double* v_out, double* f_out,
@@ -230,7 +520,7 @@ __global__ void k_md_finalize(MdArgs a, double* r_out, double* v_out, double* f_
                               int64_t* status_out) {
   const int lane = blockIdx.x;
   const LaneRef R = a.lanes[lane];
-  const MdView w = md_view(R.rec, R.ld);
+  const MdView w = md_view(R.rec, R.ld, a.w);
   for (int e = threadIdx.x; e < R.nd; e += blockDim.x) {
     r_out[R.soff + e] = w.r[e];
     v_out[R.soff + e] = w.v[e];
@@ -258,10 +548,25 @@ cudaError_t md_init(const MdArgs& a, const double* r0, const double* v0, const d
 }
 
 cudaError_t md_update(const MdArgs& a, cudaStream_t st) {
-  // c = exp(-gamma dt), 1 - c^2 = -expm1(-2 gamma dt) without cancellation
+  // c = exp(-gamma dt), 1 - c^2 = -expm1(-2 gamma dt) without cancellation;
+  // the noise amplitude is sqrt((1 - c^2) T) with each lane's T
   const double c = std::exp(-a.gamma * a.dt);
-  const double noise = std::sqrt(-std::expm1(-2.0 * a.gamma * a.dt) * a.temperature);
-  k_md_update<<<a.B, kUpdThreads, 0, st>>>(a, c, noise);
+  const double noise_var = -std::expm1(-2.0 * a.gamma * a.dt);
+  if (a.w > a.nc) {
+    const dim3 grid(a.B, (a.w - a.nc + kUpdThreads - 1) / kUpdThreads);
+    k_md_waves<<<grid, kUpdThreads, 0, st>>>(a);
+  }
+  k_md_update<<<a.B, kUpdThreads, 0, st>>>(a, c, noise_var);
+  return cudaGetLastError();
+}
+
+cudaError_t md_seg_init(const MdArgs& a, const double* mats, cudaStream_t st) {
+  k_md_seg_init<<<a.B, kUpdThreads, 0, st>>>(a, mats);
+  return cudaGetLastError();
+}
+
+cudaError_t md_seg_finalize(const MdArgs& a, cudaStream_t st) {
+  k_md_seg_finalize<<<a.B, kUpdThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -172,8 +172,9 @@ cudaError_t TickPlan::tick(cudaStream_t s, int b) const {
 }
 
 int TickPlan::launches_per_tick() const {
-  // 4 evaluation kernels + the update kernels
-  return nbr * (method == Method::Lbfgs ? 8 : 5);
+  // 4 evaluation kernels + the update kernels (MD segments: + the wave sums)
+  const int md_waves = method == Method::Md && md[0].w > md[0].nc ? 1 : 0;
+  return nbr * (method == Method::Lbfgs ? 8 : 5 + md_waves);
 }
 
 void TickPlan::release(cudaStream_t st) {
@@ -894,6 +895,138 @@ extern "C" int cco_md_run(cco_problem* const* problems, void* stream, int batch,
   cudaFreeAsync(records, st);
   cudaError_t e = cudaStreamSynchronize(st);
   if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "md run");
+  return rc;
+}
+
+extern "C" int cco_md_segment(cco_problem* p, void* stream, int batch, const double* basis,
+                              const cco_md_segment_settings* cfg, const cco_md_waves* wv,
+                              cco_md_state* io, int64_t* ticks) {
+  if (!p || !basis || !cfg || !wv || !io) return fail(CCO_ERR_ARG, "null argument");
+  if (batch < 1) return fail(CCO_ERR_ARG, "need at least one lane");
+  if (!(std::isfinite(cfg->dt) && cfg->dt > 0.0))
+    return fail(CCO_ERR_ARG, "dt must be finite and positive, got %g", cfg->dt);
+  if (cfg->n_steps < 0) return fail(CCO_ERR_ARG, "n_steps must be >= 0");
+  if (cfg->scheme != MD_VERLET && cfg->scheme != MD_BAOAB) return fail(CCO_ERR_ARG, "unknown scheme");
+  if (cfg->andersen < 0 || cfg->andersen > 2) return fail(CCO_ERR_ARG, "unknown Andersen mode");
+  if (!(cfg->andersen_p >= 0.0 && cfg->andersen_p <= 1.0))
+    return fail(CCO_ERR_ARG, "andersen_p must lie in [0, 1], got %g", cfg->andersen_p);
+  if (!(cfg->gamma >= 0.0 && std::isfinite(cfg->gamma)))
+    return fail(CCO_ERR_ARG, "gamma must be finite and >= 0, got %g", cfg->gamma);
+  if (cfg->wind_every < 1) return fail(CCO_ERR_ARG, "wind_every must be >= 1");
+  if (!(cfg->phase_floor >= 0.0) || !(cfg->drift_tol > 0.0))
+    return fail(CCO_ERR_ARG, "need phase_floor >= 0 and drift_tol > 0");
+  if (cfg->n_record_steps < 0 || cfg->n_record_steps > 256 ||
+      (cfg->n_record_steps > 0 && !cfg->record_steps))
+    return fail(CCO_ERR_ARG, "record_steps: at most 256");
+  for (int j = 0; j < cfg->n_record_steps; ++j)
+    if (cfg->record_steps[j] < 1 || (j > 0 && cfg->record_steps[j] <= cfg->record_steps[j - 1]))
+      return fail(CCO_ERR_ARG, "record_steps must be strictly increasing integers >= 1");
+  if (cfg->record_rho_every < 0 || cfg->max_rho_records < 0 ||
+      (cfg->record_rho_every > 0 && cfg->max_rho_records < 1))
+    return fail(CCO_ERR_ARG, "a rho trace needs record_rho_every > 0 and max_rho_records >= 1");
+  const int d = p->d, w = wv->n_waves, nc = wv->n_constrained;
+  if (w < 1 || nc < 1 || nc > w || !wv->n_vectors || !wv->kvec || !wv->constrained_rows)
+    return fail(CCO_ERR_ARG, "need 1 <= n_constrained <= n_waves and the wave arrays");
+  const bool rec = cfg->n_record_steps > 0, trace = cfg->record_rho_every > 0;
+  if (!io->r || !io->v || !io->f || !io->phi || !io->temperature || !io->time || !io->reset_acc ||
+      !io->e0 || !io->max_drift || !io->sum_kinetic || !io->sum_phi || !io->sum_phi2 ||
+      !io->keys || !io->step || !io->status || !io->n_sum || !io->rho_prev || !io->wind_abs ||
+      !io->wind_net || !io->sum_s || !io->n_valid || !io->snap_count || !io->trace_count)
+    return fail(CCO_ERR_ARG, "incomplete state struct");
+  if (rec && (!io->snap_step || !io->snap_time || !io->snap_phi || !io->snap_kinetic ||
+              !io->snap_wind_abs || !io->snap_wind_net || !io->snap_rho || !io->snap_r))
+    return fail(CCO_ERR_ARG, "snapshot buffers missing");
+  if (trace && (!io->trace_rho || !io->trace_time)) return fail(CCO_ERR_ARG, "trace buffers missing");
+  double m27[27];
+  if (!basis_mats(basis, d, m27)) return fail(CCO_ERR_ARG, "singular basis");
+  std::vector<double> mats(27);
+  for (int q = 0; q < 9; ++q) mats[q] = m27[q];
+  for (int x = 0; x < 3; ++x)
+    for (int y = 0; y < 3; ++y) {
+      mats[9 + x * 3 + y] = m27[9 + y * 3 + x];
+      mats[18 + x * 3 + y] = m27[9 + x * 3 + y];
+    }
+  DeviceGuard guard(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  // run position of each constrained wave's density
+  std::vector<int> r2r(p->M), pos(p->M), cpos(nc);
+  CCO_CUDA(cudaMemcpy(r2r.data(), p->run2ref, sizeof(int) * p->M, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < p->M; ++k) pos[r2r[k]] = k;
+  for (int c = 0; c < nc; ++c) {
+    const int row = wv->constrained_rows[c];
+    if (row < 0 || row >= p->M) return fail(CCO_ERR_ARG, "constrained wave %d: row %d outside the problem", c, row);
+    cpos[c] = pos[row];
+  }
+  RecordShape shape;
+  shape.method = Method::Md;
+  shape.waves = w;
+  LaneTable T;
+  MdArgs& a = T.md;
+  a.dt = cfg->dt;
+  a.gamma = cfg->gamma;
+  a.temperature = 0.0;
+  a.andersen_p = cfg->andersen_p;
+  a.drift_tol = 0.0;
+  a.n_steps = cfg->n_steps;
+  a.scheme = cfg->scheme;
+  a.andersen = cfg->scheme == MD_VERLET ? cfg->andersen : ANDERSEN_OFF;
+  a.w = w;
+  a.nc = nc;
+  a.wind_every = cfg->wind_every;
+  a.corrected = (a.scheme == MD_BAOAB || a.andersen != ANDERSEN_OFF) ? 1 : 0;
+  const bool guard_on = a.scheme == MD_VERLET && a.andersen == ANDERSEN_OFF && std::isfinite(cfg->drift_tol);
+  a.drift_coef = guard_on ? cfg->drift_tol * 0.5 * d * (p->N - 1) : -1.0;
+  a.phase_floor = cfg->phase_floor;
+  a.n_rec = cfg->n_record_steps;
+  a.trace_every = trace ? cfg->record_rho_every : 0;
+  a.trace_cap = trace ? cfg->max_rho_records : 0;
+  MdSegIO& o = a.io;
+  o.r = io->r; o.v = io->v; o.f = io->f; o.phi = io->phi; o.temperature = io->temperature;
+  o.time = io->time; o.reset_acc = io->reset_acc; o.keys = io->keys; o.step = io->step;
+  o.status = io->status; o.n_valid = io->n_valid; o.n_sum = io->n_sum; o.rho_prev = io->rho_prev;
+  o.wind_abs = io->wind_abs; o.wind_net = io->wind_net; o.sum_s = io->sum_s; o.e0 = io->e0;
+  o.max_drift = io->max_drift; o.sum_kinetic = io->sum_kinetic; o.sum_phi = io->sum_phi;
+  o.sum_phi2 = io->sum_phi2; o.snap_step = io->snap_step; o.snap_count = io->snap_count;
+  o.snap_time = io->snap_time; o.snap_wind_abs = io->snap_wind_abs;
+  o.snap_wind_net = io->snap_wind_net; o.snap_rho = io->snap_rho; o.snap_r = io->snap_r;
+  o.snap_phi = io->snap_phi; o.snap_kinetic = io->snap_kinetic; o.trace_rho = io->trace_rho;
+  o.trace_time = io->trace_time; o.trace_count = io->trace_count;
+  std::vector<cco_problem*> probs(batch, p);
+  double* records = nullptr;
+  int rc = make_table(probs.data(), batch, shape, 0, st, &T, &records);
+  if (rc != CCO_OK) {
+    if (records) cudaFreeAsync(records, st);
+    return rc;
+  }
+  a.B = batch;
+  a.lanes = T.d_refs;
+  double *d_mats = nullptr, *d_wn = nullptr, *d_wk = nullptr;
+  int* d_cpos = nullptr;
+  int64_t* d_rec = nullptr;
+  cudaError_t e = upload(&d_mats, mats, st);
+  if (e == cudaSuccess) e = upload(&d_wn, std::vector<double>(wv->n_vectors, wv->n_vectors + (size_t)w * d), st);
+  if (e == cudaSuccess) e = upload(&d_wk, std::vector<double>(wv->kvec, wv->kvec + (size_t)w * d), st);
+  if (e == cudaSuccess) e = upload(&d_cpos, cpos, st);
+  if (e == cudaSuccess && rec)
+    e = upload(&d_rec, std::vector<int64_t>(cfg->record_steps, cfg->record_steps + cfg->n_record_steps), st);
+  a.wave_n = d_wn;
+  a.wave_k = d_wk;
+  a.cpos = d_cpos;
+  a.rec_steps = d_rec;
+  if (e == cudaSuccess) e = md_seg_init(a, d_mats, st);
+  if (e != cudaSuccess) rc = cuda_fail(e, "md segment setup");
+  RunStats rs;
+  if (rc == CCO_OK) rc = run_lane_table(T, st, 2 + cfg->n_steps + 4 * (kInflight + 1) * 32, &rs);
+  if (rc == CCO_OK) {
+    e = md_seg_finalize(a, st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "md segment finalize");
+  }
+  if (ticks) *ticks = rs.ticks;
+  T.release(st);
+  for (void* q : {(void*)d_mats, (void*)d_wn, (void*)d_wk, (void*)d_cpos, (void*)d_rec, (void*)records})
+    if (q) cudaFreeAsync(q, st);
+  e = cudaStreamSynchronize(st);
+  if (rc == CCO_OK && e != cudaSuccess) rc = cuda_fail(e, "md segment");
   return rc;
 }
 

@@ -149,6 +149,36 @@ class MdOutC(ctypes.Structure):
 
 
 # (name, restype, argtypes) for every symbol include/cco.h declares
+class MdSegmentSettingsC(ctypes.Structure):
+    _fields_ = [
+        ("dt", ctypes.c_double), ("gamma", ctypes.c_double), ("andersen_p", ctypes.c_double),
+        ("drift_tol", ctypes.c_double), ("phase_floor", ctypes.c_double),
+        ("n_steps", ctypes.c_int64), ("scheme", ctypes.c_int32), ("andersen", ctypes.c_int32),
+        ("wind_every", ctypes.c_int32), ("n_record_steps", ctypes.c_int32),
+        ("record_steps", ctypes.c_void_p), ("record_rho_every", ctypes.c_int32),
+        ("max_rho_records", ctypes.c_int32),
+    ]  # fmt: skip
+
+
+class MdWavesC(ctypes.Structure):
+    _fields_ = [("n_waves", ctypes.c_int32), ("n_constrained", ctypes.c_int32),
+                ("n_vectors", ctypes.c_void_p), ("kvec", ctypes.c_void_p),
+                ("constrained_rows", ctypes.c_void_p)]  # fmt: skip
+
+
+MD_STATE_FIELDS = (
+    "r", "v", "f", "phi", "temperature", "time", "reset_acc", "e0", "max_drift", "sum_kinetic",
+    "sum_phi", "sum_phi2", "keys", "step", "status", "n_sum", "rho_prev", "wind_abs", "wind_net",
+    "sum_s", "n_valid", "snap_step", "snap_count", "snap_time", "snap_phi", "snap_kinetic",
+    "snap_wind_abs", "snap_wind_net", "snap_rho", "snap_r", "trace_rho", "trace_time",
+    "trace_count",
+)
+
+
+class MdStateC(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in MD_STATE_FIELDS]
+
+
 SIGNATURES = {
     "cco_abi_version": (ctypes.c_int, []),
     "cco_error_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -198,6 +228,11 @@ SIGNATURES = {
     "cco_nearest_neighbor": (
         ctypes.c_int,
         [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp],
+    ),  # fmt: skip
+    "cco_md_segment": (
+        ctypes.c_int,
+        [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(MdSegmentSettingsC), ctypes.POINTER(MdWavesC),
+         ctypes.POINTER(MdStateC), ctypes.POINTER(ctypes.c_int64)],
     ),  # fmt: skip
     "cco_server_destroy": (ctypes.c_int, [_vp]),
     "cco_server_submit": (ctypes.c_int, [_vp, _vp, _vp, ctypes.POINTER(ctypes.c_int64)]),
