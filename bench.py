@@ -595,6 +595,168 @@ def run_serve(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ MD segments
+def _md_host_sample(ks, basis, waves, r0, v0, n_steps: int) -> float:
+    """Seconds per lane-step of the oracle chain (direct-sum forces and wave
+    densities, NumPy on the host threads) over a short sample of one lane."""
+    import oracle
+
+    from xla_cco.dynamics import baoab_step, make_key
+
+    inv = np.linalg.inv(basis)
+    nv = ks.n.astype(np.float64)
+    vol = float(abs(np.linalg.det(basis)))
+
+    def force(r):
+        s = r @ inv
+        phi, g = oracle.energy_direct(s, nv, np.ones(nv.shape[0]), vol)
+        re, im = oracle.density_direct(s, nv)
+        return phi, -(g @ inv.T), re, im
+
+    r, v, f, key = r0, v0, force(r0)[1], make_key(1)
+    rho = np.zeros((waves.n_vectors.shape[0], 2))
+    t0 = time.perf_counter()
+    for _ in range(n_steps):
+        key, r, v, out = baoab_step(key, r, v, f, force, 0.02, 1.0, 1e-3)
+        f = out[1]
+        rho, _ = oracle.md_observe(r, basis, waves.n_vectors, waves.kvec, waves.n_constrained, rho,
+                                   True, True)  # fmt: skip
+    return (time.perf_counter() - t0) / n_steps
+
+
+def run_md(args) -> None:
+    """MD segments (simulate) on the d=2 N=1000 chi=0.40 system: BAOAB lanes,
+    tracked waves |k| < 1.5 K (constrained |k| < K), wind every 10 steps,
+    200 snapshots and a rho trace every 20 steps (production recording)."""
+    import torch
+
+    from xla_cco.dynamics import MDSettings, init_state, make_key, make_waves, simulate
+
+    torch.cuda.set_device(0)
+    box, ks, energy = workload()
+    basis = np.asarray(box.basis)
+    from xla_cco import k_outer_from_ka, ka_from_chi
+
+    k2 = k_outer_from_ka(ka_from_chi(CHI, PHI_PACK, DIM), PHI_PACK, DIM)
+    waves = make_waves(basis, k2, 1.5 * k2)
+    assert waves.n_constrained == ks.n.shape[0], "constrained waves are the energy's k-set"
+    lanes, n_steps = args.md_lanes, args.md_steps
+    st = MDSettings(dt=0.02, scheme="baoab", gamma=1.0, chunk_steps=n_steps, wind_every=10,
+                    record_steps=tuple(range(n_steps // 200, n_steps + 1, max(n_steps // 200, 1)))[:200],
+                    record_rho_every=20, max_rho_records=n_steps // 20, drift_tol=float("inf"))  # fmt: skip
+    rng = np.random.default_rng(SEED)
+    r0 = rng.uniform(size=(lanes, N_PART, DIM)) @ basis
+    v0 = rng.normal(scale=0.03, size=(lanes, N_PART, DIM))
+    keys = np.stack([make_key(i) for i in range(lanes)])
+    lane0 = init_state(energy, waves, basis, r0, v0, np.full(lanes, 1e-3), keys, st)
+    for _ in range(args.warmup):
+        simulate(energy, waves, basis, st, lane0, max(n_steps // 10, 1))
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        res = simulate(energy, waves, basis, st, lane0, n_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    value = lanes * n_steps / (ms / 1e3)
+    w = int(waves.n_vectors.shape[0])
+    cpu_s = None if args.no_cpu_baseline else _md_host_sample(ks, basis, waves, r0[0], v0[0], 20)
+    # device-side algorithmic flops per lane-step: force (F_PAIR N M) + fresh waves every 10 steps
+    flops = lanes * n_steps * (F_PAIR[DIM] * N_PART * ks.n.shape[0] +
+                               0.1 * 40.0 * N_PART * (w - waves.n_constrained))  # fmt: skip
+    peak = fp64_peak_tflops()
+    line = {
+        "metric": "MD lane-steps/s (simulate: BAOAB + tracked-wave observables)", "value": value,
+        "unit": "lane-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"md_segment_d{DIM}_n{N_PART}_chi{CHI}_lanes{lanes}_steps{n_steps}",
+                   "waves": w, "constrained": int(waves.n_constrained), "wind_every": 10,
+                   "snapshots": len(st.record_steps), "trace_rows": st.max_rho_records,
+                   "final_status_running": int((res.state.status == 0).sum()),
+                   "wall_s_per_step": wall / args.steps},
+        "roofline": {"kernel": "whole MD segment (evaluations + step + observables)", "bound": "fp64",
+                     "achieved": flops / (ms / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                     "frac": flops / (ms / 1e3) / 1e12 / peak if peak else None,
+                     "algorithmic": "F_PAIR N M per force + 40 flops per (fresh wave, particle) every 10 steps"},
+        "cpu_baseline": None if cpu_s is None else {
+            "value": 1.0 / cpu_s, "unit": "lane-steps/s", "cores": 1, "kind": "port",
+            "sample": "oracle chain: 20 BAOAB steps of one lane, direct-sum forces and all waves' densities"},
+        "clocks": clocks,
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ analysis
+def run_analysis(args) -> None:
+    """S(k) (isotropic, the ground-state driver's 5 / 400 k-set) and the pair
+    histogram + nearest neighbours of 256 configurations, d=2 N=1000."""
+    import oracle
+    import torch
+
+    from xla_cco.analysis import isotropic_structure_factor, nearest_neighbor_distances, pair_distance_histogram
+    from xla_cco.analysis.structure import _isotropic_kset
+
+    torch.cuda.set_device(0)
+    box, ks, energy = workload()
+    basis = np.asarray(box.basis)
+    b = args.batch
+    s = np.random.default_rng(SEED).uniform(size=(b, N_PART, DIM))
+    s_dev = torch.from_numpy(s).cuda()
+    nv, _ = _isotropic_kset(basis, 5.0, 400.0)
+    edges = np.linspace(0.0, 0.2 * np.sqrt(N_PART), 201)
+
+    def one():
+        isotropic_structure_factor(s_dev, box, 5.0, 400.0)
+        pair_distance_histogram(s_dev, box, edges)
+        for i in range(b):
+            nearest_neighbor_distances(s_dev[i], box)
+
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    for _ in range(args.steps):
+        isotropic_structure_factor(s_dev, box, 5.0, 400.0)
+    e1.record(stream)
+    for _ in range(args.steps):
+        pair_distance_histogram(s_dev, box, edges)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    sk_ms = e0.elapsed_time(e1) / args.steps
+    pr_ms = e1.elapsed_time(e2) / args.steps
+    sk_pairs = b * N_PART * nv.shape[0]
+    hist_pairs = b * N_PART * (N_PART - 1) / 2
+    t0 = time.perf_counter()
+    oracle.structure_factor_direct(s[0], nv[:2000])
+    cpu_sk = (time.perf_counter() - t0) / (N_PART * 2000)
+    t0 = time.perf_counter()
+    oracle.min_image_distances(s[0], basis)
+    cpu_pair = (time.perf_counter() - t0) / (N_PART * (N_PART - 1) / 2)
+    line = {
+        "metric": "isotropic S(k) (k, particle) pairs/s", "value": sk_pairs / (sk_ms / 1e3),
+        "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sk_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"analysis_d{DIM}_n{N_PART}_b{b}", "sk_kvectors": int(nv.shape[0]),
+                   "pair_histogram_ms": pr_ms, "pair_histogram_pairs_per_s": hist_pairs / (pr_ms / 1e3),
+                   "g2_bins": 200},
+        "cpu_baseline": {"value": 1.0 / cpu_sk, "unit": "pairs/s", "cores": 1, "kind": "port",
+                         "sample": "oracle direct sum: 1 config x 2000 k; pair oracle 1 config",
+                         "pair_histogram_pairs_per_s": 1.0 / cpu_pair},
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def run_profile(args) -> None:
     """Kernel-level profiling driver (run under ncu): no timing, no JSON."""
     import torch
@@ -626,7 +788,10 @@ def main() -> None:
     ap.add_argument("--profile", choices=["eval", "relax"], default=None,
                     help="profiling driver for ncu: run the kernels only")  # fmt: skip
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--workload", choices=["batch", "mixed", "serve", "precision"], default="batch",
+    ap.add_argument("--md-lanes", type=int, default=64)
+    ap.add_argument("--md-steps", type=int, default=2000)
+    ap.add_argument("--workload", choices=["batch", "mixed", "serve", "precision", "md", "analysis"],
+                    default="batch",
                     help="batch: the headline 256-lane d2 N1000 relax; mixed: the 512-instance "
                          "mixed-size ensemble; serve: a Poisson request stream")  # fmt: skip
     ap.add_argument("--mixed-count", type=int, default=512)
@@ -646,6 +811,10 @@ def main() -> None:
         run_serve(args)
     elif args.workload == "precision" and args.impl == "cco":
         run_precision(args)
+    elif args.workload == "md" and args.impl == "cco":
+        run_md(args)
+    elif args.workload == "analysis" and args.impl == "cco":
+        run_analysis(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
