@@ -648,7 +648,10 @@ def run_md(args) -> None:
     r0 = rng.uniform(size=(lanes, N_PART, DIM)) @ basis
     v0 = rng.normal(scale=0.03, size=(lanes, N_PART, DIM))
     keys = np.stack([make_key(i) for i in range(lanes)])
-    lane0 = init_state(energy, waves, basis, r0, v0, np.full(lanes, 1e-3), keys, st)
+    # device-resident state (CUDA tensors) for the device number; NumPy in/out for e2e
+    lane0 = init_state(energy, waves, basis, torch.from_numpy(r0).cuda(), torch.from_numpy(v0).cuda(),
+                       np.full(lanes, 1e-3), keys, st)  # fmt: skip
+    host0 = init_state(energy, waves, basis, r0, v0, np.full(lanes, 1e-3), keys, st)
     for _ in range(args.warmup):
         simulate(energy, waves, basis, st, lane0, max(n_steps // 10, 1))
     torch.cuda.synchronize()
@@ -666,6 +669,12 @@ def run_md(args) -> None:
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.steps
     value = lanes * n_steps / (ms / 1e3)
+    t0 = time.perf_counter()
+    simulate(energy, waves, basis, st, host0, n_steps)
+    e2e_s = time.perf_counter() - t0
+    buf_bytes = sum(int(np.asarray(x).nbytes) for x in (host0.snap.r, host0.snap.rho, host0.snap.wind_abs,
+                                                        host0.snap.wind_net, host0.trace.rho, host0.r,
+                                                        host0.v, host0.f, host0.rho_prev))  # fmt: skip
     w = int(waves.n_vectors.shape[0])
     cpu_s = None if args.no_cpu_baseline else _md_host_sample(ks, basis, waves, r0[0], v0[0], 20)
     # device-side algorithmic flops per lane-step: force (F_PAIR N M) + fresh waves every 10 steps
@@ -680,12 +689,16 @@ def run_md(args) -> None:
         "config": {"workload": f"md_segment_d{DIM}_n{N_PART}_chi{CHI}_lanes{lanes}_steps{n_steps}",
                    "waves": w, "constrained": int(waves.n_constrained), "wind_every": 10,
                    "snapshots": len(st.record_steps), "trace_rows": st.max_rho_records,
-                   "final_status_running": int((res.state.status == 0).sum()),
+                   "final_status_running": int((res.state.status == 0).sum().item()),
+                   "state": "device-resident (CUDA tensors)",
                    "wall_s_per_step": wall / args.steps},
         "roofline": {"kernel": "whole MD segment (evaluations + step + observables)", "bound": "fp64",
                      "achieved": flops / (ms / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
                      "frac": flops / (ms / 1e3) / 1e12 / peak if peak else None,
                      "algorithmic": "F_PAIR N M per force + 40 flops per (fresh wave, particle) every 10 steps"},
+        "e2e": {"value": lanes * n_steps / e2e_s, "unit": "lane-steps/s",
+                "h2d_bytes_per_step": buf_bytes, "d2h_bytes_per_step": buf_bytes,
+                "note": "simulate() with a NumPy state: one upload and one download of the state"},
         "cpu_baseline": None if cpu_s is None else {
             "value": 1.0 / cpu_s, "unit": "lane-steps/s", "cores": 1, "kind": "port",
             "sample": "oracle chain: 20 BAOAB steps of one lane, direct-sum forces and all waves' densities"},

@@ -229,3 +229,27 @@ def test_select_dt():
     assert dt in (0.05, 0.005)
     with pytest.raises(ValueError):
         select_dt(en, waves, basis, lanes, [0.5], 40, 1e-14)
+
+
+def test_device_resident_state_matches_host_state():
+    """CUDA-tensor states stay on the device and give the same results bit for bit."""
+    import torch
+
+    en, waves, basis, ks = _system()
+    r0, v0 = _start(2, 48, 2, basis, 21)
+    st = MDSettings(dt=0.02, scheme="baoab", gamma=1.0, chunk_steps=3, wind_every=2,
+                    record_steps=(2, 4), record_rho_every=1, max_rho_records=5, drift_tol=math.inf)  # fmt: skip
+    keys = np.stack([make_key(7), make_key(8)])
+    host = init_state(en, waves, basis, r0, v0, np.array([0.2, 0.3]), keys, st)
+    dev = init_state(en, waves, basis, torch.from_numpy(r0).cuda(), torch.from_numpy(v0).cuda(),
+                     np.array([0.2, 0.3]), keys, st)  # fmt: skip
+    assert dev.r.is_cuda and dev.snap.rho.is_cuda
+    a = simulate(en, waves, basis, st, host, 7).state
+    b = simulate(en, waves, basis, st, dev, 7).state
+    assert b.r.is_cuda
+    for f in ("r", "v", "f", "phi", "rho_prev", "wind_abs", "sum_s", "step", "status"):
+        np.testing.assert_array_equal(getattr(a, f), getattr(b, f).cpu().numpy())
+    np.testing.assert_array_equal(a.key, b.key.cpu().numpy().view(np.uint32))
+    np.testing.assert_array_equal(a.trace.rho, b.trace.rho.cpu().numpy())
+    seg = begin_segment(b, st, True, True)
+    assert seg.r.is_cuda and torch.isnan(seg.rho_prev).all()

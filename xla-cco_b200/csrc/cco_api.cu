@@ -326,7 +326,7 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     P.gc0 = c0;
     P.gm1 = d >= 3 ? m1 : 0;
     P.gc1 = c1;
-    P.gs0 = c0 | 1;
+    P.gs0 = (c0 + 1) | 1;   // odd, with a spare column c0 (zeros in the d = 2 kernel)
     P.gs1 = c1 > 0 ? (c1 | 1) : 0;
     // fill units: the fewest rounds of one unit per thread, then the
     // shortest chains (each unit seeds with sincospi, then multiplies)

@@ -720,6 +720,98 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
   }
 }
 
+// d = 2: the A rows are a gather from the prefix table (A[r][j] = T0[j][n0(r)]),
+// so there is no A phase. The tables are double-buffered: while the CTA
+// multiplies chunk c it fills chunk c + 1 (and the roots of chunk c + 2), one
+// barrier per chunk. Rows past the group's runs read the zero column c0.
+__device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int tile, int blk,
+                                   double2* smem) {
+  constexpr int KC = kGemmChunk, D = 2;
+  const GemmBlock B = P.gblk[blk];
+  const int j0 = tile * kPass1Tile;
+  const int nj = min(kPass1Tile, P.N - j0);
+  const int c0 = P.gc0, s0 = P.gs0;           // s0 > c0: column c0 holds zeros
+  const int buf = KC * (s0 + kGemmZStride);   // one table set
+  double2* R = smem + 2 * buf;                // [2][KC * D] roots
+  const int tr = threadIdx.x >> 4, tn = threadIdx.x & 15;
+  int off[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int r = 3 * tr + i;
+    off[i] = r < B.nrun ? P.grun[B.run0 + r].n0 - P.gm0 : c0;
+  }
+  double2 acc[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) acc[i][c] = make_double2(0.0, 0.0);
+  const int L = P.gL, u0 = P.gu0, uz = P.guz;
+  const int nch = (nj + KC - 1) / KC;
+  auto fill = [&](int c) {   // tables of chunk c into buffer c & 1 (roots in R[c & 1])
+    double2* T0 = smem + (c & 1) * buf;
+    double2* Z = T0 + KC * s0;
+    const double2* zs = R + (c & 1) * KC * D;
+    const int jc = c * KC, kc = min(KC, nj - jc);
+    for (int u = threadIdx.x; u < KC * (u0 + uz); u += blockDim.x) {
+      const int j = u % KC, q = u / KC;
+      const double* sj = ln.s + (size_t)(j0 + jc + j) * D;
+      const bool live = j < kc;
+      if (q < u0) {
+        fill_powers(T0 + j * s0, L * q, min(L, c0 - L * q), P.gm0, live ? sj[0] : 0.0, zs[j * D]);
+      } else {
+        const int qq = q - u0;
+        fill_powers(Z + j * kGemmZStride, L * qq, min(L, kGemmCols - L * qq), B.lo,
+                    live ? sj[1] : 0.0, zs[j * D + 1]);
+      }
+    }
+    if (threadIdx.x < KC) T0[threadIdx.x * s0 + c0] = make_double2(0.0, 0.0);
+  };
+  chunk_roots<D>(R, ln.s, j0, min(KC, nj));
+  if (nch > 1) chunk_roots<D>(R + KC * D, ln.s, j0 + KC, min(KC, nj - KC));
+  __syncthreads();
+  fill(0);
+  __syncthreads();
+  for (int c = 0; c < nch; ++c) {
+    if (c + 1 < nch) fill(c + 1);
+    if (c + 2 < nch)   // roots of chunk c + 2 replace those of chunk c (used by fill(c), done)
+      chunk_roots<D>(R + (c & 1) * KC * D, ln.s, j0 + (c + 2) * KC, min(KC, nj - (c + 2) * KC));
+    const double2* T0 = smem + (c & 1) * buf;
+    const double2* Z = T0 + KC * s0;
+    const int kc = min(KC, nj - c * KC);
+    for (int j = 0; j < kc; ++j) {
+      double2 a[3], z[3];
+#pragma unroll
+      for (int i = 0; i < 3; ++i) a[i] = T0[j * s0 + off[i]];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) z[q] = Z[j * kGemmZStride + tn + 16 * q];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          acc[i][q].x = fma(a[i].x, z[q].x, acc[i][q].x);
+          acc[i][q].x = fma(-a[i].y, z[q].y, acc[i][q].x);
+          acc[i][q].y = fma(a[i].x, z[q].y, acc[i][q].y);
+          acc[i][q].y = fma(a[i].y, z[q].x, acc[i][q].y);
+        }
+    }
+    __syncthreads();
+  }
+  double2* out = ln.part + (size_t)tile * P.M;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int r = 3 * tr + i;
+    if (r < B.nrun) {
+      const GemmRun g = P.grun[B.run0 + r];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int col = tn + 16 * q;
+        const int n = B.lo + col;
+        if (col < B.nb && n >= g.a && n <= g.b) out[g.kstart + (n - g.a)] = acc[i][q];
+      }
+    }
+  }
+}
+
 template <int D>
 __global__ void __launch_bounds__(kGemmThreads, 4) k_pass1_gemm(EvalPlan plan) {
   extern __shared__ double2 smem[];
@@ -730,7 +822,10 @@ __global__ void __launch_bounds__(kGemmThreads, 4) k_pass1_gemm(EvalPlan plan) {
   if (plan.dyn_prec && lane_prec(ln) == PREC_FP32) return;   // the FP32 body handles it
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
-  pass1_gemm_body<D>(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
+  if constexpr (D == 2)
+    pass1_gemm_body_d2(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
+  else
+    pass1_gemm_body<D>(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
 }
 
 // One kernel per dimension D (and per precision mode) keeps each kernel's
@@ -848,6 +943,8 @@ size_t eval_smem1(const ProbDev& p) {
 
 size_t eval_smemG(const ProbDev& p) {
   if (!p.gemm) return 0;
+  if (p.d == 2)   // two table sets (prefix, last axis) and two root sets
+    return (size_t)kGemmChunk * (2 * (p.gs0 + kGemmZStride) + 2 * p.d) * sizeof(double2);
   const int s1 = p.d == 3 ? p.gs1 : 0;
   return (size_t)kGemmChunk * (p.gs0 + s1 + kGemmZStride + kGemmRows + 2 * p.d) *
          sizeof(double2);

@@ -28,15 +28,21 @@ def tmp_path_of(path: Path) -> Path:
     return Path(str(path) + TMP_SUFFIX)
 
 
+def _host(x: Any) -> np.ndarray:
+    return x.detach().cpu().numpy() if hasattr(x, "detach") else np.asarray(x)
+
+
 def _flat(state: MDState) -> Dict[str, np.ndarray]:
     out: Dict[str, np.ndarray] = {}
     for f in dataclasses.fields(state):
         v = getattr(state, f.name)
         if isinstance(v, (Snapshots, RhoTrace)):
             for g in dataclasses.fields(v):
-                out[f"{f.name}.{g.name}"] = np.asarray(getattr(v, g.name))
+                out[f"{f.name}.{g.name}"] = _host(getattr(v, g.name))
         else:
-            out[f.name] = np.asarray(v)
+            out[f.name] = _host(v)
+    if out["key"].dtype == np.int32:   # device keys travel as int32 bits
+        out["key"] = out["key"].view(np.uint32)
     return out
 
 

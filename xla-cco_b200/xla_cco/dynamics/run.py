@@ -132,15 +132,15 @@ def make_waves(basis: np.ndarray, k_constraint: float, k_track: float) -> Waves:
 
 
 # ------------------------------------------------------------------ state
-def _batch(x: Any) -> np.ndarray:
-    return np.asarray(x)[None]
+def _batch(x: Any) -> Any:
+    return x[None] if hasattr(x, "shape") else np.asarray(x)[None]
 
 
 def _unbatch(state: MDState) -> MDState:
     def cut(obj):
-        return dataclasses.replace(obj, **{f.name: np.asarray(getattr(obj, f.name))[0]
+        return dataclasses.replace(obj, **{f.name: getattr(obj, f.name)[0]
                                            for f in dataclasses.fields(obj)})  # fmt: skip
-    out = {f.name: np.asarray(getattr(state, f.name))[0] for f in dataclasses.fields(state)
+    out = {f.name: getattr(state, f.name)[0] for f in dataclasses.fields(state)
            if f.name not in ("snap", "trace")}  # fmt: skip
     return MDState(**out, snap=cut(state.snap), trace=cut(state.trace))
 
@@ -175,7 +175,9 @@ def init_state(energy: Any, waves: Waves, basis: Any, r0: Any, v0: Any, temperat
     _check_settings(settings)
     require_float64(r0, "r0")
     require_float64(v0, "v0")
-    r0, v0 = np.asarray(r0), np.asarray(v0)
+    on_dev = hasattr(r0, "is_cuda") and bool(r0.is_cuda)
+    host = lambda x: x.detach().cpu().numpy() if hasattr(x, "detach") else np.asarray(x)  # noqa: E731
+    r0, v0, temperature, key = host(r0), host(v0), host(temperature), host(key)
     single = r0.ndim == 2
     if single:
         require_key(np.asarray(key))
@@ -203,7 +205,9 @@ def init_state(energy: Any, waves: Waves, basis: Any, r0: Any, v0: Any, temperat
         sum_phi2=zf.copy(), sum_s=np.zeros((b, w)), n_sum=np.zeros(b, np.int64),
         status=np.full(b, STATUS_RUNNING, np.int64), snap=snap, trace=trace,
     )  # fmt: skip
-    out = _segment(energy, waves, basis, settings, st, 0)
+    dev = _to_device(st)
+    _run_device(energy, waves, basis, settings, dev, 0)
+    out = _from_device(dev, to_host=not on_dev)
     return _unbatch(out) if single else out
 
 
@@ -212,27 +216,39 @@ def begin_segment(state: MDState, settings: MDSettings, reset_sums: bool,
     """Start a segment: optional COM momentum removal (``settings.remove_com``),
     e0 = Phi + KE, max_drift = 0, optional reset of the sums and of the winding
     (rho_prev then pending: recomputed before the next step). Lanes whose
-    status is not STATUS_RUNNING are returned unchanged."""
-    run = np.asarray(state.status) == STATUS_RUNNING
-    v = state.v - np.mean(state.v, axis=-2, keepdims=True) if settings.remove_com else state.v
+    status is not STATUS_RUNNING are returned unchanged. NumPy or CUDA-tensor
+    states; the result is of the same kind."""
+    if _on_device(state):
+        import torch as xp
 
-    def pick(new, old, extra=0):
-        m = run.reshape(run.shape + (1,) * (np.ndim(old) - run.ndim))
-        return np.where(m, new, old)
+        mean = lambda x: x.mean(dim=-2, keepdim=True)  # noqa: E731
+        ke = lambda v: 0.5 * (v * v).sum(dim=(-2, -1))  # noqa: E731
+        zeros, full = xp.zeros_like, lambda x, val: xp.full_like(x, val)  # noqa: E731
+    else:
+        xp = np
+        mean = lambda x: np.mean(x, axis=-2, keepdims=True)  # noqa: E731
+        ke = kinetic_energy
+        zeros, full = np.zeros_like, lambda x, val: np.full_like(x, val)  # noqa: E731
+    run = state.status == STATUS_RUNNING
 
+    def pick(new, old):
+        m = run.reshape(tuple(run.shape) + (1,) * (old.ndim - run.ndim))
+        return xp.where(m, new, old)
+
+    v = state.v - mean(state.v) if settings.remove_com else state.v
     out = dataclasses.replace(state)
     out.v = pick(v, state.v)
-    out.e0 = pick(state.phi + kinetic_energy(out.v), state.e0)
-    out.max_drift = pick(np.zeros_like(state.max_drift), state.max_drift)
+    out.e0 = pick(state.phi + ke(out.v), state.e0)
+    out.max_drift = pick(zeros(state.max_drift), state.max_drift)
     if reset_sums:
         for name in ("sum_kinetic", "sum_phi", "sum_phi2", "sum_s", "n_sum"):
             old = getattr(state, name)
-            setattr(out, name, pick(np.zeros_like(old), old))
+            setattr(out, name, pick(zeros(old), old))
     if reset_winding:
         for name in ("wind_abs", "wind_net", "n_valid"):
             old = getattr(state, name)
-            setattr(out, name, pick(np.zeros_like(old), old))
-        out.rho_prev = pick(np.full_like(state.rho_prev, np.nan), state.rho_prev)
+            setattr(out, name, pick(zeros(old), old))
+        out.rho_prev = pick(full(state.rho_prev, float("nan")), state.rho_prev)
     return out
 
 
@@ -240,13 +256,55 @@ def begin_segment(state: MDState, settings: MDSettings, reset_sums: bool,
 _SCHEME_C = {"verlet": (0, 0), "andersen": (0, None), "baoab": (1, 0)}
 
 
-def _segment(energy: Any, waves: Waves, basis: Any, settings: MDSettings, state: MDState,
-             n_steps: int) -> MDState:  # fmt: skip
-    """One ``cco_md_segment`` call over a batched state; returns the new state."""
+def _on_device(state: MDState) -> bool:
+    r = state.r
+    return hasattr(r, "is_cuda") and bool(r.is_cuda)
+
+
+def _fields(state: MDState) -> Dict[str, Any]:
+    out: Dict[str, Any] = {}
+    for f in dataclasses.fields(state):
+        v = getattr(state, f.name)
+        if f.name in ("snap", "trace"):
+            for g in dataclasses.fields(v):
+                out[f"{f.name}_{g.name}"] = getattr(v, g.name)
+        else:
+            out["keys" if f.name == "key" else f.name] = v
+    return out
+
+
+def _to_device(state: MDState) -> Dict[str, Any]:
+    """Device copies of every array (uint32 keys travel as int32 bits)."""
+    import torch
+
+    dev: Dict[str, Any] = {}
+    for k, v in _fields(state).items():
+        if isinstance(v, torch.Tensor):
+            dev[k] = v.detach().to("cuda").contiguous().clone()
+        else:
+            a = np.ascontiguousarray(np.asarray(v))
+            dev[k] = torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).cuda()
+    return dev
+
+
+def _from_device(dev: Dict[str, Any], to_host: bool) -> MDState:
+    vals = {k: (t.cpu().numpy() if to_host else t) for k, t in dev.items()}
+    if to_host:
+        vals["keys"] = vals["keys"].view(np.uint32)
+    snap = Snapshots(**{g.name: vals[f"snap_{g.name}"] for g in dataclasses.fields(Snapshots)})
+    trace = RhoTrace(**{g.name: vals[f"trace_{g.name}"] for g in dataclasses.fields(RhoTrace)})
+    plain = {f.name: vals["keys" if f.name == "key" else f.name] for f in dataclasses.fields(MDState)
+             if f.name not in ("snap", "trace")}  # fmt: skip
+    return MDState(**plain, snap=snap, trace=trace)
+
+
+def _run_device(energy: Any, waves: Waves, basis: Any, settings: MDSettings, dev: Dict[str, Any],
+                n_steps: int) -> None:  # fmt: skip
+    """One ``cco_md_segment`` call over the device arrays ``dev`` (updated in place)."""
     import torch
 
     _native.require_gpu()
-    b, n, d = state.r.shape
+    b, n, d = dev["r"].shape
     w = int(waves.kvec.shape[0])
     bm = np.ascontiguousarray(np.asarray(basis, dtype=np.float64))
     if bm.shape != (d, d):
@@ -258,8 +316,8 @@ def _segment(energy: Any, waves: Waves, basis: Any, settings: MDSettings, state:
     if not np.allclose(kv, nv @ (2.0 * math.pi * np.linalg.inv(bm).T), rtol=1e-9, atol=1e-12):
         raise ValueError("waves.kvec must equal n_vectors 2 pi B^-T for this basis")
     rows = _constrained_rows(energy, waves)
-    dev = torch.cuda.current_device()
-    h = energy.problem_handle(dev, n)
+    idx = dev["r"].device.index
+    h = energy.problem_handle(idx if idx is not None else torch.cuda.current_device(), n)
     scheme, mode = _SCHEME_C[settings.scheme]
     if mode is None:
         mode = 1 if settings.andersen_mode == "count" else 2
@@ -272,36 +330,23 @@ def _segment(energy: Any, waves: Waves, basis: Any, settings: MDSettings, state:
     )  # fmt: skip
     cw = _native.MdWavesC(w, int(waves.n_constrained), nv.ctypes.data, kv.ctypes.data,
                           rows.ctypes.data)  # fmt: skip
-    arrays: Dict[str, np.ndarray] = {}
-    for f in dataclasses.fields(state):
-        v = getattr(state, f.name)
-        if f.name in ("snap", "trace"):
-            for g in dataclasses.fields(v):
-                arrays[f"{f.name}_{g.name}"] = np.asarray(getattr(v, g.name))
-        else:
-            arrays[f.name] = np.asarray(v)
-    arrays["keys"] = arrays.pop("key")
-    tens = {}
-    for k, a in arrays.items():
-        a = np.ascontiguousarray(a)
-        if a.dtype == np.uint32:
-            a = a.view(np.int32)
-        tens[k] = torch.from_numpy(a.copy()).cuda()
     cst = _native.MdStateC()
     for name in _native.MD_STATE_FIELDS:
-        setattr(cst, name, tens[name].data_ptr())
+        setattr(cst, name, dev[name].data_ptr())
     ticks = ctypes.c_int64(0)
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    code = _native.load().cco_md_segment(h, stream, b, bm.ctypes.data, ctypes.byref(cs),
-                                         ctypes.byref(cw), ctypes.byref(cst), ctypes.byref(ticks))  # fmt: skip
+    with torch.cuda.device(dev["r"].device):
+        stream = torch.cuda.current_stream().cuda_stream
+        code = _native.load().cco_md_segment(h, stream, b, bm.ctypes.data, ctypes.byref(cs),
+                                             ctypes.byref(cw), ctypes.byref(cst), ctypes.byref(ticks))  # fmt: skip
     _native.check(code, "cco_md_segment")
-    host = {k: t.cpu().numpy() for k, t in tens.items()}
-    host["keys"] = host["keys"].view(np.uint32)
-    snap = Snapshots(**{g.name: host[f"snap_{g.name}"] for g in dataclasses.fields(Snapshots)})
-    trace = RhoTrace(**{g.name: host[f"trace_{g.name}"] for g in dataclasses.fields(RhoTrace)})
-    plain = {f.name: host["keys" if f.name == "key" else f.name] for f in dataclasses.fields(MDState)
-             if f.name not in ("snap", "trace")}  # fmt: skip
-    return MDState(**plain, snap=snap, trace=trace)
+
+
+def _segment(energy: Any, waves: Waves, basis: Any, settings: MDSettings, state: MDState,
+             n_steps: int) -> MDState:  # fmt: skip
+    """One device call over a batched state; the result is of the state's kind."""
+    dev = _to_device(state)
+    _run_device(energy, waves, basis, settings, dev, n_steps)
+    return _from_device(dev, to_host=not _on_device(state))
 
 
 def md_chunk(energy: Any, waves: Waves, basis: Any, settings: MDSettings, state: MDState,
@@ -311,7 +356,7 @@ def md_chunk(energy: Any, waves: Waves, basis: Any, settings: MDSettings, state:
     Lanes that are not STATUS_RUNNING (or stop on a drift) keep their state
     from then on; pending rho_prev rows are recomputed first."""
     _check_settings(settings)
-    single = np.ndim(state.step) == 0
+    single = len(tuple(state.step.shape)) == 0
     st = _as_batch(state) if single else state
     _check_lane(st, waves, settings)
     out = _segment(energy, waves, basis, settings, st, min(int(settings.chunk_steps), int(n_steps)))
@@ -335,9 +380,9 @@ def simulate(energy: Any, waves: Waves, basis: Any, settings: MDSettings, state:
     match the settings, constrained waves that are not the energy's first
     n_vectors, n_steps < 0 or checkpoint_every_s <= 0."""
     _check_settings(settings)
-    if np.ndim(state.step) != 1:
+    if len(tuple(state.step.shape)) != 1:
         raise ValueError(f"state must be batched (leading lane axis), got step shape "
-                         f"{np.shape(state.step)}")  # fmt: skip
+                         f"{tuple(state.step.shape)}")  # fmt: skip
     if int(n_steps) != n_steps or n_steps < 0 or not checkpoint_every_s > 0.0:
         raise ValueError(f"need n_steps >= 0 and checkpoint_every_s > 0, got {n_steps}, "
                          f"{checkpoint_every_s}")  # fmt: skip
@@ -345,16 +390,19 @@ def simulate(energy: Any, waves: Waves, basis: Any, settings: MDSettings, state:
         raise ValueError("need at least one lane")
     _check_lane(state, waves, settings)
     _constrained_rows(energy, waves)
+    host = not _on_device(state)
+    dev = _to_device(state)
     done, last = 0, time.monotonic()
-    while done < n_steps and np.any(np.asarray(state.status) == STATUS_RUNNING):
+    while done < n_steps and bool((dev["status"] == STATUS_RUNNING).any()):
         n_this = min(settings.chunk_steps, int(n_steps) - done)
-        state = _segment(energy, waves, basis, settings, state, n_this)
+        _run_device(energy, waves, basis, settings, dev, n_this)
         done += n_this
         if checkpoint is not None and done < n_steps and time.monotonic() - last >= checkpoint_every_s:
-            _write(checkpoint, state, done, int(n_steps))
+            _write(checkpoint, _from_device(dev, True), done, int(n_steps))
             last = time.monotonic()
+    state = _from_device(dev, to_host=host)
     if checkpoint is not None:
-        _write(checkpoint, state, done, int(n_steps))
+        _write(checkpoint, state if host else _from_device(dev, True), done, int(n_steps))
     trace = state.trace if settings.record_rho_every > 0 else None
     return MDResult(state=state, snapshots=state.snap, trace=trace)
 
@@ -367,17 +415,18 @@ def select_dt(energy: Any, waves: Waves, basis: Any, state: MDState, ladder: Seq
     dts = sorted({float(x) for x in ladder}, reverse=True)
     if not dts or not all(math.isfinite(x) and x > 0.0 for x in dts):
         raise ValueError(f"ladder must hold finite positive steps, got {ladder}")
-    if n_steps < 1 or not drift_rel > 0.0 or np.ndim(state.step) != 1:
+    if n_steps < 1 or not drift_rel > 0.0 or len(tuple(state.step.shape)) != 1:
         raise ValueError("need n_steps >= 1, drift_rel > 0 and a batched state")
     for dt in dts:
         st = MDSettings(dt=dt, scheme="verlet", remove_com=False,
                         chunk_steps=min(int(n_steps), 10_000), drift_tol=math.inf)  # fmt: skip
         lanes = init_state(energy, waves, basis, state.r, state.v, state.temperature, state.key, st)
         out = simulate(energy, waves, basis, st, lanes, int(n_steps)).state
-        e_last = out.phi + kinetic_energy(out.v)
-        ke = out.sum_kinetic / np.maximum(out.n_sum, 1)
+        h = lambda x: x.detach().cpu().numpy() if hasattr(x, "detach") else np.asarray(x)  # noqa: E731
+        e_last = h(out.phi) + kinetic_energy(h(out.v))
+        ke = h(out.sum_kinetic) / np.maximum(h(out.n_sum), 1)
         with np.errstate(invalid="ignore", divide="ignore"):
-            rel = np.abs(e_last - lanes.e0) / ke
+            rel = np.abs(e_last - h(lanes.e0)) / ke
         if np.all(rel < drift_rel):
             return dt
     raise ValueError(f"no dt in {tuple(ladder)} keeps the drift below {drift_rel}")
