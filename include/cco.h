@@ -78,6 +78,10 @@ int cco_problem_destroy(cco_problem* p);
 /* Sizes of the device k-set layout (runs split into pass-1/pass-2 segments). */
 int cco_problem_info(const cco_problem* p, int* d, int* n_particles, int* m,
                      int* n_seg1, int* n_seg2, int* table_rows);
+/* Form of the FP64 density pass of a problem: *gemm_blocks > 0 when it runs
+ * as a complex GEMM over (run group x last-axis window) blocks (d >= 2, dense
+ * k-sets), 0 for the per-segment kernel. No reference counterpart. */
+int cco_problem_pass1_form(const cco_problem* p, int* gemm_blocks);
 
 /*
  * Energy, gradient and collective density of `batch` configurations.

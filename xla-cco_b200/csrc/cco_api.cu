@@ -282,7 +282,8 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   }
   // GEMM pass 1: runs grouped kGemmRows at a time by length, each group's
   // last-axis range cut into kGemmCols windows. Used when at least half of
-  // the computed grid cells are k-set rows (CCO_PASS1_GEMM=0 turns it off).
+  // the computed grid cells (rows counted by the warp's 6) are k-set rows
+  // (CCO_PASS1_GEMM=0 turns it off).
   std::vector<GemmRun> grun;
   std::vector<GemmBlock> gblk;
   {
@@ -295,6 +296,7 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
       m1 = std::min(m1, g.n1);
       M1 = std::max(M1, g.n1);
     }
+    double computed = 0.0;   // grid cells the blocks multiply
     std::vector<GemmRun> sorted = runs;
     std::stable_sort(sorted.begin(), sorted.end(), [](const GemmRun& x, const GemmRun& y) {
       return (x.b - x.a) > (y.b - y.a);
@@ -308,6 +310,8 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
       }
       const int run0 = (int)grun.size();
       for (int r = 0; r < nrun; ++r) grun.push_back(sorted[r0 + r]);
+      // warps whose 6 rows lie past the group's runs skip their products
+      computed += (double)((nrun + 5) / 6 * 6) * kGemmCols * ((hi - lo) / kGemmCols + 1);
       for (int w = lo; w <= hi; w += kGemmCols) {
         GemmBlock b{};
         b.run0 = run0;
@@ -317,7 +321,7 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
         gblk.push_back(b);
       }
     }
-    const double cells = (double)gblk.size() * kGemmRows * kGemmCols;
+    const double cells = computed;
     const int c0 = M0 - m0 + 1, c1 = d >= 3 ? M1 - m1 + 1 : 0;
     P.gemm = allow && !runs.empty() && c0 <= kGemmMaxPrefix && c1 <= kGemmMaxPrefix &&
              (double)m >= 0.5 * cells;
@@ -439,6 +443,12 @@ int cco_problem_info(const cco_problem* p, int* d, int* n_particles, int* m, int
   if (n_seg1) *n_seg1 = p->host.nseg1;
   if (n_seg2) *n_seg2 = p->host.nseg2;
   if (table_rows) *table_rows = p->host.t1.nrows * 256 + p->host.t2.nrows;
+  return CCO_OK;
+}
+
+int cco_problem_pass1_form(const cco_problem* p, int* gemm_blocks) {
+  if (!p || !gemm_blocks) return fail(CCO_ERR_ARG, "null argument");
+  *gemm_blocks = p->host.gemm ? p->host.ngblk : 0;
   return CCO_OK;
 }
 

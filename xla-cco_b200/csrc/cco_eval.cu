@@ -687,7 +687,8 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
     if (jc + KC < nj) chunk_roots<D>(R + (buf ^ 1) * KC * D, ln.s, j0 + jc + KC, min(KC, nj - jc - KC));
     buf ^= 1;
     __syncthreads();
-    for (int j = 0; j < kc; ++j) {
+    const int kr = 6 * (threadIdx.x >> 5) < B.nrun ? kc : 0;   // warps past the runs skip
+    for (int j = 0; j < kr; ++j) {
       double2 a[3], z[3];
 #pragma unroll
       for (int i = 0; i < 3; ++i) a[i] = A[j * kGemmRows + 3 * tr + i];
@@ -734,6 +735,7 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
   const int buf = KC * (s0 + kGemmZStride);   // one table set
   double2* R = smem + 2 * buf;                // [2][KC * D] roots
   const int tr = threadIdx.x >> 4, tn = threadIdx.x & 15;
+  const bool rows_live = 6 * (threadIdx.x >> 5) < B.nrun;   // this warp's rows 6w .. 6w + 5
   int off[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -777,7 +779,7 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
       chunk_roots<D>(R + (c & 1) * KC * D, ln.s, j0 + (c + 2) * KC, min(KC, nj - (c + 2) * KC));
     const double2* T0 = smem + (c & 1) * buf;
     const double2* Z = T0 + KC * s0;
-    const int kc = min(KC, nj - c * KC);
+    const int kc = rows_live ? min(KC, nj - c * KC) : 0;
     for (int j = 0; j < kc; ++j) {
       double2 a[3], z[3];
 #pragma unroll

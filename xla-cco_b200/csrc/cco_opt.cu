@@ -681,14 +681,13 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
   const int k = Lp->hk, m = A.m, head = Lp->hhead;
   double* sc = v.scal;
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
-  // three packings: triSY (SY[p][q] = s_p . y_q, p older than q) by newer rows
-  // (tri(p, q) = q (q + 1) / 2 + p) for loop 1, triSO by older rows
-  // (off(p) + q - p, off(p) = p k - p (p - 1) / 2) for loop 2, triYY (the
-  // symmetric YY) by newer rows
+  // two packings by newer rows (tri(p, q) = q (q + 1) / 2 + p, p <= q):
+  // triSY (SY[p][q] = s_p . y_q, p older than q) and triYY (the symmetric YY).
+  // Two triangles (2 m (m + 1) / 2 doubles, 81 KB at m = 100) let two CTAs
+  // share an SM, so a 256-lane update runs in one wave.
   const size_t tri_n = (size_t)m * (m + 1) / 2;
   double* triSY = A.smem_tri ? dsm : v.tri;
-  double* triSO = triSY + tri_n;
-  double* triYY = triSO + tri_n;
+  double* triYY = triSY + tri_n;
   if (k > 0) {
     const double* SYt = v.SY;
     const double* YYs = v.YY;
@@ -702,7 +701,6 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
     constexpr int U = 8;
     for (int t0 = threadIdx.x; t0 < total; t0 += U * blockDim.x) {
       double xs[U], xy[U];
-      int qs[U], ps[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int t = t0 + u * blockDim.x;
@@ -710,8 +708,6 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
         while (q * (q + 1) / 2 > t) --q;
         while ((q + 1) * (q + 2) / 2 <= t) ++q;
         const int p = t - q * (q + 1) / 2;
-        qs[u] = q;
-        ps[u] = p;
         if (t < total) {
           xs[u] = SYt[(size_t)sl[q] * m + sl[p]];
           xy[u] = YYs[(size_t)sl[q] * m + sl[p]];
@@ -721,10 +717,8 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
       for (int u = 0; u < U; ++u) {
         const int t = t0 + u * blockDim.x;
         if (t < total) {
-          const int q = qs[u], p = ps[u];
           triSY[t] = xs[u];
           triYY[t] = xy[u];
-          triSO[p * k - p * (p - 1) / 2 + (q - p)] = xs[u];
         }
       }
     }
@@ -805,14 +799,14 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
         const int top = min(31, k - 1 - 32 * oi);
         for (int own = 0; own <= top; ++own) {
           const int p = 32 * oi + own;
-          const double* row = triSO + (p * k - p * (p - 1) / 2) - p;  // row[q] = SY[p][q]
+          const double* col = triSY + p;   // col[q (q + 1) / 2] = SY[p][q]
           const double bp = __shfl_sync(0xffffffffu, rh[p] * (gam * bet[p] + u[oi]), own);
           const double dq = alp[p] - bp;
           if (wl == 0) bet[p] = bp;
 #pragma unroll
           for (int i = oi; i < R8; ++i) {
             const int q = 32 * i + wl;
-            if (q > p && q < k) u[i] += dq * row[q];
+            if (q > p && q < k) u[i] += dq * col[q * (q + 1) / 2];
           }
         }
       }
@@ -955,7 +949,7 @@ cudaError_t descent_finalize(const DescentArgs& a, double* s_out, double* e_out,
   return cudaGetLastError();
 }
 
-size_t lbfgs_update_smem(int m) { return 3 * ((size_t)m * (m + 1) / 2) * sizeof(double); }
+size_t lbfgs_update_smem(int m) { return 2 * ((size_t)m * (m + 1) / 2) * sizeof(double); }
 cudaError_t lbfgs_configure(size_t smem) {
   return cudaFuncSetAttribute(k_lbfgs_scalar, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)smem);

@@ -113,7 +113,7 @@ __host__ __device__ __forceinline__ size_t lb_scal_len(int m, int ld) {
 }
 
 // Record: [0, 32) LbState, pf at [31]; SY (m m, row = newer slot), YY (m m);
-// the packed triangles of the scalar kernel (tri_len = 3 m (m + 1) / 2 when
+// the packed triangles of the scalar kernel (tri_len = m (m + 1) when
 // they do not fit in shared memory, else 0); the scalar row; x, s, g, dir, glo, ps, pg (ld each); the
 // history rings S and Y (m ld each); the evaluation scratch.
 struct LbView {

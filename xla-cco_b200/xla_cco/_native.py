@@ -229,6 +229,7 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp],
     ),  # fmt: skip
+    "cco_problem_pass1_form": (ctypes.c_int, [_vp, _c_int_p]),
     "cco_md_segment": (
         ctypes.c_int,
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(MdSegmentSettingsC), ctypes.POINTER(MdWavesC),
