@@ -289,13 +289,7 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   {
     const char* env = getenv("CCO_PASS1_GEMM");
     const bool allow = d >= 2 && !(env && atoi(env) == 0);
-    int m0 = 1 << 30, M0 = -(1 << 30), m1 = 1 << 30, M1 = -(1 << 30);
-    for (const GemmRun& g : runs) {
-      m0 = std::min(m0, g.n0);
-      M0 = std::max(M0, g.n0);
-      m1 = std::min(m1, g.n1);
-      M1 = std::max(M1, g.n1);
-    }
+    int c0 = 0, c1 = 0;      // widest group prefix windows
     double computed = 0.0;   // grid cells the blocks multiply
     std::vector<GemmRun> sorted = runs;
     std::stable_sort(sorted.begin(), sorted.end(), [](const GemmRun& x, const GemmRun& y) {
@@ -304,10 +298,20 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     for (size_t r0 = 0; r0 < sorted.size(); r0 += kGemmRows) {
       const int nrun = (int)std::min<size_t>(kGemmRows, sorted.size() - r0);
       int lo = 1 << 30, hi = -(1 << 30);
+      int gm0 = 1 << 30, gM0 = -(1 << 30), gm1 = 1 << 30, gM1 = -(1 << 30);
       for (int r = 0; r < nrun; ++r) {
-        lo = std::min(lo, sorted[r0 + r].a);
-        hi = std::max(hi, sorted[r0 + r].b);
+        const GemmRun& g = sorted[r0 + r];
+        lo = std::min(lo, g.a);
+        hi = std::max(hi, g.b);
+        gm0 = std::min(gm0, g.n0);
+        gM0 = std::max(gM0, g.n0);
+        gm1 = std::min(gm1, g.n1);
+        gM1 = std::max(gM1, g.n1);
       }
+      // each group's prefix tables cover only its own prefixes
+      const int gc0 = gM0 - gm0 + 1, gc1 = d >= 3 ? gM1 - gm1 + 1 : 0;
+      c0 = std::max(c0, gc0);
+      c1 = std::max(c1, gc1);
       const int run0 = (int)grun.size();
       for (int r = 0; r < nrun; ++r) grun.push_back(sorted[r0 + r]);
       // warps whose 6 rows lie past the group's runs skip their products
@@ -318,17 +322,20 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
         b.nrun = nrun;
         b.lo = w;
         b.nb = std::min(kGemmCols, hi - w + 1);
+        b.m0 = gm0;
+        b.c0 = gc0;
+        b.m1 = d >= 3 ? gm1 : 0;
+        b.c1 = gc1;
         gblk.push_back(b);
       }
     }
     const double cells = computed;
-    const int c0 = M0 - m0 + 1, c1 = d >= 3 ? M1 - m1 + 1 : 0;
     P.gemm = allow && !runs.empty() && c0 <= kGemmMaxPrefix && c1 <= kGemmMaxPrefix &&
              (double)m >= 0.5 * cells;
     P.ngblk = (int)gblk.size();
-    P.gm0 = m0;
+    P.gm0 = 0;
     P.gc0 = c0;
-    P.gm1 = d >= 3 ? m1 : 0;
+    P.gm1 = 0;
     P.gc1 = c1;
     P.gs0 = (c0 + 1) | 1;   // odd, with a spare column c0 (zeros in the d = 2 kernel)
     P.gs1 = c1 > 0 ? (c1 | 1) : 0;

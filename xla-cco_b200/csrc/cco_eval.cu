@@ -636,7 +636,7 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
   const GemmBlock B = P.gblk[blk];
   const int j0 = tile * kPass1Tile;
   const int nj = min(kPass1Tile, P.N - j0);
-  const int c0 = P.gc0, c1 = D == 3 ? P.gc1 : 0;
+  const int c0 = B.c0, c1 = D == 3 ? B.c1 : 0;   // this group's prefix windows
   const int s0 = P.gs0, s1 = D == 3 ? P.gs1 : 0;
   double2* T0 = smem;                       // [KC][s0]
   double2* T1 = T0 + KC * s0;               // [KC][s1]
@@ -661,12 +661,14 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
       const double* sj = ln.s + (size_t)(j0 + jc + j) * D;
       const bool live = j < kc;
       if (q < u0) {
-        fill_powers(T0 + j * s0, L * q, min(L, c0 - L * q), P.gm0, live ? sj[0] : 0.0,
-                    zs[j * D]);
+        if (L * q < c0)
+          fill_powers(T0 + j * s0, L * q, min(L, c0 - L * q), B.m0, live ? sj[0] : 0.0,
+                      zs[j * D]);
       } else if (q < u0 + u1) {
         const int qq = q - u0;
-        fill_powers(T1 + j * s1, L * qq, min(L, c1 - L * qq), P.gm1, live ? sj[1] : 0.0,
-                    zs[j * D + 1]);
+        if (L * qq < c1)
+          fill_powers(T1 + j * s1, L * qq, min(L, c1 - L * qq), B.m1, live ? sj[1] : 0.0,
+                      zs[j * D + 1]);
       } else {
         const int qq = q - u0 - u1;
         fill_powers(Z + j * kGemmZStride, L * qq, min(L, kGemmCols - L * qq), B.lo,
@@ -679,8 +681,8 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
       double2 v = make_double2(0.0, 0.0);
       if (j < kc && r < B.nrun) {
         const GemmRun g = P.grun[B.run0 + r];
-        v = T0[j * s0 + (g.n0 - P.gm0)];
-        if (D == 3) v = cmul(v, T1[j * s1 + (g.n1 - P.gm1)]);
+        v = T0[j * s0 + (g.n0 - B.m0)];
+        if (D == 3) v = cmul(v, T1[j * s1 + (g.n1 - B.m1)]);
       }
       A[j * kGemmRows + r] = v;
     }
@@ -731,7 +733,8 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
   const GemmBlock B = P.gblk[blk];
   const int j0 = tile * kPass1Tile;
   const int nj = min(kPass1Tile, P.N - j0);
-  const int c0 = P.gc0, s0 = P.gs0;           // s0 > c0: column c0 holds zeros
+  const int c0 = B.c0, s0 = P.gs0;           // s0 > P.gc0 >= c0: column P.gc0 holds zeros
+  const int zc = P.gc0;
   const int buf = KC * (s0 + kGemmZStride);   // one table set
   double2* R = smem + 2 * buf;                // [2][KC * D] roots
   const int tr = threadIdx.x >> 4, tn = threadIdx.x & 15;
@@ -740,7 +743,7 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const int r = 3 * tr + i;
-    off[i] = r < B.nrun ? P.grun[B.run0 + r].n0 - P.gm0 : c0;
+    off[i] = r < B.nrun ? P.grun[B.run0 + r].n0 - B.m0 : zc;
   }
   double2 acc[3][3];
 #pragma unroll
@@ -759,14 +762,15 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
       const double* sj = ln.s + (size_t)(j0 + jc + j) * D;
       const bool live = j < kc;
       if (q < u0) {
-        fill_powers(T0 + j * s0, L * q, min(L, c0 - L * q), P.gm0, live ? sj[0] : 0.0, zs[j * D]);
+        if (L * q < c0)   // the problem's widest window sets the units; this one may be narrower
+          fill_powers(T0 + j * s0, L * q, min(L, c0 - L * q), B.m0, live ? sj[0] : 0.0, zs[j * D]);
       } else {
         const int qq = q - u0;
         fill_powers(Z + j * kGemmZStride, L * qq, min(L, kGemmCols - L * qq), B.lo,
                     live ? sj[1] : 0.0, zs[j * D + 1]);
       }
     }
-    if (threadIdx.x < KC) T0[threadIdx.x * s0 + c0] = make_double2(0.0, 0.0);
+    if (threadIdx.x < KC) T0[threadIdx.x * s0 + zc] = make_double2(0.0, 0.0);
   };
   chunk_roots<D>(R, ln.s, j0, min(KC, nj));
   if (nch > 1) chunk_roots<D>(R + KC * D, ln.s, j0 + KC, min(KC, nj - KC));

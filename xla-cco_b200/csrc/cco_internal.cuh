@@ -57,6 +57,7 @@ struct GemmRun {
 };
 struct GemmBlock {
   int run0, nrun, lo, nb;            // runs [run0, run0 + nrun), columns lo .. lo + nb - 1
+  int m0, c0, m1, c1;                // the group's prefix windows [m, m + c) per axis
 };
 
 // Per-particle phase tables of one pass: row r holds z_a^(e * base^l) for one
@@ -77,7 +78,7 @@ struct ProbDev {
   int ntile1, ntile2;        // particle tiles of pass 1 / pass 2 (pass 2 at split 1)
   int sl2;                   // logical slices of the pass-2 segment pairs (power of 2, <= 8)
   int gemm;                  // 1: FP64 pass 1 runs as the GEMM below
-  int ngblk, gm0, gc0, gm1, gc1;   // GEMM blocks; prefix tables [gm, gm + gc) per axis
+  int ngblk, gm0, gc0, gm1, gc1;   // GEMM blocks; gc0, gc1: the widest group prefix windows
   int gs0, gs1;              // their shared-memory row strides (odd)
   int gL, gu0, gu1, guz;     // table fill: gL entries per unit; units per particle per table
   const GemmBlock* gblk;
