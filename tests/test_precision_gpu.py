@@ -41,7 +41,7 @@ def _system(n, d, chi):
     return box, ks, make_stealthy_energy(box, ks)
 
 
-@pytest.mark.parametrize("n,d,chi,b", [(400, 1, 0.3, 3), (500, 2, 0.4, 3), (300, 3, 0.45, 3)])
+@pytest.mark.parametrize("n,d,chi,b", [(400, 1, 0.3, 3), (500, 2, 0.4, 3), (300, 3, 0.45, 3), (600, 2, 0.49, 3)])
 def test_fp32_evaluation_against_oracle(n, d, chi, b):
     import torch
 
