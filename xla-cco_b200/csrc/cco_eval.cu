@@ -1000,18 +1000,6 @@ void launch_d(const EvalPlan& plan, bool pass2, cudaStream_t stream) {
   }
 }
 
-void launch_pass(const EvalPlan& plan, bool pass2, cudaStream_t stream) {
-  if (plan.dyn_prec) {
-    launch_d<1, true>(plan, pass2, stream);
-    launch_d<2, true>(plan, pass2, stream);
-    launch_d<3, true>(plan, pass2, stream);
-  } else {
-    launch_d<1, false>(plan, pass2, stream);
-    launch_d<2, false>(plan, pass2, stream);
-    launch_d<3, false>(plan, pass2, stream);
-  }
-}
-
 }  // namespace
 
 cudaError_t eval_configure() {
@@ -1029,18 +1017,79 @@ cudaError_t eval_configure() {
   return e;
 }
 
-cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream) {
-  launch_pass(plan, false, stream);
-  {
-    const int n2 = plan.d_offG[2] - plan.d_offG[1], n3 = plan.d_offG[3] - plan.d_offG[2];
-    if (n2 > 0) k_pass1_gemm<2><<<n2, kGemmThreads, plan.smemG, stream>>>(plan);
-    if (n3 > 0) k_pass1_gemm<3><<<n3, kGemmThreads, plan.smemG, stream>>>(plan);
+namespace {
+
+// The pass kernels of dimension D on stream s (pass 1: per-segment and GEMM forms).
+void launch_dim(const EvalPlan& plan, bool pass2, int D, cudaStream_t s) {
+  if (D == 1) {
+    if (plan.dyn_prec) launch_d<1, true>(plan, pass2, s);
+    else launch_d<1, false>(plan, pass2, s);
+  } else if (D == 2) {
+    if (plan.dyn_prec) launch_d<2, true>(plan, pass2, s);
+    else launch_d<2, false>(plan, pass2, s);
+    const int n = plan.d_offG[2] - plan.d_offG[1];
+    if (!pass2 && n > 0) k_pass1_gemm<2><<<n, kGemmThreads, plan.smemG, s>>>(plan);
+  } else {
+    if (plan.dyn_prec) launch_d<3, true>(plan, pass2, s);
+    else launch_d<3, false>(plan, pass2, s);
+    const int n = plan.d_offG[3] - plan.d_offG[2];
+    if (!pass2 && n > 0) k_pass1_gemm<3><<<n, kGemmThreads, plan.smemG, s>>>(plan);
   }
+}
+
+// One pass over every dimension present: in order on `stream`, or, with side
+// streams and more than one dimension, the first dimension on `stream` and the
+// others on side streams forked from it and joined back before returning.
+cudaError_t launch_pass_all(const EvalPlan& plan, bool pass2, cudaStream_t stream,
+                            const EvalSide* side) {
+  bool has[4] = {false, false, false, false};
+  int nd = 0;
+  for (int D = 1; D <= 3; ++D) {
+    has[D] = pass2 ? plan.d_off2[D] > plan.d_off2[D - 1]
+                   : (plan.d_off1[D] > plan.d_off1[D - 1] || plan.d_offG[D] > plan.d_offG[D - 1]);
+    nd += has[D];
+  }
+  if (!side || nd < 2) {
+    for (int D = 1; D <= 3; ++D)
+      if (has[D]) launch_dim(plan, pass2, D, stream);
+    return cudaGetLastError();
+  }
+  cudaError_t e = cudaEventRecord(side->fork, stream);
+  cudaStream_t sd[4] = {stream, stream, stream, stream};
+  int used = 0;
+  bool first = true;
+  for (int D = 1; D <= 3 && e == cudaSuccess; ++D) {
+    if (!has[D]) continue;
+    if (first) {
+      first = false;
+      continue;
+    }
+    sd[D] = side->aux[used++];
+    e = cudaStreamWaitEvent(sd[D], side->fork, 0);
+  }
+  if (e != cudaSuccess) return e;
+  for (int D = 1; D <= 3; ++D)
+    if (has[D]) launch_dim(plan, pass2, D, sd[D]);
+  for (int u = 0; u < used && e == cudaSuccess; ++u) {
+    e = cudaEventRecord(side->join[u], side->aux[u]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, side->join[u], 0);
+  }
+  return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+}  // namespace
+
+cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream, const EvalSide* side) {
+  cudaError_t e = launch_pass_all(plan, false, stream, side);
+  if (e != cudaSuccess) return e;
   if (plan.n_lanes > 0) {
     k_reduce<<<dim3(plan.red_chunks, plan.n_lanes), kReduceChunk, 0, stream>>>(plan);
     k_energy<<<plan.n_lanes, 32, 0, stream>>>(plan);
   }
-  if (plan.want_grad) launch_pass(plan, true, stream);
+  if (plan.want_grad) {
+    e = launch_pass_all(plan, true, stream, side);
+    if (e != cudaSuccess) return e;
+  }
   return cudaGetLastError();
 }
 

@@ -287,7 +287,7 @@ struct TickPlan {
   MdArgs md[kMaxBranches];
   cudaGraphExec_t exec = nullptr;
   int build(const LaneTable& T, const Schedule& sch, cudaStream_t st);
-  cudaError_t tick(cudaStream_t s, int b) const;
+  cudaError_t tick(cudaStream_t s, int b, const EvalSide* side = nullptr) const;
   int launches_per_tick() const;
   void release(cudaStream_t st);
 };

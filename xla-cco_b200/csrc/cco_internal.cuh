@@ -177,7 +177,25 @@ __host__ __device__ __forceinline__ int reduce_chunks(int M) {
   return (M + kReduceChunk - 1) / kReduceChunk;
 }
 
-cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream);
+// Side streams of one launching stream: when a plan holds lanes of several
+// dimensions, each dimension's pass kernels run on their own stream (forked
+// from and joined back into the launching stream with these events), so the
+// small per-dimension grids of a mixed plan overlap instead of running back
+// to back. The kernels and their results are the same either way.
+struct EvalSide {
+  cudaStream_t aux[2];
+  cudaEvent_t fork, join[2];
+};
+cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream,
+                        const EvalSide* side = nullptr);
+// Dimensions whose pass kernels a plan launches (side streams pay off from 2).
+inline int eval_dims(const EvalPlan& p) {
+  int n = 0;
+  for (int D = 1; D <= 3; ++D)
+    n += p.d_off1[D] > p.d_off1[D - 1] || p.d_offG[D] > p.d_offG[D - 1] ||
+         p.d_off2[D] > p.d_off2[D - 1];
+  return n;
+}
 size_t eval_smem1(const ProbDev& p);
 size_t eval_smemG(const ProbDev& p);   // GEMM pass 1 (0 when the problem has none)
 size_t eval_smem2(const ProbDev& p, int split);

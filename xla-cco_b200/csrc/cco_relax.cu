@@ -126,9 +126,18 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
   // back into the first capture stream
   cudaStream_t cap[kMaxBranches] = {};
   cudaEvent_t fork = nullptr, join[kMaxBranches] = {};
+  EvalSide side[kMaxBranches] = {};   // per-dimension side streams of each branch
   cudaError_t e = cudaSuccess;
   for (int b = 0; b < nbr && e == cudaSuccess; ++b)
     e = cudaStreamCreateWithFlags(&cap[b], cudaStreamNonBlocking);
+  for (int b = 0; b < nbr && e == cudaSuccess; ++b) {
+    if (eval_dims(ev[b].plan) < 2) continue;   // one dimension: no side streams
+    for (int u = 0; u < 2 && e == cudaSuccess; ++u) {
+      e = cudaStreamCreateWithFlags(&side[b].aux[u], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&side[b].join[u], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&side[b].fork, cudaEventDisableTiming);
+  }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
   for (int b = 0; b < nbr && e == cudaSuccess; ++b)
     e = cudaEventCreateWithFlags(&join[b], cudaEventDisableTiming);
@@ -143,7 +152,8 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
     e = cudaEventRecord(fork, cap[0]);
     for (int b = 1; b < nbr && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(cap[b], fork, 0);
     for (int t = 0; t < sch.graph_ticks && e == cudaSuccess; ++t)
-      for (int b = 0; b < nbr && e == cudaSuccess; ++b) e = tick(cap[b], b);
+      for (int b = 0; b < nbr && e == cudaSuccess; ++b)
+        e = tick(cap[b], b, side[b].fork ? &side[b] : nullptr);
     for (int b = 1; b < nbr && e == cudaSuccess; ++b) {
       e = cudaEventRecord(join[b], cap[b]);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(cap[0], join[b], 0);
@@ -156,6 +166,11 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
   for (int b = 0; b < nbr; ++b) {
     if (cap[b]) cudaStreamDestroy(cap[b]);
     if (join[b]) cudaEventDestroy(join[b]);
+    for (int u = 0; u < 2; ++u) {
+      if (side[b].aux[u]) cudaStreamDestroy(side[b].aux[u]);
+      if (side[b].join[u]) cudaEventDestroy(side[b].join[u]);
+    }
+    if (side[b].fork) cudaEventDestroy(side[b].fork);
   }
   if (fork) cudaEventDestroy(fork);
   if (ready) cudaEventDestroy(ready);
@@ -163,8 +178,8 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
   return CCO_OK;
 }
 
-cudaError_t TickPlan::tick(cudaStream_t s, int b) const {
-  cudaError_t e = eval_launch(ev[b].plan, s);
+cudaError_t TickPlan::tick(cudaStream_t s, int b, const EvalSide* side) const {
+  cudaError_t e = eval_launch(ev[b].plan, s, side);
   if (e != cudaSuccess) return e;
   if (method == Method::Flow) return flow_update(fl[b], s);
   if (method == Method::Md) return md_update(md[b], s);
