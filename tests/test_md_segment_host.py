@@ -132,3 +132,33 @@ def test_thermal_helpers():
         maxwell_boltzmann(key, 0, 2, 1.0, False)
     with pytest.raises(ValueError):
         kinetic_temperature(v, 0)
+
+
+def test_observable_helpers_match_the_oracle():
+    """com_correct and winding_update (the reference's observables API) against
+    the oracle's restatement used for the device parity tests."""
+    import oracle
+    from xla_cco.dynamics import center_of_mass, com_correct, winding_update
+
+    rng = np.random.default_rng(4)
+    w, n = 9, 30
+    rho_old, rho_new = rng.normal(size=(w, 2)) * 3, rng.normal(size=(w, 2)) * 3
+    rho_new[0] = 0.0                      # below the phase floor: no winding
+    kvec = rng.normal(size=(w, 2))
+    r = rng.uniform(size=(n, 2)) * 5
+    rcm = center_of_mass(r)
+    np.testing.assert_allclose(rcm, r.mean(0))
+    got = com_correct(rho_new, kvec, rcm)
+    ph = kvec @ rcm
+    want = np.stack([rho_new[:, 0] * np.cos(ph) + rho_new[:, 1] * np.sin(ph),
+                     rho_new[:, 1] * np.cos(ph) - rho_new[:, 0] * np.sin(ph)], -1)  # fmt: skip
+    np.testing.assert_allclose(got, want, rtol=1e-15, atol=1e-15)
+    np.testing.assert_allclose(np.hypot(*got.T), np.hypot(*rho_new.T), rtol=1e-14)  # a pure phase
+    active = np.array([True] * 6 + [False] * 3)
+    args = (rho_old, rho_new, np.ones(w), np.full(w, 0.5), np.arange(w, dtype=np.int64), active, n, 1e-16)
+    mine = winding_update(*args)
+    ref = oracle.md_winding(*args)
+    for a, b in zip(mine, ref):
+        np.testing.assert_array_equal(a, b)
+    assert mine[3][0] == 0 and mine[3][1] == 2   # zero density: not counted; active: +1
+    np.testing.assert_array_equal(mine[0][6:], rho_old[6:])   # inactive rows keep rho_prev
