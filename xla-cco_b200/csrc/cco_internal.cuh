@@ -188,6 +188,18 @@ struct EvalSide {
 };
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream,
                         const EvalSide* side = nullptr);
+// Kernels one eval_launch of a plan issues: per dimension the per-segment and
+// GEMM pass-1 kernels and the pass-2 kernel that have items, plus reduce and energy.
+inline int eval_kernels(const EvalPlan& p) {
+  int n = p.n_lanes > 0 ? 2 : 0;
+  for (int D = 1; D <= 3; ++D) {
+    n += p.d_off1[D] > p.d_off1[D - 1];
+    n += p.d_offG[D] > p.d_offG[D - 1];
+    if (p.want_grad) n += p.d_off2[D] > p.d_off2[D - 1];
+  }
+  return n;
+}
+
 // Dimensions whose pass kernels a plan launches (side streams pay off from 2).
 inline int eval_dims(const EvalPlan& p) {
   int n = 0;

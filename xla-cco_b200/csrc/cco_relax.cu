@@ -187,9 +187,13 @@ cudaError_t TickPlan::tick(cudaStream_t s, int b, const EvalSide* side) const {
 }
 
 int TickPlan::launches_per_tick() const {
-  // 4 evaluation kernels + the update kernels (MD segments: + the wave sums)
+  // the evaluation kernels each branch's plan issues + the update kernels
+  // (L-BFGS: probe, pass A, scalar, pass B; MD segments: + the wave sums)
   const int md_waves = method == Method::Md && md[0].w > md[0].nc ? 1 : 0;
-  return nbr * (method == Method::Lbfgs ? 8 : 5 + md_waves);
+  const int upd = method == Method::Lbfgs ? 4 : 1 + md_waves;
+  int n = 0;
+  for (int b = 0; b < nbr; ++b) n += eval_kernels(ev[b].plan) + upd;
+  return n;
 }
 
 void TickPlan::release(cudaStream_t st) {
