@@ -88,3 +88,44 @@ def test_serving_structs_match_header():
     assert ctypes.sizeof(_native.ServerConfigC) == 3 * 8
     assert ctypes.sizeof(_native.RequestResultC) == 12 * 8
     assert ctypes.sizeof(_native.ServerStatsC) == 13 * 8
+
+
+PAIRS = [
+    ("cco_descent_settings", "DescentSettingsC"), ("cco_lbfgs_settings", "LBFGSSettingsC"),
+    ("cco_relax_out", "RelaxOutC"), ("cco_flow_settings", "FlowSettingsC"),
+    ("cco_flow_out", "FlowOutC"), ("cco_md_settings", "MdSettingsC"), ("cco_md_out", "MdOutC"),
+    ("cco_md_segment_settings", "MdSegmentSettingsC"), ("cco_md_waves", "MdWavesC"),
+    ("cco_md_state", "MdStateC"), ("cco_server_config", "ServerConfigC"),
+    ("cco_request_result", "RequestResultC"), ("cco_server_stats", "ServerStatsC"),
+]  # fmt: skip
+
+
+def test_every_ctypes_struct_matches_the_c_layout(tmp_path):
+    """Compile a probe against include/cco.h with the host C compiler and compare
+    every field offset and struct size with the ctypes mirrors."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "cco.h"', "int main(void) {"]
+    for cname, pyname in PAIRS:
+        st = getattr(_native, pyname)
+        lines.append(f'  printf("{pyname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in st._fields_:
+            lines.append(f'  printf("{pyname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "probe"
+    subprocess.run([cc, "-std=c11", "-I", str(HEADER.parent), "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    seen = 0
+    for line in filter(None, out):
+        pyname, field, value = line.split()
+        st = getattr(_native, pyname)
+        got = ctypes.sizeof(st) if field == "size" else getattr(st, field).offset
+        assert got == int(value), f"{pyname}.{field}: ctypes {got} != C {value}"
+        seen += 1
+    assert seen == sum(1 + len(getattr(_native, p)._fields_) for _, p in PAIRS)
