@@ -61,7 +61,7 @@ def main() -> None:
         sc[f"k2_{chi}_{d}"] = float.hex(kv.k_outer_from_ka(ka, 0.05, d))
     sc["chi_13_100_3"] = float.hex(kv.chi_from_count(13, 100, 3))
 
-    # ---- k-sets: BASELINE boxes, C++ MD box, sheared boxes, +-1 ulp shells
+    # ---- k-sets: benchmark boxes, C++ MD box, sheared boxes, +-1 ulp shells
     cases = []
     for n, d, chi in [(100, 3, 0.05), (1000, 2, 0.40), (4000, 3, 0.45), (8000, 1, 0.49),
                       (200, 1, 0.05), (8000, 3, 0.49), (20000, 3, 0.45), (20000, 2, 0.45),

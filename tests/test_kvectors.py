@@ -2,7 +2,7 @@
 
 Golden values come from the reference's own ``enumerate_kvectors`` and
 conversion functions (tests/golden/make_golden.py). Mirrors the reference's
-tests/unit/test_kvectors.py:39-142 plus the BASELINE problem sizes.
+tests/unit/test_kvectors.py:39-142 plus the benchmark problem sizes (d1-d3, N 100-20000).
 """
 
 from __future__ import annotations
