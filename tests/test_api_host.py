@@ -108,3 +108,21 @@ def test_flow_settings_defaults_and_validation():
         gradient_flow(None, np.zeros((4, 2), np.float32), basis, FlowSettings())
     with pytest.raises(ValueError):
         gradient_flow(None, s0, np.eye(3), FlowSettings())
+
+
+def test_top_level_exports_cover_the_reference_package():
+    """Every name the reference's package __init__ exports (src/xla_cco/__init__.py:54-100)."""
+    import xla_cco
+
+    ref_names = {
+        "AbstractEnergy", "Box", "DescentSettings", "KSet", "LBFGSSettings", "PackedConfig",
+        "RelaxResult", "StealthyEnergy", "Trajectory", "adaptive_descent", "chi_from_count",
+        "collective_density", "cubic_box", "enumerate_kvectors", "g2_from_histogram",
+        "isotropic_structure_factor", "k_outer_from_ka", "ka_from_chi", "lbfgs",
+        "make_stealthy_energy", "nearest_neighbor_distances", "pair_distance_histogram",
+        "read_configpack", "relax", "require_float64", "stack_fractional", "structure_factor",
+        "unit_ball_volume", "wrap_fractional", "write_configpack", "write_function_table",
+    }  # fmt: skip
+    assert ref_names <= set(xla_cco.__all__)
+    for name in ref_names:
+        assert getattr(xla_cco, name) is not None

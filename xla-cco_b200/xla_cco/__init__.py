@@ -7,6 +7,12 @@ hand-written CUDA kernels of ``libcco.so`` (no CPU fallback).
 """
 
 from xla_cco._types import require_float64
+from xla_cco.analysis.pairs import (
+    g2_from_histogram,
+    nearest_neighbor_distances,
+    pair_distance_histogram,
+)
+from xla_cco.analysis.structure import isotropic_structure_factor, structure_factor
 from xla_cco.box import Box, cubic_box, wrap_fractional
 from xla_cco.energy import (
     AbstractEnergy,
@@ -14,6 +20,13 @@ from xla_cco.energy import (
     collective_density,
     make_stealthy_energy,
 )
+from xla_cco.io.configpack import (
+    PackedConfig,
+    read_configpack,
+    stack_fractional,
+    write_configpack,
+)
+from xla_cco.io.tables import write_function_table
 from xla_cco.kvectors import (
     KSet,
     chi_from_count,
@@ -33,6 +46,7 @@ __all__ = [
     "DescentSettings",
     "KSet",
     "LBFGSSettings",
+    "PackedConfig",
     "RelaxResult",
     "StealthyEnergy",
     "Trajectory",
@@ -41,13 +55,22 @@ __all__ = [
     "collective_density",
     "cubic_box",
     "enumerate_kvectors",
+    "g2_from_histogram",
+    "isotropic_structure_factor",
     "k_outer_from_ka",
     "ka_from_chi",
     "lbfgs",
     "make_stealthy_energy",
+    "nearest_neighbor_distances",
+    "pair_distance_histogram",
+    "read_configpack",
     "relax",
     "relax_mixed",
     "require_float64",
+    "stack_fractional",
+    "structure_factor",
     "unit_ball_volume",
     "wrap_fractional",
+    "write_configpack",
+    "write_function_table",
 ]
