@@ -19,7 +19,7 @@ from xla_cco import _native
 from xla_cco._types import require_float64
 from xla_cco.minimize.descent import DescentSettings
 from xla_cco.minimize.lbfgs import LBFGSSettings
-from xla_cco.minimize.result import RelaxResult, Trajectory
+from xla_cco.minimize.result import STATUS_BUDGET, STATUS_RUNNING, RelaxResult, Trajectory  # noqa: F401
 
 __all__ = ["relax", "relax_device", "relax_mixed", "relax_mixed_device", "DescentSettings",
            "LBFGSSettings"]
