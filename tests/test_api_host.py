@@ -126,3 +126,11 @@ def test_top_level_exports_cover_the_reference_package():
     assert ref_names <= set(xla_cco.__all__)
     for name in ref_names:
         assert getattr(xla_cco, name) is not None
+
+
+def test_auto_chunk_size_as_the_reference():
+    from xla_cco.energy import auto_chunk_size
+
+    assert auto_chunk_size(1000, 802) is None                     # 1000 x 802 x 96 B < 1 GiB
+    assert auto_chunk_size(20000, 27085) == (1 << 30) // (20000 * 96)
+    assert auto_chunk_size(10, 5, budget_bytes=100, bytes_per_pair=96) == 1

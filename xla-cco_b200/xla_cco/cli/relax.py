@@ -174,7 +174,7 @@ def load_input(prefix: Path, dim: int, input_basis: str = "auto"
     if d_pack != dim:
         raise ValueError(f"--dim {dim} does not match pack dimension {d_pack}")
     s0, _ = stack_fractional(configs)
-    s0 = wrap_fractional(s0)
+    s0 = wrap_fractional_batch(s0)
     n = int(s0.shape[1])
     side = float(n) ** (1.0 / dim)
     unit = []
@@ -234,7 +234,7 @@ def relax_batches(energy: Any, s0: np.ndarray, settings: Settings, batch_size: i
     parts: List[Dict[str, np.ndarray]] = []
     for lo in range(0, s0.shape[0], batch_size):
         res = relax(energy, np.ascontiguousarray(s0[lo:lo + batch_size]), settings)
-        part = {"s": wrap_fractional(np.asarray(res.s)), "energy": np.asarray(res.energy),
+        part = {"s": wrap_fractional_batch(np.asarray(res.s)), "energy": np.asarray(res.energy),
                 "n_evals": np.asarray(res.n_evals), "n_iters": np.asarray(res.n_iters),
                 "status": np.asarray(res.status)}  # fmt: skip
         if res.trajectory is not None:
@@ -242,6 +242,12 @@ def relax_batches(energy: Any, s0: np.ndarray, settings: Settings, batch_size: i
                 part[f"traj_{name}"] = np.asarray(getattr(res.trajectory, name))
         parts.append(part)
     return {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
+
+
+def wrap_fractional_batch(s: np.ndarray) -> np.ndarray:
+    """Wrap a (b, n, d) batch of fractional positions into [0, 1)."""
+    assert np.ndim(s) == 3, "s must have shape (b, n, d)"
+    return wrap_fractional(np.asarray(s))
 
 
 def pack_configs(template: Sequence[PackedConfig], s: np.ndarray, side: float

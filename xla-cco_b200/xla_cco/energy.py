@@ -248,6 +248,19 @@ class StealthyEnergy(AbstractEnergy):
         return out.cpu().numpy() if host else out
 
 
+def auto_chunk_size(n_particles: int, n_vectors: int, budget_bytes: int = 1 << 30,
+                    bytes_per_pair: int = 96) -> Optional[int]:  # fmt: skip
+    """A ``chunk_size`` whose (c, N) work arrays fit ``budget_bytes``, or None when
+    the whole (M, N) matrix fits (``energy.py:86-101``). The device kernels never
+    materialise (k, particle) arrays, so ``chunk_size`` is accepted everywhere and
+    changes nothing here; this keeps the reference's helper for callers that size
+    their own arrays with it."""
+    assert n_particles >= 1 and n_vectors >= 1, "sizes must be positive"
+    assert budget_bytes >= 1 and bytes_per_pair >= 1, "budget must be positive"
+    size = max(1, budget_bytes // (n_particles * bytes_per_pair))
+    return None if size >= n_vectors else size
+
+
 def collective_density(s: Any, n_vectors: Any, chunk_size: Optional[int] = None):
     """(Re rho, Im rho) with rho_k = sum_j exp(2 pi i n_k . s_j) (``energy.py:327-358``)."""
     require_float64(s, "s")
