@@ -134,3 +134,19 @@ def test_auto_chunk_size_as_the_reference():
     assert auto_chunk_size(1000, 802) is None                     # 1000 x 802 x 96 B < 1 GiB
     assert auto_chunk_size(20000, 27085) == (1 << 30) // (20000 * 96)
     assert auto_chunk_size(10, 5, budget_bytes=100, bytes_per_pair=96) == 1
+
+
+def test_device_guard_names_the_cause():
+    from xla_cco._device import classify_failure, require_gpu
+
+    assert classify_failure(1, {}, None) is None
+    assert "CUDA_VISIBLE_DEVICES" in classify_failure(0, {"CUDA_VISIBLE_DEVICES": ""}, None)
+    assert "no CPU path" in classify_failure(0, {}, None)
+    assert "cannot be loaded" in classify_failure(0, {}, "libcco.so not found")
+    from xla_cco import _native
+
+    if _native.device_count() == 0:
+        with pytest.raises(RuntimeError, match="CUDA|GPU"):
+            require_gpu()
+    else:
+        require_gpu()   # a visible device passes the guard
