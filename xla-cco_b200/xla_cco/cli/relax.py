@@ -40,6 +40,7 @@ from typing import Any, Dict, List, Sequence, Tuple, Union
 import numpy as np
 
 from xla_cco import _native
+from xla_cco._device import require_gpu
 from xla_cco.analysis.pairs import (
     g2_from_histogram,
     nearest_neighbor_distances,
@@ -152,7 +153,7 @@ def select_device(device: str) -> str:
     if device == "cpu":
         raise RuntimeError("requested --device cpu, but this build computes on the GPU only "
                            "(libcco.so, sm_100a); run with --device gpu")  # fmt: skip
-    _native.require_gpu()
+    require_gpu()
     return "gpu"
 
 
