@@ -785,6 +785,49 @@ def run_analysis(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ ground-state driver
+def run_cli(args) -> None:
+    """The ground-state driver end to end (``python -m xla_cco.cli.relax``) on a
+    ConfigPack of 256 seeded d=2 N=1000 configurations at chi = 0.40: read the
+    pack, relax on the GPU, write the packs, S(k), g2, Hp tables and the log."""
+    import tempfile
+
+    import torch
+
+    from xla_cco import ka_from_chi
+    from xla_cco.cli import relax as cli
+    from xla_cco.io import PackedConfig, write_configpack
+
+    torch.cuda.set_device(0)
+    b = args.batch
+    rng = np.random.default_rng(SEED)
+    names = (b"a\x00\x00\x00",) * N_PART
+    cfgs = [PackedConfig(np.eye(DIM), rng.uniform(size=(N_PART, DIM)), 1.0, names) for _ in range(b)]
+    with tempfile.TemporaryDirectory() as tmp:
+        write_configpack(Path(tmp) / "in", cfgs)
+        argv = ["--dim", str(DIM), "--ka", repr(ka_from_chi(CHI, PHI_PACK, DIM)), "--phi", str(PHI_PACK),
+                "--load", str(Path(tmp) / "in"), "--save", str(Path(tmp) / "out"), "--batch-size", str(b)]
+        for _ in range(args.warmup):
+            cli.run(cli.build_parser().parse_args(argv))
+        walls, logs = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            logs.append(cli.run(cli.build_parser().parse_args(argv)))
+            walls.append(time.perf_counter() - t0)
+    wall = float(np.median(walls))
+    log = logs[-1]
+    line = {
+        "metric": "ground-state driver: configurations/s end to end (read, relax, write, S(k), g2, Hp)",
+        "value": b / wall, "unit": "configs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"cli_relax_d{DIM}_n{N_PART}_chi{CHI}_b{b}", "M": log["M"],
+                   "n_success": log["n_success"], "stage_seconds": log["wall_seconds"],
+                   "timing": "host wall clock around cli.run, median over steps"},
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def run_profile(args) -> None:
     """Kernel-level profiling driver (run under ncu): no timing, no JSON."""
     import torch
@@ -818,7 +861,7 @@ def main() -> None:
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--md-lanes", type=int, default=64)
     ap.add_argument("--md-steps", type=int, default=2000)
-    ap.add_argument("--workload", choices=["batch", "mixed", "serve", "precision", "md", "analysis"],
+    ap.add_argument("--workload", choices=["batch", "mixed", "serve", "precision", "md", "analysis", "cli"],
                     default="batch",
                     help="batch: the headline 256-lane d2 N1000 relax; mixed: the 512-instance "
                          "mixed-size ensemble; serve: a Poisson request stream")  # fmt: skip
@@ -843,6 +886,8 @@ def main() -> None:
         run_md(args)
     elif args.workload == "analysis" and args.impl == "cco":
         run_analysis(args)
+    elif args.workload == "cli" and args.impl == "cco":
+        run_cli(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
