@@ -38,12 +38,6 @@ UNIT = "relaxations/s"
 N_PART, DIM, CHI, PHI_PACK, BATCH, SEED = 1000, 2, 0.40, 0.05, 256, 0
 TOL = 1e-20
 F_PAIR = {1: 7, 2: 21, 3: 35}  # algorithmic FP64 flops per (k, particle) pair and evaluation
-# Mean energy+force evaluations per relaxation of this workload (reference
-# counting: line-search probes + 1), measured by the device arm on seeds
-# 0..255 with the same algorithm; converts the CPU arm's evals/s into
-# relaxations/s. Refreshed from the device arm's "evals_per_relax"
-# (first B200 run: 433.1 evaluations per relaxation, 256/256 lanes < 1e-20).
-EVALS_PER_RELAX = 433.1
 
 
 def workload():
@@ -54,10 +48,22 @@ def workload():
     return box, ks, make_stealthy_energy(box, ks)
 
 
-def config_dict(ks, extra=None):
+def oracle_inputs():
+    """(basis, volume, k-set n) of the headline workload built by the oracle
+    alone: its own cutoff formula and brute-force half-space scan in the
+    reference's order (the same rows, bit for bit, as the product's
+    enumeration). The CPU arms import nothing from the product package."""
+    import oracle
+
+    basis = float(N_PART) ** (1.0 / DIM) * np.eye(DIM)
+    n = oracle.sorted_kset(basis, 0.0, oracle.k_outer_for_chi(CHI, PHI_PACK, DIM))
+    return basis, float(abs(np.linalg.det(basis))), n
+
+
+def config_dict(m: int, extra=None):
     c = {
-        "workload": f"lbfgs_relax_d{DIM}_n{N_PART}_chi{CHI}_m{ks.n.shape[0]}_b{BATCH}",
-        "d": DIM, "n_particles": N_PART, "chi": CHI, "m_kvectors": int(ks.n.shape[0]),
+        "workload": f"lbfgs_relax_d{DIM}_n{N_PART}_chi{CHI}_m{m}_b{BATCH}",
+        "d": DIM, "n_particles": N_PART, "chi": CHI, "m_kvectors": int(m),
         "batch": BATCH, "energy_tol": TOL, "minimizer": "L-BFGS m=100, rescales 1e4/1/1e-2",
         "seeds": "default_rng(seed + rank).uniform((B, N, d))",
         "l2": "inputs larger than L2: history 2*100*N*d*8 B per lane = 0.8 GB per step",
@@ -131,52 +137,79 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ CPU arm
-def cpu_sample(s0: np.ndarray, ks, box, evals_per_relax: float | None, budget: int = 200):
-    """Time the oracle L-BFGS on all host threads; returns the cpu_baseline dict."""
+def cpu_relax(s0: np.ndarray, lanes, threads: int) -> tuple[int, int, float]:
+    """Relax the given lanes of s0 to completion with the oracle L-BFGS (the
+    reference's three-pass schedule, energy_tol 1e-20), one lane after another,
+    each evaluation spread over `threads` host threads. Returns (successes,
+    evaluations, wall seconds)."""
     import oracle
-    from xla_cco import LBFGSSettings
+
+    basis, vol, n = oracle_inputs()
+    st = oracle.lbfgs_settings(energy_tol=TOL)
+    lanes = list(lanes)
+    t0 = time.perf_counter()
+    out = oracle.relax_lanes("lbfgs", s0[lanes], n, np.ones(n.shape[0]), vol, st, threads=threads)
+    dt = time.perf_counter() - t0
+    return int((out["energy"] < TOL).sum()), int(out["n_evals"].sum()), dt
+
+
+def cpu_sample(s0: np.ndarray, min_seconds: float = 10.0, max_lanes: int = 16) -> dict:
+    """cpu_baseline: the oracle relaxes lanes 0, 1, ... of the same seeded
+    batch to Phi < 1e-20 on all host threads until `min_seconds` have passed
+    (at most `max_lanes`); value = completed relaxations / wall time."""
+    import oracle
 
     threads = oracle.max_threads()
-    lanes = min(threads, s0.shape[0])
-    cfg = LBFGSSettings(energy_tol=TOL, rescales=(1e4,), max_evals_per_pass=budget)
-    t0 = time.perf_counter()
-    out = oracle.relax_batch("lbfgs", s0[:lanes], ks.n, ks.weights, box.volume, cfg, threads=threads)
-    dt = time.perf_counter() - t0
-    evals = int(out["n_evals"].sum())
-    eps = evals / dt
-    value = eps / evals_per_relax if evals_per_relax else None
+    succ = evals = 0
+    wall = 0.0
+    lane = 0
+    while lane < min(max_lanes, s0.shape[0]) and (lane == 0 or wall < min_seconds):
+        s, e, dt = cpu_relax(s0, [lane], threads)
+        succ, evals, wall, lane = succ + s, evals + e, wall + dt, lane + 1
     return {
-        "value": value, "unit": UNIT, "cores": threads, "kind": "port",
-        "evals_per_s": eps,
-        "sample": (f"C oracle L-BFGS (OpenMP, {threads} threads) on {lanes} of the seeded "
-                   f"configurations, {budget}-evaluation budget each ({evals} energy+force "
-                   f"evaluations in {dt:.1f} s); relaxations/s = evals/s / "
-                   f"{evals_per_relax} evaluations per relaxation of this workload"),
+        "value": succ / wall, "unit": UNIT, "cores": threads, "kind": "port",
+        "evals_per_s": evals / wall,
+        "sample": (f"C oracle (direct-sum FP64 energy, L-BFGS three-pass schedule) relaxing lanes "
+                   f"0..{lane - 1} of the seeded batch to Phi<1e-20, one after another, each "
+                   f"evaluation on {threads} host threads: {succ}/{lane} relaxed, {evals} "
+                   f"evaluations in {wall:.1f} s"),
     }  # fmt: skip
 
 
 def run_reference(args) -> None:
+    """The reference arm: the CPU restatement of the reference's path (the
+    oracle; the reference's JAX package cannot be installed here) relaxing
+    lanes of the same seeded batch to Phi < 1e-20. Step i relaxes lane i to
+    completion on every host thread; value = completed relaxations / wall
+    time of the timed steps. Imports nothing from the product package."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import oracle  # noqa: F401
+    import oracle
 
-    box, ks, _ = workload()
+    threads = oracle.max_threads()
+    _, _, n = oracle_inputs()
     s0 = np.random.default_rng(SEED).uniform(size=(BATCH, N_PART, DIM))
-    for _ in range(args.warmup):
-        cpu_sample(s0, ks, box, EVALS_PER_RELAX, budget=args.ref_budget)
-    vals, cb = [], None
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        cb = cpu_sample(s0, ks, box, EVALS_PER_RELAX, budget=args.ref_budget)
-        vals.append(cb["value"] if cb["value"] is not None else float("nan"))
-    wall = time.perf_counter() - t0
-    value = float(np.mean(vals))
+    for i in range(args.warmup):
+        cpu_relax(s0, [i % BATCH], threads)
+    succ = evals = 0
+    wall = 0.0
+    first = args.warmup % BATCH
+    for i in range(args.steps):
+        s, e, dt = cpu_relax(s0, [(args.warmup + i) % BATCH], threads)
+        succ, evals, wall = succ + s, evals + e, wall + dt
+    value = succ / wall
+    cb = {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+          "evals_per_s": evals / wall,
+          "sample": (f"C oracle relaxing lanes {first}..{(first + args.steps - 1) % BATCH} of the "
+                     f"seeded batch to Phi<1e-20 (one lane per step, each evaluation on {threads} "
+                     f"host threads): {succ}/{args.steps} relaxed, {evals} evaluations in "
+                     f"{wall:.1f} s")}  # fmt: skip
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": config_dict(ks),
+        "data": "synthetic", "config": config_dict(n.shape[0]),
         "cpu_baseline": cb,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }  # fmt: skip
@@ -314,12 +347,12 @@ def run_device(args) -> None:
     epr = float(evals.mean())
     cb = None
     if not args.no_cpu_baseline:
-        cb = cpu_sample(s0, ks, box, epr)
+        cb = cpu_sample(s0)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_dict(ks, {
+        "config": config_dict(int(ks.n.shape[0]), {
             "parallelism": f"replicas x{world}",
             "success": f"{succ}/{args.batch * args.steps * world}",
             "p50_latency_ms": float(np.percentile(lat, 50)),
@@ -467,6 +500,88 @@ def run_mixed(args) -> None:
                      "algorithmic": "sum over lanes of evals x N M x flop/pair(d)"},  # fmt: skip
         "clocks": clocks,
         "gpu_launches": sum(o["launches"] for o in outs),
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ descent (d3 N100)
+DESCENT_TOL = 9.99999968e-21
+
+
+def run_descent(args) -> None:
+    """The reference README's relax call at the ground-state driver's default
+    tolerance: d=3, N=100, chi=0.05 (M=13), batch 5 from seed 0,
+    DescentSettings(grow=2.0, max_evals=200_000, energy_tol=9.99999968e-21).
+    One step relaxes the 5 configurations; the oracle relaxes the same 5 on
+    all host threads as the CPU baseline."""
+    import oracle
+    import torch
+
+    from xla_cco import DescentSettings, cubic_box, enumerate_kvectors, k_outer_from_ka, ka_from_chi
+    from xla_cco import make_stealthy_energy, relax
+    from xla_cco.minimize import relax_device
+
+    torch.cuda.set_device(0)
+    n, d, chi, b = 100, 3, 0.05, 5
+    box = cubic_box(n, d)
+    ks = enumerate_kvectors(box.basis, 0.0, k_outer_from_ka(ka_from_chi(chi, PHI_PACK, d), PHI_PACK, d))
+    en = make_stealthy_energy(box, ks)
+    st = DescentSettings(grow=2.0, max_evals=200_000, energy_tol=DESCENT_TOL)
+    s0 = np.random.default_rng(SEED).uniform(size=(b, n, d))
+    s_dev = torch.from_numpy(s0).cuda()
+    for _ in range(args.warmup):
+        relax_device(en, s_dev, st)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    outs = [relax_device(en, s_dev, st) for _ in range(args.steps)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    succ = sum(int((o["energy"] < DESCENT_TOL).sum().item()) for o in outs)
+    iters = outs[-1]["n_iters"].cpu().numpy()
+    lat = np.concatenate([o["latency_ns"].cpu().numpy() for o in outs]) / 1e6
+    # end to end: host arrays in, host arrays out
+    pinned = torch.from_numpy(s0).pin_memory()
+    t0 = time.perf_counter()
+    e2e_succ = 0
+    for _ in range(args.steps):
+        e2e_succ += int((relax(en, pinned, st).energy < DESCENT_TOL).sum())
+    e2e_s = time.perf_counter() - t0
+    cb = None
+    if not args.no_cpu_baseline:
+        threads = oracle.max_threads()
+        reps, c_succ, wall = 0, 0, 0.0
+        while reps == 0 or wall < 10.0:
+            t0 = time.perf_counter()
+            out = oracle.relax_batch("descent", s0, ks.n, ks.weights, box.volume, st, threads=threads)
+            wall += time.perf_counter() - t0
+            c_succ += int((out["energy"] < DESCENT_TOL).sum())
+            reps += 1
+        cb = {"value": c_succ / wall, "unit": UNIT, "cores": min(threads, b), "kind": "port",
+              "sample": (f"C oracle descent on the same 5 configurations (one host thread per "
+                         f"lane), {reps} repetitions: {c_succ}/{5 * reps} relaxed in {wall:.1f} s")}
+    launches = sum(o["launches"] for o in outs)
+    line = {
+        "metric": "relaxations/s to Phi<9.99999968e-21 (batched adaptive descent, plain FP64)",
+        "value": succ / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"descent_relax_d{d}_n{n}_chi{chi}_m{ks.n.shape[0]}_b{b}",
+                   "settings": "DescentSettings(grow=2.0, max_evals=200000, energy_tol=9.99999968e-21)",
+                   "success": f"{succ}/{b * args.steps}", "n_iters": iters.tolist(),
+                   "p50_latency_ms": float(np.percentile(lat, 50)),
+                   "p99_latency_ms": float(np.percentile(lat, 99)),
+                   "l2": "latency-bound: 5 lanes of 1300 (k, particle) pairs"},
+        "cpu_baseline": cb,
+        "e2e": {"value": e2e_succ / e2e_s, "unit": UNIT, "h2d_bytes_per_step": s0.nbytes,
+                "d2h_bytes_per_step": s0.nbytes + b * 8 * 5,
+                "timing": "host wall clock around relax(numpy->numpy)"},
+        "clocks": clocks, "gpu_launches": launches,
     }  # fmt: skip
     print(json.dumps(line), flush=True)
 
@@ -854,14 +969,14 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cco", "reference"], default="cco")
     ap.add_argument("--batch", type=int, default=BATCH)
-    ap.add_argument("--ref-budget", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", choices=["eval", "relax"], default=None,
                     help="profiling driver for ncu: run the kernels only")  # fmt: skip
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--md-lanes", type=int, default=64)
     ap.add_argument("--md-steps", type=int, default=2000)
-    ap.add_argument("--workload", choices=["batch", "mixed", "serve", "precision", "md", "analysis", "cli"],
+    ap.add_argument("--workload", choices=["batch", "descent", "mixed", "serve", "precision", "md", "analysis",
+                                           "cli"],
                     default="batch",
                     help="batch: the headline 256-lane d2 N1000 relax; mixed: the 512-instance "
                          "mixed-size ensemble; serve: a Poisson request stream")  # fmt: skip
@@ -876,6 +991,8 @@ def main() -> None:
     args = ap.parse_args()
     if args.profile:
         run_profile(args)
+    elif args.workload == "descent" and args.impl == "cco":
+        run_descent(args)
     elif args.workload == "mixed" and args.impl == "cco":
         run_mixed(args)
     elif args.workload == "serve" and args.impl == "cco":

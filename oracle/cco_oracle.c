@@ -57,11 +57,20 @@ typedef struct {
 
 /* ------------------------------------------------------------------ energy */
 
+/* Threads that one evaluation may use (oracle_relax_lanes sets it; 1 = the
+ * plain serial loops). Rows and particles are split between the threads, and
+ * every sum keeps its serial order, so the bits do not depend on it. */
+static int g_inner_threads = 1;
+
 /* Phi, dPhi/ds and rho of one configuration; grad/re/im may be NULL. */
 double oracle_energy_grad(int N, int d, const double* s, int M, const double* n,
                           const double* w, double V, double* grad, double* re, double* im) {
   double* rr = (double*)malloc(sizeof(double) * 2 * (size_t)M);
-  double total = 0.0;
+  const int inner = g_inner_threads;
+  (void)inner;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(inner) if (inner > 1)
+#endif
   for (int k = 0; k < M; ++k) {
     double a = 0.0, b = 0.0;
     for (int j = 0; j < N; ++j) {
@@ -73,6 +82,10 @@ double oracle_energy_grad(int N, int d, const double* s, int M, const double* n,
     }
     rr[2 * k] = a;
     rr[2 * k + 1] = b;
+  }
+  double total = 0.0;
+  for (int k = 0; k < M; ++k) {
+    const double a = rr[2 * k], b = rr[2 * k + 1];
     total += w[k] * (a * a + b * b);
     if (re) re[k] = a;
     if (im) im[k] = b;
@@ -80,6 +93,9 @@ double oracle_energy_grad(int N, int d, const double* s, int M, const double* n,
   const double phi = total / V;
   if (grad) {
     const double pref = 2.0 * TWO_PI / V;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(inner) if (inner > 1)
+#endif
     for (int j = 0; j < N; ++j) {
       double acc[3] = {0.0, 0.0, 0.0};
       for (int k = 0; k < M; ++k) {
@@ -94,6 +110,99 @@ double oracle_energy_grad(int N, int d, const double* s, int M, const double* n,
   }
   free(rr);
   return phi;
+}
+
+/* ------------------------------------------------------ accurate energy
+ * A higher-accuracy restatement of the same sums, used only to measure the
+ * device kernels' own error. The FP64 trig path above rounds the phase
+ * argument 2 pi (n . s): for |n . s| ~ 10^3 that alone is ~1e-13 rad per
+ * term. Here n . s is formed from error-free products (fma) and compensated
+ * two-sums, its nearest integer removed exactly, and only the reduced
+ * fraction r in [-1/2, 1/2] is scaled by 2 pi; the density, energy and
+ * gradient sums are compensated (Neumaier). */
+static void exact_phase(const double* nk, const double* sj, int d, double* c, double* s) {
+  double hi = 0.0, lo = 0.0;
+  for (int a = 0; a < d; ++a) {
+    const double p = nk[a] * sj[a];
+    const double e = fma(nk[a], sj[a], -p); /* p + e == n_a s_a exactly */
+    const double t = hi + p;
+    const double z = t - hi;
+    lo += ((hi - (t - z)) + (p - z)) + e;
+    hi = t;
+  }
+  const double r = (hi - nearbyint(hi)) + lo;
+  *c = cos(TWO_PI * r);
+  *s = sin(TWO_PI * r);
+}
+
+typedef struct { double s, c; } nsum;
+static inline void nadd(nsum* a, double x) {
+  const double t = a->s + x;
+  if (fabs(a->s) >= fabs(x)) a->c += (a->s - t) + x; else a->c += (x - t) + a->s;
+  a->s = t;
+}
+
+double oracle_energy_grad_accurate(int N, int d, const double* s, int M, const double* n,
+                                   const double* w, double V, double* grad, double* re,
+                                   double* im) {
+  double* rr = (double*)malloc(sizeof(double) * 2 * (size_t)M);
+  const int inner = g_inner_threads;
+  (void)inner;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(inner) if (inner > 1)
+#endif
+  for (int k = 0; k < M; ++k) {
+    nsum a = {0.0, 0.0}, b = {0.0, 0.0};
+    for (int j = 0; j < N; ++j) {
+      double c, sn;
+      exact_phase(n + (size_t)k * d, s + (size_t)j * d, d, &c, &sn);
+      nadd(&a, c);
+      nadd(&b, sn);
+    }
+    rr[2 * k] = a.s + a.c;
+    rr[2 * k + 1] = b.s + b.c;
+  }
+  nsum total = {0.0, 0.0};
+  for (int k = 0; k < M; ++k) {
+    const double a = rr[2 * k], b = rr[2 * k + 1];
+    nadd(&total, w[k] * a * a);
+    nadd(&total, w[k] * b * b);
+    if (re) re[k] = a;
+    if (im) im[k] = b;
+  }
+  const double phi = (total.s + total.c) / V;
+  if (grad) {
+    const double pref = 2.0 * TWO_PI / V;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(inner) if (inner > 1)
+#endif
+    for (int j = 0; j < N; ++j) {
+      nsum acc[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+      for (int k = 0; k < M; ++k) {
+        double c, sn;
+        exact_phase(n + (size_t)k * d, s + (size_t)j * d, d, &c, &sn);
+        const double coef = w[k] * (rr[2 * k + 1] * c - rr[2 * k] * sn);
+        for (int a = 0; a < d; ++a) nadd(&acc[a], coef * n[(size_t)k * d + a]);
+      }
+      for (int a = 0; a < d; ++a) grad[(size_t)j * d + a] = pref * (acc[a].s + acc[a].c);
+    }
+  }
+  free(rr);
+  return phi;
+}
+
+/* Batched accurate evaluations, `threads` threads inside each one. */
+void oracle_energy_grad_accurate_batch(int B, int N, int d, const double* s, int M,
+                                       const double* n, const double* w, double V, double* phi,
+                                       double* grad, double* re, double* im, int threads) {
+  g_inner_threads = threads > 1 ? threads : 1;
+  for (int b = 0; b < B; ++b) {
+    const size_t off = (size_t)b * N * d;
+    phi[b] = oracle_energy_grad_accurate(N, d, s + off, M, n, w, V, grad ? grad + off : NULL,
+                                         re ? re + (size_t)b * M : NULL,
+                                         im ? im + (size_t)b * M : NULL);
+  }
+  g_inner_threads = 1;
 }
 
 /* Batched energies/gradients, OpenMP over configurations. */
@@ -454,6 +563,28 @@ void oracle_relax_batch(int method, int B, int N, int d, const double* s0, int M
       oracle_lbfgs(N, d, s0 + o, M, n, w, V, (const ol_settings*)settings, s_out + o, f_out + b,
                    gn_out + b, ne + b, ni + b, status + b, NULL, NULL, NULL, NULL, NULL);
   }
+}
+
+/* The same relaxations one lane after another, each evaluation spread over
+ * `threads` threads (rows of the density pass, particles of the gradient
+ * pass). Results are bit-identical to oracle_relax_batch; this form lets a
+ * short sample of a batch use every host thread. */
+void oracle_relax_lanes(int method, int B, int N, int d, const double* s0, int M,
+                        const double* n, const double* w, double V, const void* settings,
+                        double* s_out, double* f_out, double* gn_out, int64_t* ne, int64_t* ni,
+                        int64_t* status, int threads) {
+  const size_t nd = (size_t)N * d;
+  g_inner_threads = threads > 1 ? threads : 1;
+  for (int b = 0; b < B; ++b) {
+    const size_t o = (size_t)b * nd;
+    if (method == 0)
+      oracle_descent(N, d, s0 + o, M, n, w, V, (const od_settings*)settings, s_out + o, f_out + b,
+                     gn_out + b, ne + b, ni + b, status + b, NULL, NULL, NULL, NULL, NULL);
+    else
+      oracle_lbfgs(N, d, s0 + o, M, n, w, V, (const ol_settings*)settings, s_out + o, f_out + b,
+                   gn_out + b, ne + b, ni + b, status + b, NULL, NULL, NULL, NULL, NULL);
+  }
+  g_inner_threads = 1;
 }
 
 int oracle_max_threads(void) {

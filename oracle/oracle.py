@@ -129,6 +129,40 @@ def energy_grad_batch(s: np.ndarray, n: np.ndarray, w: np.ndarray, volume: float
     return phi, g
 
 
+def lbfgs_settings(**overrides):
+    """Settings object with the reference's LBFGSSettings fields and defaults
+    (src/xla_cco/minimize/lbfgs.py:55-67), for callers that must not import
+    the product package."""
+    import types
+
+    base = dict(memory=100, rescales=(1e4, 1.0, 1e-2), max_evals_per_pass=500_000,
+                energy_tol=0.0, grad_tol=0.0, stagnation_patience=50, max_linesearch_steps=30,
+                record_every=0, max_records=0)  # fmt: skip
+    base.update(overrides)
+    return types.SimpleNamespace(**base)
+
+
+def energy_grad_accurate(s: np.ndarray, n: np.ndarray, w: np.ndarray, volume: float,
+                         want_rho: bool = False, threads: int = 0):  # fmt: skip
+    """(Phi, dPhi/ds[, re, im]) of a batch (B, N, d) with the phase argument
+    reduced exactly and compensated sums (cco_oracle.c): a higher-accuracy
+    reference than the FP64 trig path, for measuring the kernels' own error."""
+    s = np.ascontiguousarray(s, dtype=np.float64)
+    n = np.ascontiguousarray(n, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    B, N, d = s.shape
+    M = n.shape[0]
+    phi, g = np.zeros(B), np.zeros_like(s)
+    re = np.zeros((B, M)) if want_rho else None
+    im = np.zeros((B, M)) if want_rho else None
+    lib().oracle_energy_grad_accurate_batch(
+        ctypes.c_int(B), ctypes.c_int(N), ctypes.c_int(d), _p(s), ctypes.c_int(M), _p(n), _p(w),
+        ctypes.c_double(volume), _p(phi), _p(g), _p(re), _p(im),
+        ctypes.c_int(threads or max_threads()),
+    )  # fmt: skip
+    return (phi, g, re, im) if want_rho else (phi, g)
+
+
 def _descent_c(st) -> DescentC:
     return DescentC(st.step_init, st.step_min, st.shrink, st.grow, st.rel_tol, st.max_evals,
                     st.energy_tol, st.record_every, st.max_records)  # fmt: skip
@@ -203,8 +237,52 @@ def relax_batch(method: str, s0: np.ndarray, n: np.ndarray, w: np.ndarray, volum
     return out
 
 
+def relax_lanes(method: str, s0: np.ndarray, n: np.ndarray, w: np.ndarray, volume: float,
+                settings, threads: int = 0) -> dict:  # fmt: skip
+    """The lanes of ``relax_batch`` one after another, each evaluation spread
+    over ``threads`` host threads (same bits as ``relax_batch``)."""
+    s0 = np.ascontiguousarray(s0, dtype=np.float64)
+    n = np.ascontiguousarray(n, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    B, N, d = s0.shape
+    out = dict(s=np.zeros_like(s0), energy=np.zeros(B), grad_norm=np.zeros(B),
+               n_evals=np.zeros(B, np.int64), n_iters=np.zeros(B, np.int64),
+               status=np.zeros(B, np.int64))  # fmt: skip
+    c = _descent_c(settings) if method == "descent" else _lbfgs_c(settings)
+    lib().oracle_relax_lanes(
+        ctypes.c_int(0 if method == "descent" else 1), ctypes.c_int(B), ctypes.c_int(N),
+        ctypes.c_int(d), _p(s0), ctypes.c_int(n.shape[0]), _p(n), _p(w), ctypes.c_double(volume),
+        ctypes.byref(c), _p(out["s"]), _p(out["energy"]), _p(out["grad_norm"]),
+        _p(out["n_evals"]), _p(out["n_iters"]), _p(out["status"]),
+        ctypes.c_int(threads or max_threads()),
+    )  # fmt: skip
+    return out
+
+
 def max_threads() -> int:
     return int(lib().oracle_max_threads())
+
+
+# ------------------------------------------------------------ cutoffs and k-sets
+# Unit-ball volumes for d <= 3 as the C++ engine hard-codes them
+# (src/xla_cco/kvectors.py:131-149 keeps those literals).
+_UNIT_BALL = {1: 2.0, 2: math.pi, 3: 4.1887902047863909846}
+
+
+def k_outer_for_chi(chi: float, phi: float, dim: int) -> float:
+    """K2 for a target chi (src/xla_cco/kvectors.py:152-163 restated):
+    Ka = (2^(d+1) d chi Gamma(d/2+1)^2 phi)^(1/d), a = (phi / V_d)^(1/d), K2 = Ka / a."""
+    ka = (2.0 ** (dim + 1) * dim * chi * math.gamma(dim / 2.0 + 1.0) ** 2 * phi) ** (1.0 / dim)
+    a = (phi / _UNIT_BALL[dim]) ** (1.0 / dim)
+    return ka / a
+
+
+def sorted_kset(basis: np.ndarray, k_inner: float, k_outer: float) -> np.ndarray:
+    """The brute-force half-space scan ordered as the reference orders its
+    k-set (src/xla_cco/kvectors.py:91-93): by |k|^2, then n_0, n_1, ..."""
+    n, ksq = halfspace_kvectors(basis, k_inner, k_outer)
+    keys = tuple(n[:, i] for i in range(n.shape[1] - 1, -1, -1)) + (ksq,)
+    return n[np.lexsort(keys)]
 
 
 # ------------------------------------------------------------ pure Python
@@ -250,6 +328,27 @@ def energy_direct(s: np.ndarray, n: np.ndarray, w: np.ndarray, volume: float):
     coef = w[:, None] * (im[:, None] * c - re[:, None] * si)  # (M, N)
     grad = (2.0 * 2.0 * math.pi / volume) * (coef.T @ n.astype(np.float64))
     return phi, grad
+
+
+def hessian_direct(s: np.ndarray, n: np.ndarray, w: np.ndarray, volume: float) -> np.ndarray:
+    """Closed-form Hessian (N d, N d) of one configuration by NumPy direct sums
+    (src/xla_cco/energy.py:272-299 restated):
+    d2 Phi / ds_ja ds_lb = (2 (2 pi)^2 / V) sum_k w_k n_ka n_kb
+    [cos th_kj cos th_kl + sin th_kj sin th_kl - delta_jl (Re rho_k cos th_kj + Im rho_k sin th_kj)].
+    Small cases only (forms (N, M) matrices)."""
+    nf = np.asarray(n, dtype=np.float64)
+    N, d = s.shape
+    theta = 2.0 * math.pi * (s @ nf.T)          # (N, M)
+    c, si = np.cos(theta), np.sin(theta)
+    re, im = c.sum(0), si.sum(0)
+    pref = 2.0 * (2.0 * math.pi) ** 2 / volume
+    out = np.zeros((N, d, N, d))
+    for a in range(d):
+        for b in range(d):
+            q = w * nf[:, a] * nf[:, b]
+            pair = (c * q) @ c.T + (si * q) @ si.T
+            out[:, a, :, b] = pref * (pair - np.diag((re * c + im * si) @ q))
+    return out.reshape(N * d, N * d)
 
 
 # ------------------------------------------------------------------ gradient flow

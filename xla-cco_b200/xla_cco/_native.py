@@ -194,6 +194,7 @@ SIGNATURES = {
     "cco_energy_grad": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
     "cco_energy_grad_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
     "cco_energy_grad_fp32": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
+    "cco_hessian": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp]),
     "cco_relax_descent": (
         ctypes.c_int,
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(DescentSettingsC), ctypes.c_int,
@@ -275,6 +276,11 @@ def load() -> ctypes.CDLL:
             fn.argtypes = args
         _lib = lib
         return lib
+
+
+def loaded():
+    """The library if an earlier call loaded it, else None (never loads it)."""
+    return _lib
 
 
 class CcoError(RuntimeError):
