@@ -1,7 +1,7 @@
 """Parity of the two forms of the FP64 density pass: the complex-GEMM form
 (dense k-sets, d = 2 and d = 3) and the per-segment form (the same problem
 built with CCO_PASS1_GEMM=0), each against the C oracle's direct sums
-(energy 1e-12 relative, forces 1e-10 of max |F|), batch sizes that leave
+(energy 1e-12 relative, forces 1e-12 of max |F| against the accurate oracle), batch sizes that leave
 ragged particle tiles and ragged run groups."""
 
 from __future__ import annotations
@@ -51,8 +51,7 @@ def test_gemm_and_segment_forms_vs_oracle(monkeypatch, d, n, chi, b):
         assert (blocks > 0) == (form == "gemm"), (form, blocks)
         phi, g, _, _ = en.evaluate(s)
         phis[form], grads[form] = phi, g
-    e_ref, g_ref = oracle.energy_grad_batch(s, ks.n.astype(np.int64), np.ones(ks.n.shape[0]), float(n),
-                                            threads=oracle.max_threads())  # fmt: skip
+    e_ref, g_ref = oracle.energy_grad_accurate(s, ks.n.astype(np.int64), np.ones(ks.n.shape[0]), float(n))
     for form in ("gemm", "segment"):
         np.testing.assert_allclose(phis[form], e_ref, rtol=RTOL_KERNEL_E, atol=0)
         for i in range(b):
@@ -78,8 +77,7 @@ def test_gemm_form_on_a_sheared_box():
     assert _gemm_blocks(en, n) > 0
     s = np.random.default_rng(31).uniform(size=(3, n, d))
     phi, g, _, _ = en.evaluate(s)
-    e_ref, g_ref = oracle.energy_grad_batch(s, ks.n.astype(np.int64), np.ones(ks.n.shape[0]), box.volume,
-                                            threads=oracle.max_threads())  # fmt: skip
+    e_ref, g_ref = oracle.energy_grad_accurate(s, ks.n.astype(np.int64), np.ones(ks.n.shape[0]), box.volume)
     np.testing.assert_allclose(phi, e_ref, rtol=RTOL_KERNEL_E, atol=0)
     for i in range(3):
         np.testing.assert_allclose(g[i], g_ref[i], rtol=0, atol=RTOL_KERNEL_F * np.abs(g_ref[i]).max())

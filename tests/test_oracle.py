@@ -34,6 +34,11 @@ def test_oracle_energy_forces_vs_reference_oracle(golden):
         phi2, g2 = oracle.energy_direct(s, n, np.ones(n.shape[0]), c["volume"])
         np.testing.assert_allclose(phi2, c["phi"], rtol=RTOL_KERNEL_E)
         np.testing.assert_allclose(g2, g, rtol=1e-10, atol=1e-10 * np.abs(g).max())
+        # the accurate mode (exact phase reduction, compensated sums) against the same pins
+        pa, ga = oracle.energy_grad_accurate(s[None], n, np.ones(n.shape[0]), c["volume"])
+        np.testing.assert_allclose(pa[0], c["phi"], rtol=RTOL_KERNEL_E)
+        fa = Box(basis).cartesian_forces(ga[0])
+        np.testing.assert_allclose(fa, ref, rtol=0, atol=RTOL_KERNEL_F * np.abs(ref).max())
 
 
 def test_oracle_matches_cpp_golden_energies(golden):
@@ -91,3 +96,26 @@ def test_oracle_lbfgs_reaches_ground_state():
     assert r["energy"] < 1e-20 and r["status"] == 1
     phi, _ = oracle.energy_grad(r["s"], ks.n, ks.weights, box.volume)
     assert phi < 1e-19
+
+
+def test_oracle_hessian_vs_central_differences():
+    """The oracle's closed-form Hessian restatement against central differences
+    of its own gradient (small box)."""
+    rng = np.random.default_rng(4)
+    n_pts, d = 12, 2
+    basis = np.sqrt(n_pts) * np.eye(2)
+    nv, _ = oracle.halfspace_kvectors(basis, 0.0, 4.0)
+    w = np.ones(nv.shape[0])
+    s = rng.uniform(size=(n_pts, d))
+    h = oracle.hessian_direct(s, nv, w, float(n_pts))
+    eps = 1e-6
+    fd = np.zeros_like(h)
+    for i in range(s.size):
+        dp, dm = s.ravel().copy(), s.ravel().copy()
+        dp[i] += eps
+        dm[i] -= eps
+        _, gp = oracle.energy_grad(dp.reshape(n_pts, d), nv, w, float(n_pts))
+        _, gm = oracle.energy_grad(dm.reshape(n_pts, d), nv, w, float(n_pts))
+        fd[:, i] = ((gp - gm) / (2 * eps)).ravel()
+    np.testing.assert_allclose(h, fd, rtol=0, atol=1e-6 * np.abs(h).max())
+    np.testing.assert_allclose(h, h.T, rtol=0, atol=1e-12 * np.abs(h).max())

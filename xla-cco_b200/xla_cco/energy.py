@@ -4,7 +4,7 @@ Drop-in for ``xla_cco/energy.py``: ``make_stealthy_energy(box, kset,
 chunk_size=None, pad_to=64)`` returns a ``StealthyEnergy`` whose ``__call__``,
 ``value_and_grad`` and ``value_grad_density`` have the reference's signatures,
 error behaviour and results (energy within 1e-12 relative, forces within
-1e-10 of the FP64 direct sum):
+1e-12 of max|F| of an exactly reduced FP64 direct sum):
 
     Phi = (1/V) sum_k w_k |rho_k|^2,   rho_k = sum_j exp(2 pi i n_k . s_j)
     dPhi/ds_j = (2 (2 pi) / V) sum_k w_k (Im rho_k cos th_kj - Re rho_k sin th_kj) n_k
@@ -29,8 +29,6 @@ from xla_cco import _native
 from xla_cco._types import require_float64
 from xla_cco.box import Box
 from xla_cco.kvectors import KSet
-
-_TWO_PI = 2.0 * np.pi
 
 
 def _torch():
@@ -82,8 +80,14 @@ class _Problems:
             return self._handles[key]
 
     def __del__(self) -> None:
+        # Handles exist only if the library was loaded to create them; an
+        # energy that never reached the device must not map libcco.so here.
+        if not self._handles:
+            return
+        lib = _native.loaded()
+        if lib is None:
+            return
         try:
-            lib = _native.load()
             for h in self._handles.values():
                 lib.cco_problem_destroy(h)
         except Exception:
@@ -219,32 +223,35 @@ class StealthyEnergy(AbstractEnergy):
         return phi[0], grad[0], re[0], im[0]
 
     def hessian(self, s: Any) -> Any:
-        """Closed-form Hessian d^2 Phi / ds_ja ds_lb flattened to (N d, N d).
-
-        ``energy.py:272-299``: two (N, M) x (M, N) float64 products per axis
-        pair, evaluated on the GPU (cuBLAS DGEMM through torch).
+        """Closed-form Hessian d^2 Phi / ds_ja ds_lb flattened to (N d, N d)
+        (``energy.py:272-299``), by the ``cco_hessian`` kernels: phases of
+        each k-chunk formed in shared memory per particle-tile pair, no
+        (N, M) arrays. ``s`` is (N, d), or (B, N, d) for a batch of Hessians
+        (B, N d, N d); NumPy in, NumPy out, CUDA tensors stay on the device.
         """
         torch = _torch()
         require_float64(s, "s")
-        assert s.ndim == 2, "s must have shape (n, d)"
+        assert s.ndim in (2, 3), "s must have shape (n, d) or (b, n, d)"
+        assert s.shape[-1] == self.dim, "dimension mismatch"
         _native.require_gpu()
         host = not (isinstance(s, torch.Tensor) and s.is_cuda)
-        st = torch.from_numpy(np.asarray(s)).cuda() if host else s
-        nv = torch.from_numpy(np.asarray(self.n_vectors, dtype=np.float64)).to(st.device)
-        w = torch.from_numpy(np.asarray(self.weights, dtype=np.float64)).to(st.device)
-        n, d = st.shape
-        theta = _TWO_PI * (st @ nv.T)
-        cos, sin = torch.cos(theta), torch.sin(theta)
-        re, im = cos.sum(0), sin.sum(0)
-        pref = 2.0 * _TWO_PI**2 / float(self.volume)
-        diag_core = re * cos + im * sin
-        hess = torch.empty((n, d, n, d), dtype=torch.float64, device=st.device)
-        for a in range(d):
-            for b in range(d):
-                wab = w * nv[:, a] * nv[:, b]
-                pair = (cos * wab) @ cos.T + (sin * wab) @ sin.T
-                hess[:, a, :, b] = pref * (pair - torch.diag(diag_core @ wab))
-        out = hess.reshape(n * d, n * d)
+        st = torch.from_numpy(np.ascontiguousarray(np.asarray(s))).cuda() if host else s.contiguous()
+        batched = st.ndim == 3
+        if not batched:
+            st = st[None]
+        b, n, d = st.shape
+        dev = st.device.index if st.device.index is not None else torch.cuda.current_device()
+        h = self.problem_handle(dev, n)
+        with torch.cuda.device(dev):
+            out = torch.empty((b, n * d, n * d), dtype=torch.float64, device=st.device)
+            stream = torch.cuda.current_stream(dev).cuda_stream
+            for lo in range(0, b, 65535):
+                hi = min(b, lo + 65535)
+                code = _native.load().cco_hessian(h, stream, hi - lo, st[lo:hi].data_ptr(),
+                                                  out[lo:hi].data_ptr())  # fmt: skip
+                _native.check(code, "cco_hessian")
+        if not batched:
+            out = out[0]
         return out.cpu().numpy() if host else out
 
 
