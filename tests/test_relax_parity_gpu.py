@@ -1,0 +1,78 @@
+"""Relaxation parity on the plain FP64 workloads' exact seeds, against the
+oracle run to completion (fixtures written by tests/golden/make_relax_golden.py).
+
+* descent_d3_n100: d = 3, N = 100, chi = 0.05 (M = 13), batch 5, seed 0,
+  DescentSettings(grow=2.0, max_evals=200_000, energy_tol=9.99999968e-21), the
+  reference README's relax call (README.md:78) with the ground-state driver's
+  default tolerance (src/xla_cco/cli/relax.py:84).
+* lbfgs_d2_n1000: d = 2, N = 1000, chi = 0.40 (M = 802), batch 256, seed 0,
+  LBFGSSettings(energy_tol=1e-20).
+
+Gates: identical success masks (energy < tol) and identical statuses; each
+device energy re-evaluated by the oracle at the device's final positions
+within the energy gate (1e-12 relative, floor C_E eps sqrt(N M E)). The
+descent is the reference's deterministic loop, so its iteration counts and
+final positions are compared with the oracle's too. L-BFGS iterates are not
+pinned (the reference takes them from optax), so for L-BFGS only the
+outcome is compared.
+"""
+
+from __future__ import annotations
+
+import json
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN, RTOL_KERNEL_E, energy_atol
+from golden.make_relax_golden import workload_inputs
+from xla_cco import cubic_box, enumerate_kvectors, k_outer_from_ka, ka_from_chi, make_stealthy_energy, relax
+
+pytestmark = pytest.mark.gpu
+
+
+def _fixture(name):
+    meta = json.loads((GOLDEN / "relax_golden.json").read_text())[name]
+    with np.load(GOLDEN / "relax_golden.npz") as z:
+        arr = {k.split("/", 1)[1]: np.asarray(z[k]) for k in z.files if k.startswith(name + "/")}
+    return meta, arr
+
+
+def _energy(meta):
+    box = cubic_box(meta["n"], meta["d"])
+    ks = enumerate_kvectors(box.basis, 0.0,
+                            k_outer_from_ka(ka_from_chi(meta["chi"], 0.05, meta["d"]), 0.05, meta["d"]))
+    assert ks.n.shape[0] == meta["m"]
+    return box, ks, make_stealthy_energy(box, ks)
+
+
+def _check_outcome(name):
+    meta, ref = _fixture(name)
+    s0, n, w, vol, st, tol = workload_inputs(name)
+    box, ks, en = _energy(meta)
+    res = relax(en, s0, st)
+    ok = res.energy < tol
+    np.testing.assert_array_equal(ok, ref["success"])
+    np.testing.assert_array_equal(res.status, ref["status"])
+    # the device's final energies, checked by the oracle at the device's final positions
+    e_chk, _ = oracle.energy_grad_accurate(res.s, ks.n, ks.weights, box.volume)
+    for i in range(s0.shape[0]):
+        atol = energy_atol(meta["n"], meta["m"], float(e_chk[i]))
+        np.testing.assert_allclose(res.energy[i], e_chk[i], rtol=RTOL_KERNEL_E, atol=atol)
+    return meta, ref, res
+
+
+def test_descent_d3_n100_matches_oracle_run_to_completion():
+    meta, ref, res = _check_outcome("descent_d3_n100")
+    assert ref["success"].all()
+    # the descent loop is deterministic: the same accepted steps, hence the
+    # same iteration counts and final positions (to rounding)
+    np.testing.assert_array_equal(res.n_iters, ref["n_iters"])
+    np.testing.assert_array_equal(res.n_evals, ref["n_evals"])
+    np.testing.assert_allclose(res.s, ref["s"], rtol=0, atol=1e-9)
+
+
+def test_lbfgs_d2_n1000_b256_masks_match_oracle_run_to_completion():
+    meta, ref, res = _check_outcome("lbfgs_d2_n1000")
+    assert ref["success"].sum() == meta["successes"]
