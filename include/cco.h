@@ -19,8 +19,9 @@
  *   cco_relax_lbfgs      <- relax(energy, s0, LBFGSSettings, chunk_iters)
  *                                                         src/xla_cco/minimize/lbfgs.py:163-350
  *   cco_device_count     <- require_gpu                  src/xla_cco/_device.py:137-142
- * The JAX FFI handlers a maintainer would register over these entry points
- * are described in INTEGRATION.md.
+ *   cco_hessian          <- StealthyEnergy.hessian       src/xla_cco/energy.py:272-299
+ * Each entry point is plain C so that an XLA FFI handler (or any other
+ * foreign-function binding) can wrap it without C++ types.
  */
 #ifndef CCO_H
 #define CCO_H
@@ -95,6 +96,18 @@ int cco_energy_grad(cco_problem* p, void* stream, int batch, const double* s,
                     double* phi, double* grad, double* rho_re, double* rho_im);
 
 /*
+ * Closed-form Hessian d2 Phi / ds_ja ds_lb of `batch` configurations
+ *   <- StealthyEnergy.hessian             src/xla_cco/energy.py:272-299
+ * (the Jacobian of the ROS2 gradient flow, src/xla_cco/minimize/flow.py:367-398).
+ *   s     device [batch][N][d] fractional positions
+ *   hess  device [batch][N d][N d], row (j d + a), column (l d + b)
+ * No (N, M) phase matrix is formed: the kernels build each k-chunk's phases
+ * of a particle-tile pair in shared memory and exploit the symmetry. batch
+ * <= 65535.
+ */
+int cco_hessian(cco_problem* p, void* stream, int batch, const double* s, double* hess);
+
+/*
  * The mixed-precision evaluation that relaxations with precision = FP32 use
  * while a lane's energy is large (no reference counterpart; the reference is
  * FP64 only): phase tables seeded by FP64 sincospi and stored in FP32, FP32
@@ -127,7 +140,10 @@ int cco_energy_grad_fp32(cco_problem* p, void* stream, int batch, const double* 
  * rejected with CCO_ERR_ARG and nothing is launched - split it into smaller
  * calls. The first call on each device resolves the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. All calls share the one array and nothing in it
+ * before any stream capture. The resolved address is cached for the life of
+ * the process: after cudaDeviceReset (or any teardown of the device's primary
+ * context) it is stale, and this entry point must not be called again on that
+ * device. All calls share the one array and nothing in it
  * needs to start at zero (every call writes all the scratch it reads), but
  * two calls that overlap on the GPU (different streams, or graph branches
  * without an ordering edge) race on it: order them.

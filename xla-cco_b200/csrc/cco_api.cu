@@ -388,9 +388,12 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   pr->M = m;
   std::vector<double> w_run(m);
   std::vector<int> r2r(m);
+  std::vector<double4> krow(m);
   for (int k = 0; k < m; ++k) {
     w_run[k] = weights[order[k]];
     r2r[k] = order[k];
+    const int32_t* nv = n_vectors + (size_t)order[k] * d;
+    krow[k] = make_double4(nv[0], d > 1 ? nv[1] : 0, d > 2 ? nv[2] : 0, w_run[k]);
   }
   cudaError_t e = cudaSuccess;
   e = cudaMalloc(&pr->seg1, s1.size() * sizeof(SegHdr));
@@ -402,6 +405,8 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   if (e == cudaSuccess) e = cudaMemcpy(pr->seg2, s2.data(), s2.size() * sizeof(SegHdr), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(pr->w_run, w_run.data(), m * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(pr->run2ref, r2r.data(), m * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&pr->krow, m * sizeof(double4));
+  if (e == cudaSuccess) e = cudaMemcpy(pr->krow, krow.data(), m * sizeof(double4), cudaMemcpyHostToDevice);
   if (P.gemm) {
     if (e == cudaSuccess) e = cudaMalloc(&pr->grun, grun.size() * sizeof(GemmRun));
     if (e == cudaSuccess) e = cudaMalloc(&pr->gblk, gblk.size() * sizeof(GemmBlock));
@@ -436,6 +441,7 @@ int cco_problem_destroy(cco_problem* p) {
   cudaFree(p->run2ref);
   if (p->grun) cudaFree(p->grun);
   if (p->gblk) cudaFree(p->gblk);
+  if (p->krow) cudaFree(p->krow);
   cudaFree(p->dev);
   delete p;
   return CCO_OK;
@@ -613,6 +619,29 @@ extern "C" int cco_energy_grad_fp32(cco_problem* p, void* stream, int batch, con
   CCO_CUDA(ws.build(p, batch, s, nd, phi, 1, grad, nd, nullptr, 0, st));
   CCO_CUDA(eval_launch(ws.plan, st));
   ws.release(st);
+  CCO_CUDA(cudaGetLastError());
+  return CCO_OK;
+}
+
+extern "C" int cco_hessian(cco_problem* p, void* stream, int batch, const double* s,
+                           double* hess) {
+  if (!p) return fail(CCO_ERR_ARG, "null problem");
+  if (batch < 0) return fail(CCO_ERR_ARG, "batch must be >= 0");
+  if (batch == 0) return CCO_OK;
+  if (!s || !hess) return fail(CCO_ERR_ARG, "null s or hess");
+  if (batch > 65535) return fail(CCO_ERR_ARG, "batch %d > 65535: split it", batch);
+  DeviceGuard guard(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  EvalWS ws;
+  double* phi = nullptr;
+  CCO_CUDA(ws.alloc(p, batch, st));
+  CCO_CUDA(pool_alloc(&phi, sizeof(double) * batch, st));
+  const size_t nd = (size_t)p->N * p->d;
+  CCO_CUDA(ws.build(p, batch, s, nd, phi, 1, nullptr, 0, nullptr, 0, st));
+  CCO_CUDA(eval_launch(ws.plan, st));   // the density the diagonal blocks need
+  CCO_CUDA(hessian_launch(p, st, batch, s, ws.rho, hess));
+  ws.release(st);
+  cudaFreeAsync(phi, st);
   CCO_CUDA(cudaGetLastError());
   return CCO_OK;
 }

@@ -27,10 +27,17 @@ struct cco_problem {
   int* run2ref = nullptr;
   cco::GemmRun* grun = nullptr;
   cco::GemmBlock* gblk = nullptr;
+  double4* krow = nullptr;     // run-order rows (n_0, n_1, n_2, w) for the Hessian kernels
   size_t smem1 = 0, smem2 = 0, smemG = 0;
 };
 
 namespace cco {
+
+// Closed-form Hessians of `batch` configurations (cco_hessian.cu): rho_run is
+// each configuration's run-order density from the evaluation kernels, H is
+// [batch][N d][N d].
+cudaError_t hessian_launch(const cco_problem* p, cudaStream_t st, int batch, const double* s,
+                           const double2* rho_run, double* H);
 
 // Records the message for cco_last_error and returns `code`.
 int fail(int code, const char* fmt, ...);
