@@ -301,12 +301,13 @@ def test_success_mask_is_strict():
 
 def test_hp_g2_tables():
     edges = np.array([0.0, 1.0, 3.0])
-    h = cli.hp_table(np.array([1, 3]), edges)
+    counts = np.array([1, 3])
+    h = np.stack(cli.table_columns(edges, cli.hp_density(counts, edges), counts), axis=1)
     np.testing.assert_allclose(h[:, 0], [0.5, 2.0])
     np.testing.assert_allclose(h[:, 2], [0.5, 1.0])
     np.testing.assert_allclose(h[:, 1], [0.25, 0.375])
     np.testing.assert_allclose(h[:, 3], [0.25, 0.375 / np.sqrt(3)])
     assert math.isclose((h[:, 1] * 2.0 * h[:, 2]).sum(), 1.0)
-    g = cli.g2_table(np.array([2.0, 4.0]), np.array([4, 0]), edges)
+    g = np.stack(cli.table_columns(edges, np.array([2.0, 4.0]), np.array([4, 0])), axis=1)
     np.testing.assert_allclose(g[:, 3], [1.0, 0.0])
     np.testing.assert_allclose(g[:, 1], [2.0, 4.0])

@@ -56,6 +56,31 @@ def nearest_neighbor_distances(s: Any, box: Box) -> Any:
     return out.cpu().numpy() if host else out
 
 
+def nearest_neighbor_distances_batch(s: Any, box: Box) -> Any:
+    """Nearest-neighbour distances (b, n) of a batch (b, n, d) in one kernel
+    call per 65535 configurations (no reference counterpart: the reference
+    maps ``nearest_neighbor_distances`` over configurations). A CUDA input
+    gives a CUDA result; NumPy in, NumPy out."""
+    import torch
+
+    require_float64(s, "s")
+    assert s.ndim == 3 and s.shape[2] == box.dim, "s must have shape (b, n, d)"
+    st, host = _device_positions(s)
+    b, n, d = st.shape
+    basis = _basis(box)
+    dev = st.device.index if st.device.index is not None else torch.cuda.current_device()
+    with torch.cuda.device(dev):
+        out = torch.empty((b, n), dtype=torch.float64, device=st.device)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        for lo in range(0, b, 65535):
+            hi = min(b, lo + 65535)
+            code = _native.load().cco_nearest_neighbor(
+                dev, stream, hi - lo, n, d, st[lo:hi].data_ptr(), basis.ctypes.data,
+                out[lo:hi].data_ptr())  # fmt: skip
+            _native.check(code, "cco_nearest_neighbor")
+    return out.cpu().numpy() if host else out
+
+
 def pair_distance_histogram(s: Any, box: Box, edges: np.ndarray) -> np.ndarray:
     """int64 pair counts (every i < j once per configuration) of (b, n, d) ``s``.
 
