@@ -83,6 +83,36 @@ def test_mixed_precision_success_masks_match_plain(n, d, chi, b):
                                    atol=energy_atol(n, ks.n.shape[0], e_ref))  # fmt: skip
 
 
+@pytest.mark.parametrize("case", ["grad_tol", "budget", "energy_tol"])
+def test_fp32_lane_never_ends_on_an_fp32_judgement(case):
+    """A lane still in FP32 that meets a stopping rule (gradient tolerance,
+    budget, or an energy below the tolerance) first switches to FP64; the
+    status and the energy it reports are FP64 results at its final point."""
+    import torch
+
+    box, ks, en = _system(300, 2, 0.3)
+    b = 4
+    s0 = torch.from_numpy(np.random.default_rng(11).uniform(size=(b, 300, 2))).cuda()
+    if case == "grad_tol":   # met at the first iteration, while every lane is in FP32
+        st = LBFGSSettings(grad_tol=1e30, precision="mixed")
+        want = 6
+    elif case == "budget":   # one pass whose budget ends inside the FP32 phase
+        st = LBFGSSettings(rescales=(1.0,), max_evals_per_pass=6, precision="mixed")
+        want = 3
+    else:                    # a tolerance the very first (FP32) evaluation meets
+        st = LBFGSSettings(energy_tol=1e30, precision="mixed")
+        want = 1
+    out = relax_device(en, s0, st)
+    status = out["status"].cpu().numpy()
+    np.testing.assert_array_equal(status, np.full(b, want))
+    n32 = out["n_evals_fp32"].cpu().numpy()
+    ne = out["n_evals"].cpu().numpy()
+    assert (n32 > 0).all() and (n32 < ne).all(), (n32, ne)
+    # the reported energy is an FP64 evaluation at the reported (wrapped) positions
+    phi64, _, _, _ = en.evaluate(out["s"], want_grad=False)
+    np.testing.assert_allclose(out["energy"].cpu().numpy(), phi64.cpu().numpy(), rtol=1e-12, atol=0)
+
+
 def test_mixed_precision_served_equals_relaxed_alone():
     _, _, en = _system(400, 2, 0.35)
     rng = np.random.default_rng(3)

@@ -392,14 +392,17 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
     int local = L.pass_evals >= A.budget ? CCO_STATUS_BUDGET : CCO_STATUS_RUNNING;
     if (L.stag >= A.patience) local = CCO_STATUS_STAGNATED;
     if (fail) local = CCO_STATUS_LINESEARCH_FAIL;
-    // mixed precision: an FP32 lane switches to FP64 instead of ending its
-    // pass on a failed or stagnating line search, and once its energy is low
+    // mixed precision: an FP32 lane never ends, and never ends a pass, on an
+    // FP32 judgement. Once its energy is low, or on any outcome that would
+    // stop it (energy or gradient tolerance, budget, stagnation, a failed
+    // line search), it switches to FP64 at the current point; the FP64
+    // re-evaluation and the FP64 iterations after it decide the status.
     bool sw = false;
-    if (L.prec == PREC_FP32 && glob == CCO_STATUS_RUNNING) {
+    if (L.prec == PREC_FP32) {
       const bool low = L.f < kFp32SwitchPerParticle * (double)R.n;
-      const bool stuck = local == CCO_STATUS_LINESEARCH_FAIL || local == CCO_STATUS_STAGNATED;
-      if (low || stuck) {
+      if (low || glob != CCO_STATUS_RUNNING || local != CCO_STATUS_RUNNING) {
         sw = true;
+        glob = CCO_STATUS_RUNNING;
         local = CCO_STATUS_RUNNING;
       }
     }
@@ -519,8 +522,16 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
       L.status = L.f < A.energy_tol ? CCO_STATUS_ENERGY_TOL : CCO_STATUS_RUNNING;
       L.last_step = 0.0;
       L.phase = PH_EXPAND;
-      if (L.status != CCO_STATUS_RUNNING) L.t1 = gtimer();
-      else L.need_dir = 1;
+      if (L.status != CCO_STATUS_RUNNING && L.prec == PREC_FP32) {
+        // an FP32 start below the tolerance is judged again in FP64
+        L.status = CCO_STATUS_RUNNING;
+        L.prec = PREC_FP64;
+        L.phase = PH_REEVAL;
+      } else if (L.status != CCO_STATUS_RUNNING) {
+        L.t1 = gtimer();
+      } else {
+        L.need_dir = 1;
+      }
     }
     __syncthreads();
     lb_record(A, lane, R, sh, v.s);
