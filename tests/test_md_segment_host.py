@@ -118,6 +118,52 @@ def test_checkpoint_round_trip(tmp_path):
     assert not (tmp_path / "x.npz").exists() and not (tmp_path / "x.npz.tmp").exists()
 
 
+# The reference's leaf order (jax.tree_util flattening of its MDState,
+# src/xla_cco/dynamics/state.py:129-164): fields in declaration order, the
+# Snapshots and RhoTrace buffers flattened in place.
+_REFERENCE_LEAVES = (
+    "r", "v", "f", "phi", "temperature", "key", "step", "time", "reset_acc", "rho_prev",
+    "wind_abs", "wind_net", "n_valid", "e0", "max_drift", "sum_kinetic", "sum_phi", "sum_phi2",
+    "sum_s", "n_sum", "status", "snap.step", "snap.time", "snap.wind_abs", "snap.wind_net",
+    "snap.rho", "snap.r", "snap.phi", "snap.kinetic", "snap.count", "trace.rho", "trace.time",
+    "trace.count",
+)  # fmt: skip
+
+
+def _field(state, dotted):
+    obj = state
+    for name in dotted.split("."):
+        obj = getattr(obj, name)
+    return np.asarray(obj)
+
+
+def test_checkpoint_reads_and_writes_the_reference_layout(tmp_path):
+    """A file in the reference's layout (leaf_NNN, __n_leaves__, __meta__),
+    written here by hand, loads into the right fields; our own files have
+    exactly that layout, key as uint32[2]."""
+    st = _state()
+    arrays = {f"leaf_{i:03d}": _field(st, name) for i, name in enumerate(_REFERENCE_LEAVES)}
+    arrays["__n_leaves__"] = np.int64(len(_REFERENCE_LEAVES))
+    arrays["__meta__"] = np.asarray('{"chunk": 7}')
+    np.savez(tmp_path / "ref.npz", **arrays)
+    got, meta = load_state(tmp_path / "ref.npz", st)
+    assert meta == {"chunk": 7}
+    for name in _REFERENCE_LEAVES:
+        np.testing.assert_array_equal(_field(got, name), _field(st, name))
+    save_state(tmp_path / "ours.npz", st, {"chunk": 7})
+    with np.load(tmp_path / "ours.npz") as z:
+        assert sorted(z.files) == sorted(arrays)
+        assert int(z["__n_leaves__"]) == len(_REFERENCE_LEAVES)
+        for i, name in enumerate(_REFERENCE_LEAVES):
+            np.testing.assert_array_equal(z[f"leaf_{i:03d}"], _field(st, name))
+        assert z["leaf_005"].dtype == np.uint32 and z["leaf_005"].shape[-1] == 2
+    # a wrong leaf count is a CheckpointError naming both counts
+    arrays["__n_leaves__"] = np.int64(32)
+    np.savez(tmp_path / "short.npz", **arrays)
+    with pytest.raises(CheckpointError, match="32 leaves"):
+        load_state(tmp_path / "short.npz", st)
+
+
 def test_thermal_helpers():
     key = make_key(3)
     v = maxwell_boltzmann(key, 4000, 3, 2.0, remove_com=True)
