@@ -222,6 +222,33 @@ int cco_relax_lbfgs(cco_problem* p, void* stream, int batch, const double* s0,
                     cco_relax_out* out);
 
 /*
+ * Relaxations whose energy the caller evaluates  <- relax(energy, s0, settings)
+ * with any AbstractEnergy          src/xla_cco/minimize/__init__.py:102-151,
+ *                                  src/xla_cco/energy.py:115-137
+ * The reference's minimizers only call energy.value_and_grad, so relax takes
+ * any energy. A stepper runs the same device lanes as cco_relax_descent /
+ * cco_relax_lbfgs (method 0 / 1, settings a cco_descent_settings or
+ * cco_lbfgs_settings; FP64, no trajectory) and leaves every evaluation to the
+ * caller:
+ *   loop { cco_stepper_probes(h, st, ps)        ps: device [B][N][d] out, the
+ *                                                positions to evaluate
+ *          caller: f[B] = E(ps), g[B][N][d] = dE/ds at ps (device arrays)
+ *          cco_stepper_advance(h, st, f, g, &n) one tick; n = lanes still running
+ *   } until n == 0, then cco_stepper_finish(h, st, out) (the cco_relax_out
+ * results, trajectory fields unused) and cco_stepper_destroy(h). s0: device
+ * [B][N][d]. Lanes that have finished ignore further evaluations. batch <=
+ * 65535.
+ */
+typedef struct cco_stepper cco_stepper;
+int cco_stepper_create(int device, void* stream, int method, const void* settings, int batch,
+                       int n_particles, int d, const double* s0, cco_stepper** out);
+int cco_stepper_probes(cco_stepper* h, void* stream, double* ps);
+int cco_stepper_advance(cco_stepper* h, void* stream, const double* f, const double* g,
+                        int64_t* n_running);
+int cco_stepper_finish(cco_stepper* h, void* stream, cco_relax_out* out);
+int cco_stepper_destroy(cco_stepper* h);
+
+/*
  * Mixed batches: lane i relaxes configuration i of problems[i], so one call
  * runs instances of different N, d and k-set side by side (the same
  * evaluation and minimizer launches serve every lane). All problems live on

@@ -195,6 +195,15 @@ SIGNATURES = {
     "cco_energy_grad_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
     "cco_energy_grad_fp32": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp, _vp]),
     "cco_hessian": (ctypes.c_int, [_vp, _vp, ctypes.c_int, _vp, _vp]),
+    "cco_stepper_create": (
+        ctypes.c_int,
+        [ctypes.c_int, _vp, ctypes.c_int, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+         ctypes.POINTER(_vp)],
+    ),  # fmt: skip
+    "cco_stepper_probes": (ctypes.c_int, [_vp, _vp, _vp]),
+    "cco_stepper_advance": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int64)]),
+    "cco_stepper_finish": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(RelaxOutC)]),
+    "cco_stepper_destroy": (ctypes.c_int, [_vp]),
     "cco_relax_descent": (
         ctypes.c_int,
         [_vp, _vp, ctypes.c_int, _vp, ctypes.POINTER(DescentSettingsC), ctypes.c_int,

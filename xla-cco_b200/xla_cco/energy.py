@@ -40,8 +40,13 @@ def _torch():
 class AbstractEnergy(abc.ABC):
     """Extension point for energies on fractional positions (``energy.py:115-137``).
 
-    The B200 minimizers drive only ``StealthyEnergy`` (its kernel is fused
-    into the device loop); other subclasses can be evaluated on the host.
+    A subclass provides ``__call__`` (the scalar energy of one (N, d)
+    configuration). As in the reference, ``value_and_grad`` and ``hessian``
+    default to automatic differentiation of ``__call__`` - here torch
+    autograd, so ``__call__`` must accept a float64 CUDA tensor and use torch
+    operations; a subclass may override either with a closed form.
+    ``relax`` accepts any subclass: the minimizer lanes run on the device and
+    call the energy's ``value_and_grad`` once per tick.
     """
 
     @abc.abstractmethod
@@ -49,8 +54,32 @@ class AbstractEnergy(abc.ABC):
         """Scalar energy of fractional positions ``s``."""
 
     def value_and_grad(self, s: Any) -> Tuple[Any, Any]:
-        """(energy, dE/ds); subclasses that are minimized must override this."""
-        raise NotImplementedError("value_and_grad must be provided by the subclass")
+        """(energy, dE/ds) by autograd of ``__call__`` (the reference uses
+        ``jax.value_and_grad``)."""
+        torch = _torch()
+        x = _as_cuda(s).detach().clone().requires_grad_(True)
+        with torch.enable_grad():
+            value = self(x)
+            (grad,) = torch.autograd.grad(value, x)
+        return value.detach(), grad.detach()
+
+    def hessian(self, s: Any) -> Any:
+        """d^2 E / ds ds flattened to (N d, N d), by autograd of ``__call__``
+        (the reference uses ``jax.hessian``)."""
+        torch = _torch()
+        x = _as_cuda(s).detach()
+        h = torch.autograd.functional.hessian(lambda y: self(y), x)
+        return h.reshape(x.numel(), x.numel())
+
+
+def _as_cuda(s: Any):
+    """``s`` as a float64 CUDA tensor (a NumPy array is copied to the device)."""
+    torch = _torch()
+    require_float64(s, "s")
+    if isinstance(s, torch.Tensor):
+        return s if s.is_cuda else s.cuda()
+    _native.require_gpu()
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(s))).cuda()
 
 
 class _Problems:

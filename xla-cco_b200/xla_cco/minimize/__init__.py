@@ -21,8 +21,8 @@ from xla_cco.minimize.descent import DescentSettings
 from xla_cco.minimize.lbfgs import LBFGSSettings
 from xla_cco.minimize.result import STATUS_BUDGET, STATUS_RUNNING, RelaxResult, Trajectory  # noqa: F401
 
-__all__ = ["relax", "relax_device", "relax_mixed", "relax_mixed_device", "DescentSettings",
-           "LBFGSSettings"]
+__all__ = ["relax", "relax_device", "relax_external", "relax_mixed", "relax_mixed_device",
+           "DescentSettings", "LBFGSSettings"]
 
 
 def _descent_c(st: DescentSettings) -> _native.DescentSettingsC:
@@ -136,6 +136,83 @@ def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSet
     return out
 
 
+def _max_ticks(settings: Union[DescentSettings, LBFGSSettings]) -> int:
+    """The tick bound of a relaxation (one evaluation per lane and tick): its
+    evaluation budget plus a margin, like the fused path's round bound."""
+    if isinstance(settings, DescentSettings):
+        return 1 + settings.max_evals // 2 + 64
+    per_pass = settings.max_evals_per_pass + settings.max_linesearch_steps + 1
+    return 1 + len(settings.rescales) * per_pass + 64
+
+
+def relax_external(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings]) -> dict:
+    """Relax a CUDA batch ``s0`` (B, N, d) under any ``AbstractEnergy``.
+
+    The lanes are the device state machines of the fused path (the same
+    records and update kernels, ``cco_stepper_*``); every tick this loop
+    hands the lanes' probe positions to ``energy.value_and_grad`` - one call
+    per lane, as the reference vmaps it, or one ``energy.value_and_grad_batch``
+    call on the whole (B, N, d) batch when the energy defines it - and feeds
+    the results back. FP64 only, no trajectory recording. Returns the dict of
+    ``relax_device``.
+    """
+    import torch
+
+    if isinstance(settings, LBFGSSettings) and settings.precision != "fp64":
+        raise ValueError("mixed precision needs a StealthyEnergy (its FP32 kernels)")
+    if settings.record_every > 0 and settings.max_records > 0:
+        raise ValueError("trajectory recording needs a StealthyEnergy")
+    cset, _ = _settings_c(settings)
+    method = 0 if isinstance(settings, DescentSettings) else 1
+    b, n, d = (int(x) for x in s0.shape)
+    dev = s0.device
+    index = dev.index if dev.index is not None else torch.cuda.current_device()
+    lib = _native.load()
+    batched = getattr(energy, "value_and_grad_batch", None)
+    out = _outputs(b, (b, n, d), (b, 0, n, d), settings, dev)
+    with torch.cuda.device(index):
+        stream = torch.cuda.current_stream(index).cuda_stream
+        h = _native._vp()
+        _native.check(lib.cco_stepper_create(index, stream, method, _native.ctypes.byref(cset), b, n,
+                                             d, s0.contiguous().data_ptr(),
+                                             _native.ctypes.byref(h)), "cco_stepper_create")  # fmt: skip
+        try:
+            ps = torch.empty((b, n, d), dtype=torch.float64, device=dev)
+            f = torch.empty(b, dtype=torch.float64, device=dev)
+            g = torch.empty((b, n, d), dtype=torch.float64, device=dev)
+            running = _native.ctypes.c_int64(b)
+            bound, ticks = _max_ticks(settings), 0
+            while running.value > 0:
+                if ticks >= bound:
+                    raise RuntimeError("relax did not finish within the round bound")
+                _native.check(lib.cco_stepper_probes(h, stream, ps.data_ptr()), "cco_stepper_probes")
+                if batched is not None:
+                    fv, gv = batched(ps)
+                    f.copy_(torch.as_tensor(fv, dtype=torch.float64, device=dev).reshape(b))
+                    g.copy_(torch.as_tensor(gv, dtype=torch.float64, device=dev).reshape(b, n, d))
+                else:
+                    for i in range(b):
+                        fv, gv = energy.value_and_grad(ps[i])
+                        f[i] = torch.as_tensor(fv, dtype=torch.float64, device=dev)
+                        g[i] = torch.as_tensor(gv, dtype=torch.float64, device=dev).reshape(n, d)
+                _native.check(lib.cco_stepper_advance(h, stream, f.data_ptr(), g.data_ptr(),
+                                                      _native.ctypes.byref(running)),
+                              "cco_stepper_advance")  # fmt: skip
+                ticks += 1
+            co = _native.RelaxOutC()
+            for key in ("s", "energy", "grad_norm", "n_evals", "n_iters", "status", "latency_ns",
+                        "n_evals_fp32"):  # fmt: skip
+                setattr(co, key, out[key].data_ptr())
+            _native.check(lib.cco_stepper_finish(h, stream, _native.ctypes.byref(co)),
+                          "cco_stepper_finish")  # fmt: skip
+        finally:
+            lib.cco_stepper_destroy(h)
+    out["ticks"] = ticks
+    out["launches"] = 0
+    out["schedule"] = (0, 0)
+    return out
+
+
 def relax(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
           chunk_iters: int = 2_000) -> RelaxResult:  # fmt: skip
     """Relax a batch of configurations; result leaves carry a leading batch axis.
@@ -159,7 +236,14 @@ def relax(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
     else:
         host = True
         s_dev = torch.from_numpy(np.ascontiguousarray(np.asarray(s0))).cuda()
-    out = relax_device(energy, s_dev, settings, chunk_iters)
+    from xla_cco.energy import AbstractEnergy, StealthyEnergy
+
+    if isinstance(energy, StealthyEnergy):
+        out = relax_device(energy, s_dev, settings, chunk_iters)
+    elif isinstance(energy, AbstractEnergy):
+        out = relax_external(energy, s_dev, settings)
+    else:
+        raise TypeError(f"energy must be an AbstractEnergy, got {type(energy).__name__}")
     conv = (lambda t: t.cpu().numpy()) if host else (lambda t: t)
     traj = None
     if "traj_s" in out:
