@@ -10,7 +10,8 @@
 // complex multiply, exp(i th_{k+1,j}) = exp(i th_kj) z_j, z_j = exp(2 pi i
 // s_{j,d-1}). A segment start takes its phase from per-particle tables in
 // shared memory: z_a^|n| = prod_l T_a,l[digit_l(|n|)]. Table entries come
-// from FP64 sincospi of the exact integer exponent, re-seeded every 8 entries
+// from FP64 sincospi of the exact integer exponent (the product e s reduced
+// without rounding, sincos_2pi_ms), re-seeded every 8 entries
 // with products in between, so a phase carries O(10 eps) error on top of the
 // <= segment-length products along a run - inside the reference's eps |theta|
 // trig error. No theta matrix ever reaches HBM: traffic per evaluation is s
@@ -85,7 +86,7 @@ __device__ void build_tables(const TabLayout& T, const double* __restrict__ s, i
     if (l == 0) {
       sincospi(2.0 * sv, &sn, &cs);
       const double2 z = make_double2(cs, sn);
-      sincospi(2.0 * ((double)e0 * sv), &sn, &cs);
+      sincos_2pi_ms((double)e0, sv, &sn, &cs);
       double2 p = make_double2(cs, sn);
       for (int e = e0; e < e1; ++e) {
         put(out + (size_t)e * stride, p);
@@ -93,7 +94,7 @@ __device__ void build_tables(const TabLayout& T, const double* __restrict__ s, i
       }
     } else {
       for (int e = e0; e < e1; ++e) {
-        sincospi(2.0 * ((double)(e * scale) * sv), &sn, &cs);
+        sincos_2pi_ms((double)(e * scale), sv, &sn, &cs);
         put(out + (size_t)e * stride, make_double2(cs, sn));
       }
     }
@@ -603,7 +604,7 @@ __device__ void pass2_body_f32(const ProbDev& P, const EvalLane& ln, int tile, i
 __device__ __forceinline__ void fill_powers(double2* dst, int e0, int cnt, int base, double s,
                                             double2 z) {
   double sn, cs;
-  sincospi(2.0 * ((double)(base + e0) * s), &sn, &cs);
+  sincos_2pi_ms((double)(base + e0), s, &sn, &cs);
   double2 p = make_double2(cs, sn);
   for (int e = 0; e < cnt; ++e) {
     dst[e0 + e] = p;

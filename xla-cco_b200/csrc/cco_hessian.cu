@@ -61,19 +61,8 @@ struct Combos<3> {
 template <int D>
 __device__ __forceinline__ double2 exact_phase(const double4& nk, const double* sj) {
   const double nv[3] = {nk.x, nk.y, nk.z};
-  double hi = 0.0, lo = 0.0;
-#pragma unroll
-  for (int a = 0; a < D; ++a) {
-    const double p = nv[a] * sj[a];
-    const double e = fma(nv[a], sj[a], -p);   // p + e = n_a s_a exactly
-    const double t = hi + p;
-    const double z = t - hi;
-    lo += ((hi - (t - z)) + (p - z)) + e;
-    hi = t;
-  }
-  const double r = (hi - rint(hi)) + lo;
   double sn, cs;
-  sincospi(2.0 * r, &sn, &cs);
+  sincos_2pi_dot<D>(nv, sj, &sn, &cs);
   return make_double2(cs, sn);
 }
 

@@ -119,6 +119,37 @@ struct EvalItem {
   int tile;
 };
 
+// ---------------------------------------------------------------- phases
+// sin and cos of 2 pi m s for an integer-valued m and any s. The product m s
+// is formed without rounding (p + e == m s, e by fma) and its nearest integer
+// removed exactly before sincospi, so the phase keeps full precision however
+// large |m s| is. Passing the rounded product instead puts |m s| eps of
+// absolute error into the argument: 1.4e-12 rad at |m s| ~ 4000, which
+// makes Phi ~ M (1.4e-12)^2 ~ 1e-20 the roundoff floor of a wide 1-D k-set.
+__device__ __forceinline__ void sincos_2pi_ms(double m, double s, double* sn, double* cs) {
+  const double p = m * s;
+  const double e = fma(m, s, -p);
+  sincospi(2.0 * ((p - rint(p)) + e), sn, cs);
+}
+
+// The same for n . s = sum_a n_a s_a (integer-valued n_a): exact products,
+// compensated sum, nearest integer removed before sincospi.
+template <int D>
+__device__ __forceinline__ void sincos_2pi_dot(const double* n, const double* s, double* sn,
+                                               double* cs) {
+  double hi = 0.0, lo = 0.0;
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const double p = n[a] * s[a];
+    const double e = fma(n[a], s[a], -p);
+    const double t = hi + p;
+    const double z = t - hi;
+    lo += ((hi - (t - z)) + (p - z)) + e;
+    hi = t;
+  }
+  sincospi(2.0 * ((hi - rint(hi)) + lo), sn, cs);
+}
+
 // ---------------------------------------------------------------- complex
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);

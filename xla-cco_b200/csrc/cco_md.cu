@@ -404,10 +404,10 @@ __global__ void __launch_bounds__(kUpdThreads) k_md_waves(MdArgs a) {
     __syncthreads();
     if (u < a.w)
       for (int jj = 0; jj < nj; ++jj) {
-        double dot = 0.0;
-        for (int q = 0; q < d; ++q) dot += nv[q] * tile[jj * d + q];
         double sn, cs;
-        sincospi(2.0 * dot, &sn, &cs);
+        if (d == 1) sincos_2pi_dot<1>(nv, tile + jj, &sn, &cs);
+        else if (d == 2) sincos_2pi_dot<2>(nv, tile + jj * 2, &sn, &cs);
+        else sincos_2pi_dot<3>(nv, tile + jj * 3, &sn, &cs);
         re += cs;
         im += sn;
       }

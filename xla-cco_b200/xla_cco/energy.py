@@ -113,10 +113,10 @@ class _Problems:
         # energy that never reached the device must not map libcco.so here.
         if not self._handles:
             return
-        lib = _native.loaded()
-        if lib is None:
-            return
-        try:
+        try:   # at interpreter shutdown the module globals may already be gone
+            lib = _native.loaded()
+            if lib is None:
+                return
             for h in self._handles.values():
                 lib.cco_problem_destroy(h)
         except Exception:
