@@ -387,13 +387,13 @@ def _flops(evals, inst) -> float:
 def plain_dropin(inst, settings, sample: int) -> dict:
     """The reference's usage on a mixed ensemble: one relax call per instance
     (relax takes one energy, so instances of different N, d, chi cannot share
-    a call). Times `sample` instances one after another, after one untimed
-    pass over the same instances."""
+    a call). Times the first `sample` instances (0: all of them) one after
+    another, after one untimed pass over the same instances."""
     import torch
 
     from xla_cco.minimize import relax_device
 
-    sub = inst[:sample]
+    sub = inst[:sample] if sample > 0 else inst
     dev = [torch.from_numpy(i.s0[None]).cuda() for i in sub]
     for i, x in zip(sub, dev):
         relax_device(i.energy, x, settings)
@@ -406,8 +406,10 @@ def plain_dropin(inst, settings, sample: int) -> dict:
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     succ = sum(int((o["energy"] < TOL).sum().item()) for o in outs)
+    ok = np.array([bool((o["energy"] < TOL).item()) for o in outs])
     return {"value": succ / (ms / 1e3), "unit": UNIT, "instances": len(sub), "success": succ,
-            "ms": ms, "how": "relax(energy_i, s0_i[None]) per instance, sequential, same device"}  # fmt: skip
+            "ms": ms, "how": "relax(energy_i, s0_i[None]) per instance, sequential, same device",
+            "mask": ok}  # fmt: skip
 
 
 def served_mixed(inst, ok_plain) -> dict:
@@ -471,7 +473,13 @@ def run_mixed(args) -> None:
     flops = _flops(evals, inst) * args.steps
     value = succ / (ms / 1e3)
     plain = plain_dropin(inst, settings, args.plain_sample)
-    served = served_mixed(inst, outs[-1]["energy"].cpu().numpy() < TOL) if args.served else None
+    plain_mask = plain.pop("mask")
+    batched_ok = outs[-1]["energy"].cpu().numpy() < TOL
+    if plain_mask.size == batched_ok.size:
+        plain["mask_equals_batched"] = bool((plain_mask == batched_ok).all())
+    # the served mixed-precision form is judged against the plain drop-in's mask
+    ref_mask = plain_mask if plain_mask.size == batched_ok.size else batched_ok
+    served = served_mixed(inst, ref_mask) if args.served else None
     peak = fp64_peak_tflops()
     achieved = flops / (ms * 1e-3) / 1e12
     line = {
@@ -981,7 +989,7 @@ def main() -> None:
                     help="batch: the headline 256-lane d2 N1000 relax; mixed: the 512-instance "
                          "mixed-size ensemble; serve: a Poisson request stream")  # fmt: skip
     ap.add_argument("--mixed-count", type=int, default=512)
-    ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--plain-sample", type=int, default=0, help="0: every instance")
     ap.add_argument("--served", action="store_true",
                     help="mixed workload: also serve the ensemble with mixed precision")  # fmt: skip
     ap.add_argument("--serve-count", type=int, default=200)
