@@ -96,6 +96,6 @@ def test_lbfgs_relaxation_through_the_gemm_form_vs_oracle():
     res = relax(en, s0, LBFGSSettings(energy_tol=1e-20))
     assert (res.energy < 1e-20).all() and (res.status == 1).all()
     # the device's final energies, re-evaluated by the oracle at the device's positions
-    e_chk, _ = oracle.energy_grad_batch(res.s, ks.n.astype(np.int64), np.ones(ks.n.shape[0]), float(n),
-                                        threads=oracle.max_threads())  # fmt: skip
+    # (the accurate mode: at Phi ~ 1e-20 the plain FP64 oracle's own rounding exceeds 1e-24)
+    e_chk, _ = oracle.energy_grad_accurate(res.s, ks.n.astype(np.int64), np.ones(ks.n.shape[0]), float(n))
     np.testing.assert_allclose(res.energy, e_chk, rtol=1e-6, atol=1e-24)

@@ -60,7 +60,7 @@ def test_fp32_evaluation_against_oracle(n, d, chi, b):
         np.testing.assert_allclose(g[i].cpu().numpy(), gr, rtol=0, atol=RTOL_FP32_F * np.abs(gr).max())
 
 
-@pytest.mark.parametrize("n,d,chi,b", [(500, 2, 0.40, 24), (300, 3, 0.45, 16), (600, 1, 0.35, 8)])
+@pytest.mark.parametrize("n,d,chi,b", [(500, 2, 0.40, 24), (300, 3, 0.45, 16), (900, 2, 0.49, 16)])
 def test_mixed_precision_success_masks_match_plain(n, d, chi, b):
     import torch
 
@@ -111,6 +111,39 @@ def test_fp32_lane_never_ends_on_an_fp32_judgement(case):
     # the reported energy is an FP64 evaluation at the reported (wrapped) positions
     phi64, _, _, _ = en.evaluate(out["s"], want_grad=False)
     np.testing.assert_allclose(out["energy"].cpu().numpy(), phi64.cpu().numpy(), rtol=1e-12, atol=0)
+
+
+def test_failed_mixed_lane_returns_the_plain_fp64_result():
+    """A mixed lane that ends above energy_tol runs again from s0 in FP64: its
+    positions, energy, status and iterations are the plain run's bits; its
+    evaluation count includes the discarded mixed run."""
+    import torch
+
+    _, _, en = _system(300, 2, 0.35)
+    s0 = torch.from_numpy(np.random.default_rng(21).uniform(size=(4, 300, 2))).cuda()
+    st = dict(energy_tol=TOL, max_evals_per_pass=40)    # too small a budget to reach 1e-20
+    plain = relax_device(en, s0, LBFGSSettings(**st))
+    mixed = relax_device(en, s0, LBFGSSettings(precision="mixed", **st))
+    assert (plain["energy"] >= TOL).all()
+    for k in ("s", "energy", "grad_norm", "n_iters", "status"):
+        np.testing.assert_array_equal(mixed[k].cpu().numpy(), plain[k].cpu().numpy())
+    ne_m, ne_p = mixed["n_evals"].cpu().numpy(), plain["n_evals"].cpu().numpy()
+    n32 = mixed["n_evals_fp32"].cpu().numpy()
+    assert (n32 > 0).all() and (ne_m > ne_p + n32 - 1).all(), (ne_m, ne_p, n32)
+
+
+def test_one_dimensional_lanes_stay_fp64_in_mixed_mode():
+    """1-D lanes of a mixed run never evaluate in FP32 and equal plain FP64
+    lanes bit for bit (the FP64 lanes of a mixed run use the plain kernels)."""
+    import torch
+
+    _, _, en = _system(500, 1, 0.3)
+    s0 = torch.from_numpy(np.random.default_rng(22).uniform(size=(3, 500, 1))).cuda()
+    plain = relax_device(en, s0, LBFGSSettings(energy_tol=TOL))
+    mixed = relax_device(en, s0, LBFGSSettings(energy_tol=TOL, precision="mixed"))
+    assert (mixed["n_evals_fp32"].cpu().numpy() == 0).all()
+    for k in ("s", "energy", "n_evals", "n_iters", "status"):
+        np.testing.assert_array_equal(mixed[k].cpu().numpy(), plain[k].cpu().numpy())
 
 
 def test_mixed_precision_served_equals_relaxed_alone():

@@ -835,18 +835,22 @@ __global__ void __launch_bounds__(kGemmThreads, 4) k_pass1_gemm(EvalPlan plan) {
     pass1_gemm_body<D>(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
 }
 
-// One kernel per dimension D (and per precision mode) keeps each kernel's
-// code small: the instruction cache holds one body instead of all of them.
-template <int D, bool DYN>
+// One kernel per dimension D and arithmetic keeps each kernel's code small:
+// the instruction cache holds one body instead of all of them. F32 = false
+// evaluates the FP64 lanes of a launch, F32 = true its FP32 lanes (a plan with
+// FP32 lanes launches both). An FP64 lane therefore always runs the same
+// kernel, in a mixed-precision run and in a plain one, and gets the same bits.
+template <int D, bool F32>
 __global__ void __launch_bounds__(kPass1Threads, 4) k_pass1(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
   const EvalItem it = plan.items1[plan.d_off1[D - 1] + blockIdx.x];
   const EvalLane ln = plan.lanes[it.lane];
   if (!lane_active(ln.status)) return;
+  if ((lane_prec(ln) == PREC_FP32) != F32) return;   // the other kernel's lane
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
-  if (DYN && lane_prec(ln) == PREC_FP32)
+  if (F32)
     pass1_body_f32<D>(sp, ln, it.tile, smem);
   else if (!sp.gemm)
     pass1_body<D>(sp, ln, it.tile, smem);   // GEMM problems: k_pass1_gemm
@@ -898,17 +902,18 @@ __global__ void k_energy(EvalPlan plan) {
   if (threadIdx.x == 0) *ln.f = e / P.vol;
 }
 
-template <int D, bool DYN>
+template <int D, bool F32>
 __global__ void __launch_bounds__(kPass2Threads, 4) k_pass2(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
   const EvalItem it = plan.items2[plan.d_off2[D - 1] + blockIdx.x];
   const EvalLane ln = plan.lanes[it.lane];
   if (!lane_active(ln.status) || ln.g == nullptr) return;
+  if ((lane_prec(ln) == PREC_FP32) != F32) return;   // the other kernel's lane
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
   const bool staged = (size_t)sp.M * sizeof(double2) <= kPass2RhoStage;
-  if (DYN && lane_prec(ln) == PREC_FP32) {
+  if (F32) {
     if (staged)
       pass2_body_f32<D, true>(sp, ln, it.tile, plan.split2, smem);
     else
@@ -981,23 +986,23 @@ int pass2_split(long long tiles_at_split1) {
 
 namespace {
 
-template <int D, bool DYN>
+template <int D, bool F32>
 cudaError_t configure_d() {
-  cudaError_t e = cudaFuncSetAttribute(k_pass1<D, DYN>,
+  cudaError_t e = cudaFuncSetAttribute(k_pass1<D, F32>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024 - 1024);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_pass2<D, DYN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_pass2<D, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               227 * 1024 - 1024);
 }
 
-template <int D, bool DYN>
+template <int D, bool F32>
 void launch_d(const EvalPlan& plan, bool pass2, cudaStream_t stream) {
   if (!pass2) {
     const int n = plan.d_off1[D] - plan.d_off1[D - 1];
-    if (n > 0) k_pass1<D, DYN><<<n, kPass1Threads, plan.smem1, stream>>>(plan);
+    if (n > 0) k_pass1<D, F32><<<n, kPass1Threads, plan.smem1, stream>>>(plan);
   } else {
     const int n = plan.d_off2[D] - plan.d_off2[D - 1];
-    if (n > 0) k_pass2<D, DYN><<<n, kPass2Threads, plan.smem2, stream>>>(plan);
+    if (n > 0) k_pass2<D, F32><<<n, kPass2Threads, plan.smem2, stream>>>(plan);
   }
 }
 
@@ -1021,18 +1026,20 @@ cudaError_t eval_configure() {
 namespace {
 
 // The pass kernels of dimension D on stream s (pass 1: per-segment and GEMM forms).
+// FP64 lanes run the F32 = false kernels whatever the plan; a plan that may
+// hold FP32 lanes (dyn_prec) launches the F32 = true kernels as well.
 void launch_dim(const EvalPlan& plan, bool pass2, int D, cudaStream_t s) {
   if (D == 1) {
+    launch_d<1, false>(plan, pass2, s);
     if (plan.dyn_prec) launch_d<1, true>(plan, pass2, s);
-    else launch_d<1, false>(plan, pass2, s);
   } else if (D == 2) {
+    launch_d<2, false>(plan, pass2, s);
     if (plan.dyn_prec) launch_d<2, true>(plan, pass2, s);
-    else launch_d<2, false>(plan, pass2, s);
     const int n = plan.d_offG[2] - plan.d_offG[1];
     if (!pass2 && n > 0) k_pass1_gemm<2><<<n, kGemmThreads, plan.smemG, s>>>(plan);
   } else {
+    launch_d<3, false>(plan, pass2, s);
     if (plan.dyn_prec) launch_d<3, true>(plan, pass2, s);
-    else launch_d<3, false>(plan, pass2, s);
     const int n = plan.d_offG[3] - plan.d_offG[2];
     if (!pass2 && n > 0) k_pass1_gemm<3><<<n, kGemmThreads, plan.smemG, s>>>(plan);
   }

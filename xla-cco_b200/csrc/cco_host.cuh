@@ -90,6 +90,7 @@ enum class Method { Descent, Lbfgs, Flow, Md };
 struct RecordShape {
   Method method = Method::Lbfgs;
   int m = 0, tri_len = 0;
+  int keep_s0 = 0;   // L-BFGS mixed precision: records hold s0
   int waves = 0;   // MD segment runs: tracked waves per lane
 };
 
@@ -99,7 +100,7 @@ inline size_t record_doubles(const RecordShape& R, const cco_problem* p) {
   if (R.method == Method::Descent) n = ds_record_doubles(ld, p->M, p->host.ntile1);
   else if (R.method == Method::Flow) n = fl_record_doubles(ld, p->M, p->host.ntile1);
   else if (R.method == Method::Md) n = md_record_doubles(ld, p->M, p->host.ntile1, R.waves);
-  else n = lb_record_doubles(R.m, R.tri_len, ld, p->M, p->host.ntile1);
+  else n = lb_record_doubles(R.m, R.tri_len, ld, p->M, p->host.ntile1, R.keep_s0);
   return (n + 31) & ~(size_t)31;   // records start on 256-byte boundaries
 }
 
@@ -134,7 +135,7 @@ inline EvalLane eval_lane(const RecordShape& R, const LaneRef& L, const cco_prob
     e.f = v.pf;
     dens = v.dens;
   } else {
-    const LbView v = lb_view(L.rec, R.m, R.tri_len, L.ld);
+    const LbView v = lb_view(L.rec, R.m, R.tri_len, L.ld, R.keep_s0);
     e.s = v.ps;
     e.g = v.pg;
     e.f = v.pf;

@@ -192,7 +192,7 @@ struct EvalPlan {
   int n_itemsG;
   int d_offG[4];
   size_t smemG;
-  int dyn_prec;             // 1: lanes may be FP32 (per-lane dispatch), 0: FP64 kernels only
+  int dyn_prec;             // 1: lanes may be FP32 (the FP32 pass kernels launch too), 0: FP64 only
   int max_d;                // largest d in the plan (template dispatch)
   int red_chunks;           // k-chunks of the reduction: ceil(max M / kReduceChunk)
   int split2;               // pass-2 threads per particle (1, 2, 4 or 8)
@@ -223,10 +223,11 @@ cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream,
 // GEMM pass-1 kernels and the pass-2 kernel that have items, plus reduce and energy.
 inline int eval_kernels(const EvalPlan& p) {
   int n = p.n_lanes > 0 ? 2 : 0;
+  const int per = p.dyn_prec ? 2 : 1;   // FP64 and FP32 pass kernels
   for (int D = 1; D <= 3; ++D) {
-    n += p.d_off1[D] > p.d_off1[D - 1];
+    n += per * (p.d_off1[D] > p.d_off1[D - 1]);
     n += p.d_offG[D] > p.d_offG[D - 1];
-    if (p.want_grad) n += p.d_off2[D] > p.d_off2[D - 1];
+    if (p.want_grad) n += per * (p.d_off2[D] > p.d_off2[D - 1]);
   }
   return n;
 }

@@ -283,7 +283,7 @@ __device__ __forceinline__ int tri(int p, int q) { return q * (q + 1) / 2 + p; }
 struct LbShared {
   LbState L;
   double red[32];
-  int outcome, new_lo, advance, reeval;
+  int outcome, new_lo, advance, reeval, restart;
 };
 
 // Lane vectors and history rows have a padded length ld (a multiple of 4
@@ -297,7 +297,7 @@ __device__ __forceinline__ void st2(double* p, int i, double2 v) {
 }
 
 __device__ __forceinline__ LbView lane_view(const LbArgs& A, const LaneRef& R) {
-  return lb_view(R.rec, A.m, A.tri_len, R.ld);
+  return lb_view(R.rec, A.m, A.tri_len, R.ld, A.keep_s0);
 }
 
 __device__ void lb_record(const LbArgs& A, int lane, const LaneRef& R, LbShared& sh,
@@ -411,10 +411,15 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
     const bool advance = pass_end && !last;
     int status = glob != CCO_STATUS_RUNNING ? glob : CCO_STATUS_RUNNING;
     if (pass_end && last) status = local;
+    // a lane that started in FP32 and ends above the energy tolerance runs
+    // again from s0 in FP64: the plain run of its configuration, bit for bit
+    const bool restart = status != CCO_STATUS_RUNNING && L.mode == 1 && A.energy_tol > 0.0 &&
+                         !(L.f < A.energy_tol);
     L.status = status;
-    if (status != CCO_STATUS_RUNNING) L.t1 = gtimer();
-    sh.advance = advance;
+    if (status != CCO_STATUS_RUNNING && !restart) L.t1 = gtimer();
+    sh.advance = advance && !restart;
     sh.reeval = sw;
+    sh.restart = restart;
     if (sw) {
       // fresh FP64 start at the current point: no history, one re-evaluation
       L.prec = PREC_FP64;
@@ -449,6 +454,27 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
     }
   }
   __syncthreads();
+  if (sh.restart) {
+    // the fresh lane of k_lbfgs_init, keeping the clock and the counts spent
+    for (int e = threadIdx.x; e < 7 * R.ld; e += blockDim.x) v.x[e] = 0.0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < R.nd; e += blockDim.x) v.ps[e] = v.s0[e];
+    if (threadIdx.x == 0) {
+      LbState F = {};
+      F.phase = PH_INIT;
+      F.status = CCO_STATUS_RUNNING;
+      F.R = A.rescales[0];
+      F.prec = PREC_FP64;
+      F.mode = 2;
+      F.t0 = L.t0;
+      F.n_fp32 = L.n_fp32;
+      F.evals_prior = L.evals_prior + L.n_evals;
+      L = F;
+      if (A.traj_count) A.traj_count[R.idx] = 0;   // the trajectory of the run that counts
+    }
+    __syncthreads();
+    return;
+  }
   lb_record(A, lane, R, sh, s);
   if (threadIdx.x == 0 && L.status == CCO_STATUS_RUNNING && L.phase != PH_REEVAL)
     L.need_dir = 1;
@@ -462,12 +488,16 @@ __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
   for (int e = threadIdx.x; e < 7 * R.ld; e += blockDim.x) v.x[e] = 0.0;
   __syncthreads();
   for (int e = threadIdx.x; e < R.nd; e += blockDim.x) v.ps[e] = s0[R.soff + e];
+  if (v.s0)
+    for (int e = threadIdx.x; e < R.nd; e += blockDim.x) v.s0[e] = s0[R.soff + e];
   if (threadIdx.x == 0) {
     LbState L = {};
     L.phase = PH_INIT;
     L.status = CCO_STATUS_RUNNING;
     L.R = A.rescales[0];
-    L.prec = A.prec0;
+    // mixed precision starts lanes of d >= 2 (N d > N) in FP32
+    L.prec = (A.prec0 == PREC_FP32 && R.nd > R.n) ? PREC_FP32 : PREC_FP64;
+    L.mode = L.prec == PREC_FP32 ? 1 : 0;
     L.t0 = gtimer();
     *v.st = L;
     if (A.traj_count) A.traj_count[R.idx] = 0;
@@ -912,7 +942,7 @@ __global__ void k_lbfgs_finalize(LbArgs A, double* s_out, double* e_out, double*
     const LbState L = *v.st;
     e_out[lane] = L.f;
     gn_out[lane] = sqrt(ss) * L.R;
-    ne_out[lane] = L.n_evals;
+    ne_out[lane] = L.n_evals + L.evals_prior;
     ni_out[lane] = L.it;
     st_out[lane] = L.status;
     if (lat_out) lat_out[lane] = L.t1 - L.t0;

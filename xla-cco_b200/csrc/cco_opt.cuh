@@ -14,12 +14,18 @@ namespace cco {
 
 enum : int { PH_INIT = 0, PH_ITER = 1, PH_EXPAND = 1, PH_ZOOM = 2, PH_REEVAL = 3 };
 
-// Mixed-precision L-BFGS: a lane starts with FP32 evaluations and switches to
-// FP64 for good once its energy falls below kFp32SwitchPerParticle * N, or
-// when an FP32 line search fails or stagnates (the FP32 energy is too coarse
-// to continue). At the switch the history is cleared and the current point is
-// evaluated again in FP64 before the next direction, so every energy the line
-// search compares and the final judgement come from FP64 evaluations.
+// Mixed-precision L-BFGS: a lane of a d >= 2 problem starts with FP32
+// evaluations and switches to FP64 for good once its energy falls below
+// kFp32SwitchPerParticle * N, or on any outcome that would stop it (the FP32
+// energy is too coarse to judge). At the switch the history is cleared and the
+// current point is evaluated again in FP64 before the next direction, so every
+// energy the line search compares and the final judgement come from FP64
+// evaluations. A lane that nevertheless ends above the energy tolerance is
+// restarted from its initial positions in FP64 and then repeats, bit for bit,
+// the plain FP64 run of the same configuration: the mixed form's success mask
+// equals the plain one's wherever plain FP64 fails. Lanes of 1-D problems run
+// FP64 throughout (their slow, marginal approach to 1e-20 is where an FP32
+// prefix changed outcomes).
 constexpr double kFp32SwitchPerParticle = 1e-6;
 
 // One lane of a launch.
@@ -96,8 +102,11 @@ struct LbState {
   int32_t phase, ls_steps, pass_idx, hk, hhead, have_lo, newpair, need_dir;
   int32_t prec;           // evaluation arithmetic (PREC_FP64 / PREC_FP32)
   int32_t n_fp32;         // evaluations done in FP32
+  int32_t mode;           // 0: FP64 lane; 1: started in FP32; 2: restarted in FP64 from s0
+  int32_t pad_;
+  int64_t evals_prior;    // evaluations before a restart (counted in the result)
 };
-constexpr int kLbHead = 32;   // LbState (28 doubles) and pf at [31]
+constexpr int kLbHead = 32;   // LbState (30 doubles) and pf at [31]
 static_assert(sizeof(LbState) <= (kLbHead - 1) * sizeof(double), "LbState outgrew its slot");
 static_assert(sizeof(DsState) <= (kDsHead - 1) * sizeof(double), "DsState outgrew its slot");
 
@@ -115,15 +124,19 @@ __host__ __device__ __forceinline__ size_t lb_scal_len(int m, int ld) {
 // Record: [0, 32) LbState, pf at [31]; SY (m m, row = newer slot), YY (m m);
 // the packed triangles of the scalar kernel (tri_len = m (m + 1) when
 // they do not fit in shared memory, else 0); the scalar row; x, s, g, dir, glo, ps, pg (ld each); the
-// history rings S and Y (m ld each); the evaluation scratch.
+// history rings S and Y (m ld each); s0 (ld, mixed precision only); the evaluation scratch.
 struct LbView {
   LbState* st;
   double *pf, *SY, *YY, *tri, *scal;
   double *x, *s, *g, *dir, *glo, *ps, *pg, *Sh, *Yh;
+  double* s0;             // the lane's initial positions (mixed precision only, else null)
   double2* dens;
 };
 
-__host__ __device__ __forceinline__ LbView lb_view(double* rec, int m, int tri_len, int ld) {
+// keep_s0: the record holds a copy of the lane's initial positions (ld
+// doubles after the history), which mixed-precision lanes restart from.
+__host__ __device__ __forceinline__ LbView lb_view(double* rec, int m, int tri_len, int ld,
+                                                   int keep_s0 = 0) {
   LbView v;
   const size_t mm = (size_t)m * m;
   v.st = reinterpret_cast<LbState*>(rec);
@@ -141,14 +154,15 @@ __host__ __device__ __forceinline__ LbView lb_view(double* rec, int m, int tri_l
   v.pg = v.x + 6 * (size_t)ld;
   v.Sh = v.x + 7 * (size_t)ld;
   v.Yh = v.Sh + (size_t)m * ld;
-  v.dens = reinterpret_cast<double2*>(v.Yh + (size_t)m * ld);
+  v.s0 = keep_s0 ? v.Yh + (size_t)m * ld : nullptr;
+  v.dens = reinterpret_cast<double2*>(v.Yh + (size_t)(m + (keep_s0 ? 1 : 0)) * ld);
   return v;
 }
 
 __host__ __device__ __forceinline__ size_t lb_record_doubles(int m, int tri_len, int ld, int M,
-                                                             int nt1) {
-  return kLbHead + 2 * (size_t)m * m + tri_len + lb_scal_len(m, ld) + (7 + 2 * (size_t)m) * ld +
-         2 * (size_t)M * (2 + nt1);
+                                                             int nt1, int keep_s0 = 0) {
+  return kLbHead + 2 * (size_t)m * m + tri_len + lb_scal_len(m, ld) +
+         (7 + 2 * (size_t)m + (keep_s0 ? 1 : 0)) * ld + 2 * (size_t)M * (2 + nt1);
 }
 
 struct LbArgs {
@@ -158,7 +172,8 @@ struct LbArgs {
   double energy_tol, grad_tol;
   int64_t budget, patience, max_ls;
   int64_t rec_every, rec_cap;
-  int prec0;              // PREC_FP32: lanes start in FP32 (mixed precision)
+  int prec0;              // PREC_FP32: lanes of d >= 2 start in FP32 (mixed precision)
+  int keep_s0;            // records hold s0 (mixed precision: restart of a failed lane)
   int nblkB;              // grid width of pass B (max over the lanes)
   size_t smem_tri;        // 0: triangles in the record (global memory)
   double *traj_s, *traj_e, *traj_step;

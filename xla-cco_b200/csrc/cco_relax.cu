@@ -639,6 +639,7 @@ int lbfgs_args(const cco_lbfgs_settings* cfg, LbArgs* A, RecordShape* shape) {
   A->rec_every = 1;
   A->rec_cap = 0;
   A->prec0 = cfg->precision == 1 ? PREC_FP32 : PREC_FP64;
+  A->keep_s0 = cfg->precision == 1 ? 1 : 0;
   const size_t tri_bytes = lbfgs_update_smem(m);
   const bool in_smem = tri_bytes <= 200 * 1024;
   A->smem_tri = in_smem ? tri_bytes : 0;
@@ -653,6 +654,7 @@ int lbfgs_args(const cco_lbfgs_settings* cfg, LbArgs* A, RecordShape* shape) {
   shape->method = Method::Lbfgs;
   shape->m = m;
   shape->tri_len = A->tri_len;
+  shape->keep_s0 = A->keep_s0;
   return CCO_OK;
 }
 

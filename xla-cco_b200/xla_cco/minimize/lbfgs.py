@@ -55,9 +55,12 @@ class LBFGSSettings:
     max_linesearch_steps: int = 30
     record_every: int = 0
     max_records: int = 0
-    # Not in the reference: "mixed" evaluates in FP32 (FP64-seeded tables,
-    # compensated FP32 density sums, FP32 back-projection) while a lane's
-    # energy is above 1e-6 N, then switches that lane to FP64 for good.
+    # Not in the reference: "mixed" evaluates a lane of a d >= 2 problem in
+    # FP32 (FP64-seeded tables, compensated FP32 density sums, FP32
+    # back-projection) while its energy is above 1e-6 N, then in FP64 for
+    # good; every status is judged in FP64. A mixed lane that ends above
+    # energy_tol (> 0) runs again from its initial positions in plain FP64, so
+    # it returns exactly the plain result; 1-D lanes run FP64 throughout.
     precision: str = "fp64"
 
 
