@@ -952,18 +952,38 @@ def run_cli(args) -> None:
 
 
 def run_profile(args) -> None:
-    """Kernel-level profiling driver (run under ncu): no timing, no JSON."""
+    """Kernel-level profiling driver (run under ncu): no timing, no JSON.
+    --profile-shape N,d,chi profiles another system than the headline one.
+    Without ncu it prints the device time per evaluation (eval mode)."""
     import torch
 
     from xla_cco import LBFGSSettings
     from xla_cco.minimize import relax_device
+    from xla_cco.workloads import energy_for
 
-    _, _, energy = workload()
-    s0 = np.random.default_rng(SEED).uniform(size=(args.batch, N_PART, DIM))
+    if args.profile_shape:
+        n_s, d_s, chi_s = args.profile_shape.split(",")
+        n, d = int(n_s), int(d_s)
+        energy = energy_for(n, d, float(chi_s))
+    else:
+        n, d = N_PART, DIM
+        _, _, energy = workload()
+    s0 = np.random.default_rng(SEED).uniform(size=(args.batch, n, d))
     s_dev = torch.from_numpy(s0).cuda()
     if args.profile == "eval":
+        energy.evaluate(s_dev)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         for _ in range(args.reps):
             energy.evaluate(s_dev)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.reps
+        m = int(energy._rows.size)
+        tf = args.batch * n * m * F_PAIR[d] / (ms * 1e-3) / 1e12
+        print(json.dumps({"profile": "eval", "n": n, "d": d, "m": m, "batch": args.batch,
+                          "ms_per_eval": ms, "tflops": tf}), flush=True)
     else:
         for _ in range(args.reps):
             relax_device(energy, s_dev, LBFGSSettings(energy_tol=TOL))
@@ -981,6 +1001,7 @@ def main() -> None:
     ap.add_argument("--profile", choices=["eval", "relax"], default=None,
                     help="profiling driver for ncu: run the kernels only")  # fmt: skip
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--profile-shape", default=None, help="N,d,chi of the profiled system")
     ap.add_argument("--md-lanes", type=int, default=64)
     ap.add_argument("--md-steps", type=int, default=2000)
     ap.add_argument("--workload", choices=["batch", "descent", "mixed", "serve", "precision", "md", "analysis",
