@@ -370,7 +370,9 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     P.sl2 = sl;
   }
 
-  const size_t smem1 = eval_smem1(P), smem2 = std::max(eval_smem2(P, 1), eval_smem2(P, 8));
+  const size_t smem1 = eval_smem1(P);
+  const size_t smem2 = std::max(std::max(eval_smem2(P, 1), eval_smem2(P, 8)),
+                                std::max(eval_smem2(P, 1, true), eval_smem2(P, 8, true)));
   if (smem1 > 220 * 1024 || smem2 > 220 * 1024)
     return fail(CCO_ERR_ARG, "k-set phase tables too large for shared memory (%d / %d rows)",
                 P.t1.nrows, P.t2.nrows);
@@ -564,6 +566,7 @@ struct EvalWS {
     plan.max_d = p->d;
     plan.smem1 = p->smem1;
     plan.smem2 = eval_smem2(p->host, split);
+    plan.smem2_f32 = eval_smem2(p->host, split, true);
     plan.split2 = split;
     plan.red_chunks = reduce_chunks(p->M);
     plan.want_grad = g != nullptr;

@@ -367,6 +367,109 @@ __device__ void pass2_body(const ProbDev& P, const EvalLane& ln, int tile, int s
   }
 }
 
+// ------------------------------------------------------------ 1-D pass 2
+// A 1-D k-set is one run n = n_min, n_min + 1, ... (1..M without K1), cut into
+// segments of <= kSeg2Len rows. Each thread seeds a segment's phase z_j^n0
+// directly (one exactly reduced sincospi per segment and particle, ~2% of the
+// row work at M = 2000) and walks the rows by products with z_j, so the pass
+// needs no phase tables and the whole weighted density is staged in shared
+// memory (broadcast reads) for M <= kPass2RhoStage1D / 16.
+__device__ __forceinline__ void pass2_slice_1d(const ProbDev& P, const double2* __restrict__ rw,
+                                               double sj, double2 z, int q, int sl, double& G) {
+  const int nseg = P.nseg2;
+  G = 0.0;
+  for (int sg = 2 * q; sg < nseg; sg += 2 * sl) {
+    const SegHdr hA = P.seg2[sg];
+    const SegHdr hB = P.seg2[min(sg + 1, nseg - 1)];
+    double sn, cs;
+    sincos_2pi_ms((double)hA.n[0], sj, &sn, &cs);
+    double2 pA = make_double2(cs, sn);
+    sincos_2pi_ms((double)hB.n[0], sj, &sn, &cs);
+    double2 pB = make_double2(cs, sn);
+    double SA = 0.0, TA = 0.0, SB = 0.0, TB = 0.0;
+    const double2* rA = rw + hA.kstart;
+    const double2* rB = rw + hB.kstart;
+    const int la = hA.len, lb = (sg + 1 < nseg) ? hB.len : 0;
+    int i = 0;
+    double di = 0.0;
+    for (; i + 2 <= lb; i += 2) {
+      const double2 a0 = rA[i], a1 = rA[i + 1];
+      const double2 b0 = rB[i], b1 = rB[i + 1];
+      bp_step(a0, pA, z, di, SA, TA);
+      bp_step(b0, pB, z, di, SB, TB);
+      bp_step(a1, pA, z, di + 1.0, SA, TA);
+      bp_step(b1, pB, z, di + 1.0, SB, TB);
+      di += 2.0;
+    }
+    if (i < lb) {
+      bp_step(rA[i], pA, z, di, SA, TA);
+      bp_step(rB[i], pB, z, di, SB, TB);
+      ++i;
+      di += 1.0;
+    }
+    for (; i + 2 <= la; i += 2) {
+      const double2 a0 = rA[i], a1 = rA[i + 1];
+      bp_step(a0, pA, z, di, SA, TA);
+      bp_step(a1, pA, z, di + 1.0, SA, TA);
+      di += 2.0;
+    }
+    if (i < la) bp_step(rA[i], pA, z, di, SA, TA);
+    G += ((double)hA.n[0] * SA + TA) + ((double)hB.n[0] * SB + TB);
+  }
+}
+
+// Pass 2 of one particle tile of a 1-D problem (FP64): the slices and their
+// tree sum as in pass2_body, the phases from pass2_slice_1d.
+template <bool STAGED>
+__device__ void pass2_body_1d(const ProbDev& P, const EvalLane& ln, int tile, int split,
+                              double2* smem) {
+  const int tw = kPass2Tile / split;
+  const int j0 = tile * tw;
+  const int nj = min(tw, P.N - j0);
+  const double2* __restrict__ rw = ln.rhow;
+  double2* after = smem;
+  if (STAGED) {
+    for (int k = threadIdx.x; k < P.M; k += blockDim.x) after[k] = rw[k];
+    rw = after;
+    after += P.M;
+  }
+  double* comb = reinterpret_cast<double*>(after);   // [split][tw]
+  __syncthreads();
+  const int j = threadIdx.x % tw, qp = threadIdx.x / tw;
+  const double sj = (j < nj) ? ln.s[j0 + j] : 0.0;
+  double sn, cs;
+  sincospi(2.0 * sj, &sn, &cs);
+  const double2 z = make_double2(cs, sn);
+  const int sl = P.sl2;
+  const int per = sl > split ? sl / split : 1;
+  const int nblk = sl / per;
+  if (qp < nblk) {
+    Pairwise<1> acc;
+    for (int q = qp * per; q < (qp + 1) * per; ++q) {
+      double G[1];
+      pass2_slice_1d(P, rw, sj, z, q, sl, G[0]);
+      acc.push(G);
+    }
+    double G[1];
+    acc.total(G);
+    if (nblk > 1) comb[(size_t)qp * tw + j] = G[0];
+    else if (j < nj) ln.g[j0 + j] = P.gpref * G[0];
+  }
+  if (nblk > 1) {
+    __syncthreads();
+    if (qp == 0 && j < nj) {
+      Pairwise<1> acc;
+      for (int b = 0; b < nblk; ++b) {
+        double G[1] = {comb[(size_t)b * tw + j]};
+        acc.push(G);
+      }
+      double G[1];
+      acc.total(G);
+      ln.g[j0 + j] = P.gpref * G[0];
+    }
+  }
+}
+
 // ------------------------------------------------------------ FP32 bodies
 // Kahan-compensated FP32 complex accumulation: s holds the sum, c minus the
 // low-order part lost so far (value = s - c).
@@ -912,6 +1015,13 @@ __global__ void __launch_bounds__(kPass2Threads, 4) k_pass2(EvalPlan plan) {
   if ((lane_prec(ln) == PREC_FP32) != F32) return;   // the other kernel's lane
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
+  if (D == 1 && !F32) {
+    if ((size_t)sp.M * sizeof(double2) <= kPass2RhoStage1D)
+      pass2_body_1d<true>(sp, ln, it.tile, plan.split2, smem);
+    else
+      pass2_body_1d<false>(sp, ln, it.tile, plan.split2, smem);
+    return;
+  }
   const bool staged = (size_t)sp.M * sizeof(double2) <= kPass2RhoStage;
   if (F32) {
     if (staged)
@@ -962,7 +1072,12 @@ size_t eval_smemG(const ProbDev& p) {
          sizeof(double2);
 }
 
-size_t eval_smem2(const ProbDev& p, int split) {
+size_t eval_smem2(const ProbDev& p, int split, bool f32) {
+  if (p.d == 1 && !f32) {   // pass2_body_1d: the staged density and the slice combine
+    const size_t rho = (size_t)p.M * sizeof(double2);
+    const size_t comb = split > 1 ? (size_t)kPass2Tile * sizeof(double) : 0;
+    return (rho <= kPass2RhoStage1D ? rho : 0) + comb;
+  }
   const size_t rho = (size_t)p.M * sizeof(double2);
   const size_t comb = split > 1 ? (size_t)kPass2Tile * p.d * sizeof(double) : 0;
   return (size_t)p.t2.nrows * (kPass2Tile / split) * sizeof(double2) +
@@ -1002,7 +1117,7 @@ void launch_d(const EvalPlan& plan, bool pass2, cudaStream_t stream) {
     if (n > 0) k_pass1<D, F32><<<n, kPass1Threads, plan.smem1, stream>>>(plan);
   } else {
     const int n = plan.d_off2[D] - plan.d_off2[D - 1];
-    if (n > 0) k_pass2<D, F32><<<n, kPass2Threads, plan.smem2, stream>>>(plan);
+    if (n > 0) k_pass2<D, F32><<<n, kPass2Threads, F32 ? plan.smem2_f32 : plan.smem2, stream>>>(plan);
   }
 }
 

@@ -169,7 +169,7 @@ struct EvalSet {
     std::vector<ProbDev> pv;
     std::vector<EvalLane> lv;
     std::vector<EvalItem> g1[3], g2[3], gG[3];   // items grouped by d
-    size_t smem1 = 0, smem2 = 0, smemG = 0;
+    size_t smem1 = 0, smem2 = 0, smem2f = 0, smemG = 0;
     int max_d = 1, max_m = 1;
     for (int i = lo; i < hi; ++i) {
       const cco_problem* p = probs_of[i];
@@ -180,6 +180,7 @@ struct EvalSet {
         pv.push_back(p->host);
         smem1 = std::max(smem1, p->smem1);
         smem2 = std::max(smem2, eval_smem2(p->host, split));
+        smem2f = std::max(smem2f, eval_smem2(p->host, split, true));
         smemG = std::max(smemG, p->smemG);
         max_d = std::max(max_d, p->d);
         max_m = std::max(max_m, p->M);
@@ -225,6 +226,7 @@ struct EvalSet {
     plan.max_d = max_d;
     plan.smem1 = smem1;
     plan.smem2 = smem2;
+    plan.smem2_f32 = smem2f;
     plan.red_chunks = reduce_chunks(max_m);
     plan.split2 = split;
     plan.want_grad = true;

@@ -28,6 +28,7 @@ constexpr int kMaxLevels = 3;
 constexpr size_t kPass1TableBudget = 56 * 1024;   // bytes of pass-1 tables per CTA
 constexpr size_t kPass2TableBudget = 44 * 1024;   // bytes of pass-2 tables per CTA
 constexpr size_t kPass2RhoStage = 24 * 1024;      // density staged in pass-2 smem up to this
+constexpr size_t kPass2RhoStage1D = 64 * 1024;    // the same for 1-D problems (no phase tables)
 
 // One segment: rows kstart .. kstart+len-1 (run order) share the prefix
 // n_0..n_{d-2}; the last axis runs n_{d-1} = n[d-1] + i.
@@ -196,7 +197,8 @@ struct EvalPlan {
   int max_d;                // largest d in the plan (template dispatch)
   int red_chunks;           // k-chunks of the reduction: ceil(max M / kReduceChunk)
   int split2;               // pass-2 threads per particle (1, 2, 4 or 8)
-  size_t smem1, smem2;      // dynamic shared memory of pass 1 / pass 2
+  size_t smem1, smem2;      // dynamic shared memory of pass 1 / pass 2 (FP64 kernels)
+  size_t smem2_f32;         // pass 2, FP32 kernels
   bool want_grad;
 };
 
@@ -242,7 +244,9 @@ inline int eval_dims(const EvalPlan& p) {
 }
 size_t eval_smem1(const ProbDev& p);
 size_t eval_smemG(const ProbDev& p);   // GEMM pass 1 (0 when the problem has none)
-size_t eval_smem2(const ProbDev& p, int split);
+// Pass-2 dynamic shared memory at `split` for the FP64 kernels, or with
+// f32 for the FP32 ones (which keep phase tables for 1-D problems too).
+size_t eval_smem2(const ProbDev& p, int split, bool f32 = false);
 // Pass-2 tiles of one configuration when `split` threads share a particle.
 int pass2_tiles(const ProbDev& p, int split);
 // Threads per particle in pass 2 for a launch whose configurations have

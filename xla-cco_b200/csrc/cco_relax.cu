@@ -393,13 +393,10 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
         refs.push_back(C.refs[i]);
         probs.push_back(C.probs[i]);
       }
-    // drain the graphs still in flight on the old table first: their snapshots
-    // describe the old row order
-    while (checked < launched) {
-      const int s2 = checked % kSlots;
-      CCO_CUDA(cudaEventSynchronize(ev[s2]));
-      ++checked;
-    }
+    // The graphs still in flight on the old table keep running while the new
+    // plan is captured: stream order puts the new graphs after them, the old
+    // plan's buffers are freed stream-ordered, and their status snapshots
+    // (older version, old row order) only feed the all-finished test.
     C.refs.swap(refs);
     C.probs.swap(probs);
     P.release(st);
