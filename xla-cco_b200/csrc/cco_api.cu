@@ -363,10 +363,11 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   P.nseg1 = (int)s1.size();
   P.nseg2 = (int)s2.size();
   {
-    // logical pass-2 slices: about two segment pairs each, at most 8
+    // logical pass-2 slices: at least one segment pair each, at most 8 (a
+    // launch of few lanes spreads a particle's slices over up to 8 threads)
     const int npairs = (P.nseg2 + 1) / 2;
     int sl = 1;
-    while (sl < 8 && 4 * sl <= npairs) sl *= 2;
+    while (sl < 8 && 2 * sl <= npairs) sl *= 2;
     P.sl2 = sl;
   }
 
