@@ -307,3 +307,25 @@ def test_lbfgs_success_mask_matches_oracle(chi):
     ref = oracle.relax_batch("lbfgs", s0, ks.n, ks.weights, box.volume, cfg)
     np.testing.assert_array_equal(dev.energy < 1e-20, ref["energy"] < 1e-20)
     assert np.all(dev.status != STATUS_LINESEARCH_FAIL) or np.all(dev.energy < 1e-20)
+
+
+def test_small_descent_lanes_run_in_one_persistent_launch():
+    """Lanes of a problem small enough for one CTA (here d=3 N=100 chi=0.05,
+    M=13) run their whole descent in one launch: no graph ticks, a handful of
+    launches, and the same bits alone and in a batch."""
+    import torch
+
+    from xla_cco.minimize import relax_device
+
+    box = cubic_box(100, 3)
+    ks = enumerate_kvectors(box.basis, 0.0, k_outer_from_ka(ka_from_chi(0.05, 0.05, 3), 0.05, 3))
+    en = make_stealthy_energy(box, ks)
+    s0 = torch.from_numpy(np.random.default_rng(1).uniform(size=(4, 100, 3))).cuda()
+    st = DescentSettings(grow=2.0, max_evals=20_000, energy_tol=1e-20)
+    out = relax_device(en, s0, st)
+    assert out["ticks"] == 0 and out["launches"] <= 5, (out["ticks"], out["launches"])
+    assert (out["energy"] < 1e-20).all()
+    for i in range(4):
+        one = relax_device(en, s0[i:i + 1].contiguous(), st)
+        for k in ("s", "energy", "n_evals", "n_iters", "status"):
+            assert torch.equal(one[k][0], out[k][i]), (i, k)

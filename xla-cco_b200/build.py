@@ -24,8 +24,9 @@ OUT_DIR = PKG_ROOT / "xla_cco" / "_lib"
 LIB = OUT_DIR / "libcco.so"
 
 SOURCES = ["cco_api.cu", "cco_eval.cu", "cco_opt.cu", "cco_relax.cu", "cco_serve.cu", "cco_flow.cu", "cco_md.cu", "cco_pairs.cu",
-           "cco_hessian.cu", "cco_stepper.cu"]
-HEADERS = ["cco_internal.cuh", "cco_opt.cuh", "cco_host.cuh", "cco_flow.cuh", "cco_md.cuh"]
+           "cco_hessian.cu", "cco_stepper.cu", "cco_persist.cu"]
+HEADERS = ["cco_internal.cuh", "cco_opt.cuh", "cco_host.cuh", "cco_flow.cuh", "cco_md.cuh",
+           "cco_eval_bodies.cuh", "cco_opt_bodies.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

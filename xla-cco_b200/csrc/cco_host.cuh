@@ -283,6 +283,20 @@ struct LaneTable {
   void release(cudaStream_t st);
 };
 
+// ------------------------------------------------------------ persistent lanes
+// Problems small enough that one CTA evaluates them in a few microseconds run
+// their whole descent in one persistent launch (cco_persist.cu) instead of
+// graph ticks. The choice depends on the problem alone, so a lane gives the
+// same bits alone and in any batch.
+constexpr double kPersistMaxFlops = 2.5e5;          // N M F_pair(d) per evaluation
+constexpr size_t kPersistMaxSmem = 200 * 1024;      // dynamic shared memory of the launch
+bool persist_eligible(const cco_problem* p);
+size_t persist_smem(const cco_problem* p);
+// One launch per dimension present (bit d-1 of `dims`) over a.B lanes;
+// *d_overrun is set to 1 if a lane reached max_ticks while still RUNNING.
+cudaError_t persist_descent(const DescentArgs& a, const EvalPlan& plan, size_t smem, int dims,
+                            int64_t max_ticks, int* d_overrun, cudaStream_t st);
+
 // One schedule of a lane table captured as an executable graph of
 // sch.graph_ticks ticks.
 struct TickPlan {

@@ -494,6 +494,91 @@ int make_table(cco_problem* const* probs, int B, const RecordShape& shape, int64
   return T->upload_refs(st);
 }
 
+// The descent lanes of a table split by problem size: the small ones run one
+// persistent launch (on a side stream when graph ticks run beside it), the
+// others form `large`, the table of the graph driver.
+struct PersistRun {
+  LaneTable large;
+  EvalSet ev;
+  LaneRef* d_small = nullptr;
+  int* d_over = nullptr;
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  int64_t launches = 0;
+  bool any = false;
+
+  int start(const LaneTable& T, cudaStream_t st, int64_t max_ticks) {
+    large.shape = T.shape;
+    large.ds = T.ds;
+    std::vector<LaneRef> small;
+    std::vector<const cco_problem*> sprobs;
+    size_t smem = 0;
+    int dims = 0;
+    for (size_t i = 0; i < T.refs.size(); ++i) {
+      const cco_problem* p = T.probs[i];
+      if (persist_eligible(p)) {
+        small.push_back(T.refs[i]);
+        sprobs.push_back(p);
+        smem = std::max(smem, persist_smem(p));
+        dims |= 1 << (p->d - 1);
+      } else {
+        large.refs.push_back(T.refs[i]);
+        large.probs.push_back(p);
+      }
+    }
+    if (!large.refs.empty()) {
+      const int rc = large.upload_refs(st);
+      if (rc != CCO_OK) return rc;
+    }
+    if (small.empty()) return CCO_OK;
+    any = true;
+    CCO_CUDA(upload(&d_small, small, st));
+    CCO_CUDA(ev.build(T.shape, small, sprobs, 0, (int)small.size(), st));
+    CCO_CUDA(pool_alloc(&d_over, sizeof(int), st));
+    CCO_CUDA(cudaMemsetAsync(d_over, 0, sizeof(int), st));
+    DescentArgs a = T.ds;
+    a.B = (int)small.size();
+    a.lanes = d_small;
+    cudaStream_t run = st;
+    if (!large.refs.empty()) {   // beside the graph ticks of the large lanes
+      CCO_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+      CCO_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+      CCO_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+      CCO_CUDA(cudaEventRecord(fork, st));
+      CCO_CUDA(cudaStreamWaitEvent(side, fork, 0));
+      run = side;
+    }
+    CCO_CUDA(persist_descent(a, ev.plan, smem, dims, max_ticks, d_over, run));
+    launches = __builtin_popcount(dims);
+    if (side) CCO_CUDA(cudaEventRecord(join, side));
+    return CCO_OK;
+  }
+
+  // Joins the persistent launch into st; CCO_ERR_ROUNDS if a lane overran.
+  int finish(cudaStream_t st) {
+    if (!any) return CCO_OK;
+    if (side) CCO_CUDA(cudaStreamWaitEvent(st, join, 0));
+    int over = 0;
+    CCO_CUDA(cudaMemcpyAsync(&over, d_over, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CCO_CUDA(cudaStreamSynchronize(st));
+    if (over) return fail(CCO_ERR_ROUNDS, "relax did not finish within the round bound");
+    return CCO_OK;
+  }
+
+  void release(cudaStream_t st) {
+    if (side && join) cudaStreamWaitEvent(st, join, 0);
+    ev.release(st);
+    large.release(st);
+    if (d_small) cudaFreeAsync(d_small, st);
+    if (d_over) cudaFreeAsync(d_over, st);
+    if (side) cudaStreamDestroy(side);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    side = nullptr;
+    fork = join = nullptr;
+  }
+};
+
 int relax_descent_set(cco_problem* const* probs, int B, cudaStream_t st, const double* s0,
                       const cco_descent_settings* cfg, cco_relax_out* out) {
   if (!cfg || !s0) return fail(CCO_ERR_ARG, "null argument");
@@ -534,16 +619,20 @@ int relax_descent_set(cco_problem* const* probs, int B, cudaStream_t st, const d
   CCO_CUDA(descent_init(a, s0, st));
   const int64_t max_ticks = 1 + a.max_iters + 4 * (kInflight + 1) * 32;
   RunStats rs;
-  rc = run_lane_table(T, st, max_ticks, &rs);
+  PersistRun pr;
+  rc = pr.start(T, st, max_ticks);
+  if (rc == CCO_OK && !pr.large.refs.empty()) rc = run_lane_table(pr.large, st, max_ticks, &rs);
+  if (rc == CCO_OK) rc = pr.finish(st);
   if (rc == CCO_OK) {
     cudaError_t e = descent_finalize(a, out->s, out->energy, out->grad_norm, out->n_evals,
                                      out->n_iters, out->status, out->latency_ns, st);
     if (e != cudaSuccess) rc = cuda_fail(e, "descent_finalize");
   }
   out->ticks = rs.ticks;
-  out->launches = rs.launches + 3;
+  out->launches = rs.launches + 3 + pr.launches;
   out->branches = rs.schedule.branches;
   out->graph_ticks = rs.schedule.graph_ticks;
+  pr.release(st);
   T.release(st);
   cudaFreeAsync(records, st);
   cudaError_t e = cudaStreamSynchronize(st);
