@@ -339,6 +339,12 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
   TickPlan P;
   P.method = T.shape.method;
   int version = 0;
+  // An L-BFGS table is tuned only once its lanes' histories have filled: in
+  // the first ticks the HBM-bound update is short, so schedules that overlap
+  // it with the FP64-bound evaluation of another branch cannot show their
+  // gain. Until then it runs the default schedule.
+  constexpr int64_t kTuneAfterTicks = 128;
+  bool defer_tune = false;
 
   // (re)start on table C: schedule, graph
   auto start = [&]() -> int {
@@ -357,9 +363,12 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
       if (force_br > 0) s.branches = force_br;
       if (force_gt > 0) s.graph_ticks = force_gt;
     } else if (!schedule_cached(C.probs, C.shape.method, &s) && tune) {
-      r = tune_schedule(C, st, max_ticks, &ticks, &launches, &s);
-      if (r != CCO_OK) return r;
-      schedule_store(C.probs, C.shape.method, s);
+      defer_tune = C.shape.method == Method::Lbfgs && ticks < kTuneAfterTicks;
+      if (!defer_tune) {
+        r = tune_schedule(C, st, max_ticks, &ticks, &launches, &s);
+        if (r != CCO_OK) return r;
+        schedule_store(C.probs, C.shape.method, s);
+      }
     }
     chosen = s;
     if (!first_set) {
@@ -420,6 +429,10 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
     rows[slot] = n;
     ++launched;
     if (e == cudaSuccess && launched - checked > kInflight) rc = land();
+    if (rc == CCO_OK && e == cudaSuccess && !done && defer_tune && ticks >= kTuneAfterTicks) {
+      P.release(st);   // the deferred tuning, on the same table
+      rc = start();
+    }
   }
   // drain the launches still in flight, oldest first
   while (rc == CCO_OK && e == cudaSuccess && !done && checked < launched) rc = land();
