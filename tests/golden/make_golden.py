@@ -1,6 +1,6 @@
 """Generate the golden fixtures in tests/golden/ from the reference checkout.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>   (or XLA_CCO_REFERENCE=<path>)
 
 Only the reference's NumPy-only modules are imported (by file path, without
 its package __init__, which needs JAX): src/xla_cco/kvectors.py,
@@ -14,6 +14,7 @@ are committed; tests never read the reference checkout.
 from __future__ import annotations
 
 import argparse
+import os
 import ast
 import importlib.util
 import json
@@ -44,7 +45,9 @@ def _cpp_descent_fn(ref: Path, oracle_mod):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("XLA_CCO_REFERENCE"),
+                    required="XLA_CCO_REFERENCE" not in os.environ,
+                    help="the reference checkout (default: $XLA_CCO_REFERENCE)")
     ref = Path(ap.parse_args().ref)
     kv = _load(ref / "src/xla_cco/kvectors.py", "ref_kvectors")
     orc = _load(ref / "tests/oracle.py", "ref_oracle")

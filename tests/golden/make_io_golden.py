@@ -1,6 +1,6 @@
 """Generate tests/golden/io_golden.{npz,json} from the reference checkout.
 
-    python tests/golden/make_io_golden.py [--ref /root/reference]
+    python tests/golden/make_io_golden.py --ref <reference checkout>   (or XLA_CCO_REFERENCE=<path>)
 
 Covers the callers either side of the relaxation path: the ConfigPack format,
 the C++ function-table writer, the isotropic S(k) k-set and binning, and the
@@ -22,6 +22,7 @@ are stored, not the files. Tests never read the reference checkout.
 from __future__ import annotations
 
 import argparse
+import os
 import ast
 import hashlib
 import importlib.util
@@ -61,7 +62,9 @@ def _names(n: int, seed: int) -> tuple:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("XLA_CCO_REFERENCE"),
+                    required="XLA_CCO_REFERENCE" not in os.environ,
+                    help="the reference checkout (default: $XLA_CCO_REFERENCE)")
     ref = Path(ap.parse_args().ref)
     cp = _load(ref / "src/xla_cco/io/configpack.py", "ref_configpack")
     tb = _load(ref / "src/xla_cco/io/tables.py", "ref_tables")
