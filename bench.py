@@ -374,9 +374,57 @@ def run_device(args) -> None:
         "clocks": clocks,
         "gpu_launches": launches,
     }  # fmt: skip
+    if world == 1 and not args.no_target:
+        line["target"] = target_comparison()
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def target_comparison() -> dict:
+    """The north-star comparison on the 512-instance mixed-size ensemble (N
+    log-uniform in [200, 8000], d in {1, 2, 3}, chi in [0.05, 0.49], seed 0):
+    the plain FP64 drop-in (one relax call per instance, every instance,
+    sequential) against the batched device run and the served mixed-precision
+    form, with success-mask equality and latency percentiles. Device time for
+    the drop-in and the batch, host wall clock for the served stream."""
+    import torch
+
+    from xla_cco import LBFGSSettings
+    from xla_cco.minimize import relax_mixed_device
+    from xla_cco.workloads import mixed_ensemble
+
+    inst = mixed_ensemble(512, seed=SEED)
+    for i in inst:
+        i.energy.problem_handle(torch.cuda.current_device(), i.n)
+    settings = LBFGSSettings(energy_tol=TOL)
+    flat = torch.from_numpy(np.concatenate([i.s0.ravel() for i in inst])).cuda()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = relax_mixed_device([i.energy for i in inst], flat, [(i.n, i.d) for i in inst], settings)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ok = out["energy"].cpu().numpy() < TOL
+    lat = out["latency_ns"].cpu().numpy() / 1e6
+    plain = plain_dropin(inst, settings, 0)
+    plain_mask = plain.pop("mask")
+    served = served_mixed(inst, plain_mask)
+    return {
+        "workload": "mixed_lbfgs_512_n200-8000_d123_chi0.05-0.49",
+        "plain_fp64_dropin": plain,
+        "batched_fp64": {"value": float(ok.sum()) / (ms / 1e3), "unit": UNIT, "ms": ms,
+                         "success": f"{int(ok.sum())}/{len(inst)}",
+                         "mask_equals_plain_dropin": bool((ok == plain_mask).all()),
+                         "p50_latency_ms": float(np.percentile(lat, 50)),
+                         "p99_latency_ms": float(np.percentile(lat, 99))},
+        "served_mixed_precision": served,
+        "served_speedup_vs_plain_dropin": served["value"] / plain["value"] if plain["value"] else None,
+        "batched_speedup_vs_plain_dropin": (float(ok.sum()) / (ms / 1e3)) / plain["value"]
+        if plain["value"] else None,
+    }  # fmt: skip
 
 
 # ------------------------------------------------------------------ mixed batch
@@ -998,6 +1046,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=["cco", "reference"], default="cco")
     ap.add_argument("--batch", type=int, default=BATCH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-target", action="store_true",
+                    help="skip the mixed-ensemble comparison the default N=1 line carries")
     ap.add_argument("--profile", choices=["eval", "relax"], default=None,
                     help="profiling driver for ncu: run the kernels only")  # fmt: skip
     ap.add_argument("--reps", type=int, default=3)
