@@ -569,6 +569,7 @@ struct EvalWS {
     plan.smem2 = eval_smem2(p->host, split);
     plan.smem2_f32 = eval_smem2(p->host, split, true);
     plan.split2 = split;
+    plan.chunks1 = 1;
     plan.red_chunks = reduce_chunks(p->M);
     plan.want_grad = g != nullptr;
     return cudaGetLastError();

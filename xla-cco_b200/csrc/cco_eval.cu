@@ -72,10 +72,12 @@ __global__ void __launch_bounds__(kPass1Threads, 4) k_pass1(EvalPlan plan) {
   if ((lane_prec(ln) == PREC_FP32) != F32) return;   // the other kernel's lane
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
-  if (F32)
+  if (F32) {
     pass1_body_f32<D>(sp, ln, it.tile, smem);
-  else if (!sp.gemm)
-    pass1_body<D>(sp, ln, it.tile, smem);   // GEMM problems: k_pass1_gemm
+  } else if (!sp.gemm) {   // GEMM problems: k_pass1_gemm
+    const int C = pass1_chunks(sp, plan.chunks1);
+    pass1_body<D>(sp, ln, it.tile / C, smem, it.tile % C, C);
+  }
 }
 
 // Reduction (grid: k-chunks x lanes): rho_k = sum over tiles of the pass-1
@@ -93,9 +95,23 @@ __global__ void __launch_bounds__(kReduceChunk) k_reduce(EvalPlan plan) {
   const int k = k0 + threadIdx.x;
   double e = 0.0;
   if (k < M) {
-    double2 t = ln.part[k];
-    for (int q = 1; q < nt; ++q) {
-      const double2 o = ln.part[(size_t)q * M + k];
+    const double2* __restrict__ col = ln.part + k;
+    double2 t = col[0];
+    int q = 1;
+    // eight tile rows in flight per step, added in tile order (the same sums
+    // as one row at a time; a lane of few wide tiles is latency-bound here)
+    for (; q + 8 <= nt; q += 8) {
+      double2 o[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) o[u] = col[(size_t)(q + u) * M];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        t.x += o[u].x;
+        t.y += o[u].y;
+      }
+    }
+    for (; q < nt; ++q) {
+      const double2 o = col[(size_t)q * M];
       t.x += o.x;
       t.y += o.y;
     }

@@ -128,8 +128,11 @@ __device__ __forceinline__ void seg_sum(const Levels<D>& L, const SegHdr& h, con
   }
 }
 
+// Chunk c of C covers the segments [c nseg / C, (c + 1) nseg / C) (C > 1 only
+// when nseg >= 2 kPass1ChunkSegs, where ns = 1).
 template <int D>
-__device__ void pass1_body(const ProbDev& P, const EvalLane& ln, int tile, double2* tab) {
+__device__ void pass1_body(const ProbDev& P, const EvalLane& ln, int tile, double2* tab,
+                           int chunk = 0, int chunks = 1) {
   const TabLayout& T = P.t1;
   const int j0 = tile * kPass1Tile;
   const int nj = min(kPass1Tile, P.N - j0);
@@ -140,11 +143,14 @@ __device__ void pass1_body(const ProbDev& P, const EvalLane& ln, int tile, doubl
   const int nseg = P.nseg1;
   int ns = 1;
   while (2 * ns * nseg <= (int)blockDim.x && 2 * ns <= nj) ns *= 2;
-  const int units = nseg * ns;
+  const int seg_lo = (int)((long long)chunk * nseg / chunks);
+  const int seg_hi = (int)((long long)(chunk + 1) * nseg / chunks);
+  const int nsc = seg_hi - seg_lo;
+  const int units = nsc * ns;
   double2* red = tab + (size_t)T.nrows * kPass1Stride;
   double2* out = ln.part + (size_t)tile * P.M;
   for (int u = threadIdx.x; u < units; u += blockDim.x) {
-    const int sg = u % nseg, slice = u / nseg;
+    const int sg = seg_lo + u % nsc, slice = u / nsc;
     const SegHdr h = P.seg1[sg];
     double2 acc[kSeg1Len];
 #pragma unroll

@@ -162,9 +162,15 @@ struct EvalSet {
   cudaError_t build(const RecordShape& R, const std::vector<LaneRef>& refs,
                     const std::vector<const cco_problem*>& probs_of, int lo, int hi,
                     cudaStream_t st, bool may_fp32 = false) {
-    long long tiles1 = 0;
-    for (int i = lo; i < hi; ++i) tiles1 += probs_of[i]->host.ntile2;
+    long long tiles1 = 0, seg_tiles = 0;
+    for (int i = lo; i < hi; ++i) {
+      tiles1 += probs_of[i]->host.ntile2;
+      if (!probs_of[i]->host.gemm) seg_tiles += probs_of[i]->host.ntile1;
+    }
     const int split = pass2_split(tiles1);
+    // pass-1 segment chunks: enough CTAs for the per-segment FP64 tiles
+    int chunks = 1;
+    while (!may_fp32 && chunks < 8 && seg_tiles * chunks < kPass2TargetCtas) chunks *= 2;
     std::vector<const cco_problem*> uniq;
     std::vector<ProbDev> pv;
     std::vector<EvalLane> lv;
@@ -192,8 +198,10 @@ struct EvalSet {
         for (int t = 0; t < ntG; ++t) gG[p->d - 1].push_back(EvalItem{j, t});
       }
       // the per-segment pass 1: FP32 lanes, and problems without the GEMM form
-      if (!p->host.gemm || may_fp32)
-        for (int t = 0; t < p->host.ntile1; ++t) g1[p->d - 1].push_back(EvalItem{j, t});
+      if (!p->host.gemm || may_fp32) {
+        const int C = pass1_chunks(p->host, chunks);
+        for (int t = 0; t < p->host.ntile1 * C; ++t) g1[p->d - 1].push_back(EvalItem{j, t});
+      }
       const int nt2 = pass2_tiles(p->host, split);
       for (int t = 0; t < nt2; ++t) g2[p->d - 1].push_back(EvalItem{j, t});
     }
@@ -229,6 +237,7 @@ struct EvalSet {
     plan.smem2_f32 = smem2f;
     plan.red_chunks = reduce_chunks(max_m);
     plan.split2 = split;
+    plan.chunks1 = chunks;
     plan.want_grad = true;
     return e;
   }

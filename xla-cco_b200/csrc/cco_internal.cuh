@@ -197,10 +197,23 @@ struct EvalPlan {
   int max_d;                // largest d in the plan (template dispatch)
   int red_chunks;           // k-chunks of the reduction: ceil(max M / kReduceChunk)
   int split2;               // pass-2 threads per particle (1, 2, 4 or 8)
+  int chunks1;              // pass-1 segment chunks per tile (FP64 per-segment form; 1 = none)
   size_t smem1, smem2;      // dynamic shared memory of pass 1 / pass 2 (FP64 kernels)
   size_t smem2_f32;         // pass 2, FP32 kernels
   bool want_grad;
 };
+
+// A launch with few pass-1 tiles (a lone wide lane: one CTA per SM at most)
+// splits each tile's segments over up to 8 CTAs. Only problems with at least
+// 2 kPass1ChunkSegs segments are split, where one thread already owns one
+// segment (no in-CTA particle slices), so every segment's sum is computed
+// exactly as unsplit: the chunking changes where the work runs, not the bits.
+constexpr int kPass1ChunkSegs = 128;
+__host__ __device__ __forceinline__ int pass1_chunks(const ProbDev& p, int plan_chunks) {
+  if (p.nseg1 < 2 * kPass1ChunkSegs) return 1;
+  const int most = p.nseg1 / kPass1ChunkSegs;
+  return plan_chunks < most ? plan_chunks : most;
+}
 
 // The reduction of the pass-1 partials runs one block per kReduceChunk
 // k-vectors of a lane; a second kernel sums the chunks' energies in a fixed
