@@ -179,6 +179,27 @@ __device__ __forceinline__ void st2(double* p, int i, double2 v) {
   reinterpret_cast<double2*>(p)[i] = v;
 }
 
+// An element loop over a lane's double2 words with U words per thread in
+// flight: all U are loaded before any is stored, since the compiler cannot
+// move a load across a store that may alias it. Thread t still handles the
+// words t, t + blockDim.x, ..., each exactly as a one-at-a-time loop would.
+template <int U, class Load, class Store>
+__device__ __forceinline__ void lb_words(int h2, Load load, Store store) {
+  for (int e0 = threadIdx.x; e0 < h2; e0 += U * blockDim.x) {
+    decltype(load(0)) t[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = e0 + u * (int)blockDim.x;
+      if (e < h2) t[u] = load(e);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = e0 + u * (int)blockDim.x;
+      if (e < h2) store(e, t[u]);
+    }
+  }
+}
+
 __device__ __forceinline__ LbView lane_view(const LbArgs& A, const LaneRef& R) {
   return lb_view(R.rec, A.m, A.tri_len, R.ld, A.keep_s0);
 }
@@ -228,22 +249,22 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
     const int sl = L.hhead;
     double* Sr = v.Sh + (size_t)sl * ld;
     double* Yr = v.Yh + (size_t)sl * ld;
-    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-      const double2 xo = ld2(x, e), dv = ld2(v.dir, e), go = ld2(g, e);
-      const double2 xn = make_double2(xo.x + al * dv.x, xo.y + al * dv.y);
-      double2 gn;
-      if (probe) {
-        const double2 pv = ld2(v.pg, e);
-        gn = make_double2(pv.x / Rs, pv.y / Rs);
-      } else {
-        gn = ld2(v.glo, e);
-      }
-      st2(Sr, e, make_double2(xn.x - xo.x, xn.y - xo.y));
-      st2(Yr, e, make_double2(gn.x - go.x, gn.y - go.y));
-      st2(x, e, xn);
-      st2(s, e, make_double2(xn.x / Rs, xn.y / Rs));
-      st2(g, e, gn);
-    }
+    struct Words {
+      double2 xo, dv, go, gn;
+    };
+    const double* gsrc = probe ? v.pg : v.glo;
+    lb_words<4>(
+        h2,
+        [&](int e) { return Words{ld2(x, e), ld2(v.dir, e), ld2(g, e), ld2(gsrc, e)}; },
+        [&](int e, const Words& w) {
+          const double2 xn = make_double2(w.xo.x + al * w.dv.x, w.xo.y + al * w.dv.y);
+          const double2 gn = probe ? make_double2(w.gn.x / Rs, w.gn.y / Rs) : w.gn;
+          st2(Sr, e, make_double2(xn.x - w.xo.x, xn.y - w.xo.y));
+          st2(Yr, e, make_double2(gn.x - w.go.x, gn.y - w.go.y));
+          st2(x, e, xn);
+          st2(s, e, make_double2(xn.x / Rs, xn.y / Rs));
+          st2(g, e, gn);
+        });
     __syncthreads();
     if (threadIdx.x == 0) {
       L.f = L.f_lo;  // accepted energy (an accepted probe is stashed in f_lo)
@@ -450,12 +471,22 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
     lb_record(A, lane, R, sh, v.s);
   } else {
     if (L.need_dir) {
-      // the direction and the first probe (alpha = 1) were written by pass B
+      // the direction and the first probe (alpha = 1) were written by pass B;
+      // g.dir is the sum of its block partials (a wide lane's many partials:
+      // strided per thread, then the block tree)
+      const double* dpart = v.scal + 4 * A.m + 1;
+      const int nb = lb_nblk(R.ld);
+      double dpw = 0.0;
+      if (lb_wide(R.ld)) {
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) dpw += dpart[b];
+        dpw = block_sum(dpw, sh.red);
+      }
       if (threadIdx.x == 0) {
-        const double* dpart = v.scal + 4 * A.m + 1;
-        const int nb = lb_nblk(R.ld);
         double dp = 0.0;
-        for (int b = 0; b < nb; ++b) dp += dpart[b];
+        if (lb_wide(R.ld))
+          dp = dpw;
+        else
+          for (int b = 0; b < nb; ++b) dp += dpart[b];
         L.f0 = L.f;
         L.dphi0 = dp;
         L.phase = PH_EXPAND;
@@ -488,17 +519,21 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
     }
     __syncthreads();
     if (sh.new_lo) {
-      for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-        const double2 pv = ld2(v.pg, e);
-        st2(v.glo, e, make_double2(pv.x / Rs, pv.y / Rs));
-      }
+      lb_words<8>(
+          h2, [&](int e) { return ld2(v.pg, e); },
+          [&](int e, double2 pv) { st2(v.glo, e, make_double2(pv.x / Rs, pv.y / Rs)); });
     }
     if (sh.outcome == LS_CONTINUE) {
       const double al = L.alpha;
-      for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-        const double2 xv = ld2(v.x, e), dv = ld2(v.dir, e);
-        st2(v.ps, e, make_double2((xv.x + al * dv.x) / Rs, (xv.y + al * dv.y) / Rs));
-      }
+      struct Words {
+        double2 xv, dv;
+      };
+      lb_words<4>(
+          h2, [&](int e) { return Words{ld2(v.x, e), ld2(v.dir, e)}; },
+          [&](int e, const Words& w) {
+            st2(v.ps, e,
+                make_double2((w.xv.x + al * w.dv.x) / Rs, (w.xv.y + al * w.dv.y) / Rs));
+          });
     } else {
       __syncthreads();
       lb_end_iteration(A, lane, R, v, sh);
@@ -508,20 +543,26 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
   if (threadIdx.x == 0) *v.st = sh.L;
 }
 
-// Pass A (grid: pair blocks x lanes): a_p = s_p.g, b_p = y_p.g for every
-// stored pair and, after a push, the newest pair's column s_p.y_n, y_p.y_n.
-// One warp per pair with four double2 words per lane in flight.
+// Pass A (grid: pair blocks x element chunks, lanes): a_p = s_p.g, b_p = y_p.g
+// for every stored pair and, after a push, the newest pair's column s_p.y_n,
+// y_p.y_n. One warp per (pair, chunk) with four double2 words per lane in
+// flight; a lane of one chunk writes the dots, a wide lane its partials.
 __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
   const int lane = blockIdx.y;
   const LaneRef R = A.lanes[lane];
+  const int chunk = blockIdx.x % A.nchA, pblk = blockIdx.x / A.nchA;
+  const int nch = lb_achunks(R.ld);
+  if (chunk >= nch) return;
   const LbView v = lane_view(A, R);
   const LbState* Lp = v.st;
   const int k = Lp->hk;
   if (Lp->status != CCO_STATUS_RUNNING || !Lp->need_dir || k == 0) return;
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
-  const int p = blockIdx.x * (kUpdThreads / 32) + warp;
+  const int p = pblk * (kUpdThreads / 32) + warp;
   if (p >= k) return;
-  const int ld = R.ld, h2 = ld >> 1, m = A.m;
+  const int ld = R.ld, m = A.m;
+  const int e_lo = chunk * kLbWide;
+  const int h2 = nch == 1 ? (ld >> 1) : min(ld >> 1, e_lo + kLbWide);   // end of this chunk
   const int head = Lp->hhead;
   const bool np = Lp->newpair != 0;
   const int sp = (head - k + p + m) % m, sn = (head - 1 + m) % m;
@@ -530,7 +571,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
   const double* yr = v.Yh + (size_t)sp * ld;
   const double* yn = v.Yh + (size_t)sn * ld;
   double ag = 0.0, bg = 0.0, sy = 0.0, yy = 0.0;
-  int e = wl;
+  int e = (nch == 1 ? 0 : e_lo) + wl;
   for (; e + 96 < h2; e += 128) {
     double2 sv[4], yv[4], gv[4];
 #pragma unroll
@@ -572,14 +613,57 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passA(LbArgs A) {
   }
   if (wl == 0) {
     double* sc = v.scal;
-    sc[p] = ag;
-    sc[m + p] = bg;
+    if (nch == 1) {
+      sc[p] = ag;
+      sc[m + p] = bg;
+      if (np) {
+        v.SY[(size_t)sn * m + sp] = sy;   // row = newer slot
+        v.YY[(size_t)sp * m + sn] = yy;
+        v.YY[(size_t)sn * m + sp] = yy;
+      }
+    } else {
+      double* ap = sc + lb_apart_off(m, ld) + (size_t)chunk * 4 * m;
+      ap[p] = ag;
+      ap[m + p] = bg;
+      if (np) {
+        ap[2 * m + p] = sy;
+        ap[3 * m + p] = yy;
+      }
+    }
+  }
+}
+
+// The dots of a wide lane: its pass-A chunk partials summed in chunk order.
+__device__ void lb_sum_apart(const LbArgs& A, const LaneRef& R, const LbView& v, int k,
+                             int head, bool np) {
+  const int m = A.m, nch = lb_achunks(R.ld);
+  const double* ap = v.scal + lb_apart_off(m, R.ld);
+  const int sn = (head - 1 + m) % m;
+  for (int p = threadIdx.x; p < k; p += blockDim.x) {
+    double ag = ap[p], bg = ap[m + p], sy = 0.0, yy = 0.0;
     if (np) {
-      v.SY[(size_t)sn * m + sp] = sy;   // row = newer slot
+      sy = ap[2 * m + p];
+      yy = ap[3 * m + p];
+    }
+    for (int c = 1; c < nch; ++c) {
+      const double* q = ap + (size_t)c * 4 * m;
+      ag += q[p];
+      bg += q[m + p];
+      if (np) {
+        sy += q[2 * m + p];
+        yy += q[3 * m + p];
+      }
+    }
+    v.scal[p] = ag;
+    v.scal[m + p] = bg;
+    if (np) {
+      const int sp = (head - k + p + m) % m;
+      v.SY[(size_t)sn * m + sp] = sy;
       v.YY[(size_t)sp * m + sn] = yy;
       v.YY[(size_t)sn * m + sp] = yy;
     }
   }
+  __syncthreads();
 }
 
 // Scalar kernel (one CTA per lane): gamma and the coefficients of the
@@ -605,6 +689,7 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
   const int k = Lp->hk, m = A.m, head = Lp->hhead;
   double* sc = v.scal;
   const int warp = threadIdx.x >> 5, wl = threadIdx.x & 31;
+  if (k > 0 && lb_wide(R.ld)) lb_sum_apart(A, R, v, k, head, Lp->newpair != 0);
   // two packings by newer rows (tri(p, q) = q (q + 1) / 2 + p, p <= q):
   // triSY (SY[p][q] = s_p . y_q, p older than q) and triYY (the symmetric YY).
   // Two triangles (2 m (m + 1) / 2 doubles, 81 KB at m = 100) let two CTAs
@@ -772,8 +857,58 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_passB(LbArgs A) {
   const double* cs = in_smem ? csv : sc + 3 * m + 1;
   const double* Sh = v.Sh;
   const double* Yh = v.Yh;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
   double dp = 0.0;
+  if (lb_wide(ld)) {
+    // warp w sums the pairs [w k / G, (w + 1) k / G) for the block's 32 words;
+    // warp 0 adds the G group sums in order and finishes the words
+    __shared__ double2 gsum[kPassBGroups][32];
+    const int w = threadIdx.x >> 5, wl = threadIdx.x & 31;
+    const int e = blockIdx.x * 32 + wl;
+    const int q1 = (w + 1) * k / kPassBGroups;
+    double ax = 0.0, ay = 0.0;
+    if (e < h2) {
+      int q = w * k / kPassBGroups;
+      for (; q + 8 <= q1; q += 8) {
+        double2 yv[8], sv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const size_t r = (size_t)((head - k + q + u + m) % m) * ld;
+          yv[u] = ld2(Yh + r, e);
+          sv[u] = ld2(Sh + r, e);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          ax += cy[q + u] * yv[u].x + cs[q + u] * sv[u].x;
+          ay += cy[q + u] * yv[u].y + cs[q + u] * sv[u].y;
+        }
+      }
+      for (; q < q1; ++q) {
+        const size_t r = (size_t)((head - k + q + m) % m) * ld;
+        const double2 yv = ld2(Yh + r, e), sv = ld2(Sh + r, e);
+        ax += cy[q] * yv.x + cs[q] * sv.x;
+        ay += cy[q] * yv.y + cs[q] * sv.y;
+      }
+    }
+    gsum[w][wl] = make_double2(ax, ay);
+    __syncthreads();
+    if (w == 0 && e < h2) {
+      double2 t = gsum[0][wl];
+#pragma unroll
+      for (int g = 1; g < kPassBGroups; ++g) {
+        t.x += gsum[g][wl].x;
+        t.y += gsum[g][wl].y;
+      }
+      const double2 gv = ld2(v.g, e), xv = ld2(v.x, e);
+      const double2 de = make_double2(t.x - gam * gv.x, t.y - gam * gv.y);
+      st2(v.dir, e, de);
+      dp = gv.x * de.x + gv.y * de.y;
+      st2(v.ps, e, make_double2((xv.x + 1.0 * de.x) / Rs, (xv.y + 1.0 * de.y) / Rs));
+    }
+    dp = block_sum(dp, red);
+    if (threadIdx.x == 0) sc[4 * m + 1 + blockIdx.x] = dp;
+    return;
+  }
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e < h2) {
     double ax = 0.0, ay = 0.0;
     int q = 0;
@@ -886,7 +1021,7 @@ cudaError_t lbfgs_init(const LbArgs& a, const double* s0, cudaStream_t st) {
 // direction stages, which exit at once for lanes that are mid line search.
 cudaError_t lbfgs_update(const LbArgs& a, cudaStream_t st) {
   k_lbfgs_probe<<<a.B, kUpdThreads, 0, st>>>(a);
-  const dim3 ga((a.m + kUpdThreads / 32 - 1) / (kUpdThreads / 32), a.B);
+  const dim3 ga((a.m + kUpdThreads / 32 - 1) / (kUpdThreads / 32) * a.nchA, a.B);
   k_lbfgs_passA<<<ga, kUpdThreads, 0, st>>>(a);
   k_lbfgs_scalar<<<a.B, kUpdThreads, a.smem_tri, st>>>(a);
   const dim3 gb(a.nblkB, a.B);

@@ -112,13 +112,33 @@ static_assert(sizeof(DsState) <= (kDsHead - 1) * sizeof(double), "DsState outgre
 
 constexpr int kUpdThreads = 256;
 
-// Pass-B element blocks of a lane: one double2 word per thread.
-__host__ __device__ __forceinline__ int lb_nblk(int ld) {
-  return ((ld >> 1) + kUpdThreads - 1) / kUpdThreads;
+// Wide lanes (more than kLbWide double2 words) split the two history passes
+// finer, so that a lone wide lane still spreads its stream over many SMs:
+// pass A over element chunks of kLbWide words (each warp's partial dots are
+// summed in chunk order by the scalar kernel), pass B over kPassBGroups pair
+// groups of 32-word element blocks (the groups' sums are added in group
+// order). Which form a lane takes depends on its size alone, so its bits do
+// not depend on the batch it runs in.
+constexpr int kLbWide = 1024;
+constexpr int kPassBGroups = kUpdThreads / 32;
+__host__ __device__ __forceinline__ bool lb_wide(int ld) { return (ld >> 1) > kLbWide; }
+// Pass-A element chunks of a lane.
+__host__ __device__ __forceinline__ int lb_achunks(int ld) {
+  return lb_wide(ld) ? ((ld >> 1) + kLbWide - 1) / kLbWide : 1;
 }
-// Scalar row: a_p, b_p (m each), gamma + cy (1 + m), cs (m), pass-B partials.
+// Pass-B element blocks of a lane: one double2 word per thread, or 32 words
+// per block (a word per warp lane, a pair group per warp) for wide lanes.
+__host__ __device__ __forceinline__ int lb_nblk(int ld) {
+  return lb_wide(ld) ? ((ld >> 1) + 31) / 32 : ((ld >> 1) + kUpdThreads - 1) / kUpdThreads;
+}
+// Scalar row: a_p, b_p (m each), gamma + cy (1 + m), cs (m), pass-B partials,
+// then (wide lanes) the pass-A partials: [chunk][a, b, sy, yy][m].
 __host__ __device__ __forceinline__ size_t lb_scal_len(int m, int ld) {
-  return ((size_t)4 * m + 1 + lb_nblk(ld) + 3) & ~(size_t)3;
+  const size_t apart = lb_wide(ld) ? (size_t)4 * m * lb_achunks(ld) : 0;
+  return ((size_t)4 * m + 1 + lb_nblk(ld) + apart + 3) & ~(size_t)3;
+}
+__host__ __device__ __forceinline__ size_t lb_apart_off(int m, int ld) {
+  return (size_t)4 * m + 1 + lb_nblk(ld);
 }
 
 // Record: [0, 32) LbState, pf at [31]; SY (m m, row = newer slot), YY (m m);
@@ -175,6 +195,7 @@ struct LbArgs {
   int prec0;              // PREC_FP32: lanes of d >= 2 start in FP32 (mixed precision)
   int keep_s0;            // records hold s0 (mixed precision: restart of a failed lane)
   int nblkB;              // grid width of pass B (max over the lanes)
+  int nchA;               // pass-A element chunks (max over the lanes)
   size_t smem_tri;        // 0: triangles in the record (global memory)
   double *traj_s, *traj_e, *traj_step;
   int64_t *traj_it, *traj_count;

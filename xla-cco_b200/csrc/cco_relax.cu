@@ -97,8 +97,11 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
     const int lo = bounds[b], hi = bounds[b + 1];
     const bool may_fp32 = T.shape.method == Method::Lbfgs && T.lb.prec0 == PREC_FP32;
     CCO_CUDA(ev[b].build(T.shape, T.refs, T.probs, lo, hi, st, may_fp32));
-    int nblk = 1;
-    for (int i = lo; i < hi; ++i) nblk = std::max(nblk, lb_nblk(T.refs[i].ld));
+    int nblk = 1, nch = 1;
+    for (int i = lo; i < hi; ++i) {
+      nblk = std::max(nblk, lb_nblk(T.refs[i].ld));
+      nch = std::max(nch, lb_achunks(T.refs[i].ld));
+    }
     if (T.shape.method == Method::Flow) {
       FlArgs a = T.fl;
       a.B = hi - lo;
@@ -119,6 +122,7 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
       a.B = hi - lo;
       a.lanes = T.d_refs + lo;
       a.nblkB = nblk;
+      a.nchA = nch;
       lb[b] = a;
     }
   }
@@ -691,9 +695,13 @@ int relax_lbfgs_set(cco_problem* const* probs, int B, cudaStream_t st, const dou
   }
   A.B = B;
   A.lanes = T.d_refs;
-  int nblk = 1;
-  for (const LaneRef& r : T.refs) nblk = std::max(nblk, lb_nblk(r.ld));
+  int nblk = 1, nch = 1;
+  for (const LaneRef& r : T.refs) {
+    nblk = std::max(nblk, lb_nblk(r.ld));
+    nch = std::max(nch, lb_achunks(r.ld));
+  }
   A.nblkB = nblk;
+  A.nchA = nch;
   CCO_CUDA(lbfgs_init(A, s0, st));
   const int64_t max_ticks =
       1 + (int64_t)cfg->n_rescales * (cfg->max_evals_per_pass + cfg->max_linesearch_steps + 1) +

@@ -136,6 +136,7 @@ int cco_stepper_create(int device, void* stream, int method, const void* setting
     }
     h->rec_doubles = (lb_record_doubles(shape.m, shape.tri_len, h->ld, 0, 0) + 31) & ~(size_t)31;
     h->lb.nblkB = lb_nblk(h->ld);
+    h->lb.nchA = lb_achunks(h->ld);
   }
   cudaError_t e = cudaMalloc(&h->records, h->rec_doubles * batch * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&h->d_refs, sizeof(LaneRef) * batch);
