@@ -358,6 +358,8 @@ def run_device(args) -> None:
             "p50_latency_ms": float(np.percentile(lat, 50)),
             "p99_latency_ms": float(np.percentile(lat, 99)),
             "evals_per_relax": epr, "ticks": ticks,
+            "schedule": {"branches": outs[-1]["schedule"][0], "graph_ticks": outs[-1]["schedule"][1],
+                         "overlap": outs[-1]["overlap"]},
             "evals_per_s": float(evals.sum()) / (ms / 1e3),
             "pair_evals_per_s": float(evals.sum()) * N_PART * m / (ms / 1e3),
         }),

@@ -204,6 +204,9 @@ typedef struct {
   int64_t launches;     /* out: kernel launches issued by the call */
   int32_t branches;     /* out: graph branches of the tick schedule used */
   int32_t graph_ticks;  /* out: ticks per captured graph of that schedule */
+  int32_t overlap;      /* out: 1 if that schedule ran the branches half a tick apart with
+                           the update kernels at high stream priority */
+  int32_t reserved;     /* zero */
 } cco_relax_out;
 
 /*
@@ -433,8 +436,9 @@ int cco_md_segment(cco_problem* p, void* stream, int batch, const double* basis,
  * first relaxation of each shape class (minimizer, lane count and total
  * N M bucketed by powers of two, largest d) and cached for the process;
  * results never depend on the schedule. This forgets every cached schedule.
- * The environment variables CCO_BRANCHES and CCO_GRAPH_TICKS force a
- * schedule, CCO_AUTOTUNE=0 keeps the default (2 branches, 16 ticks).
+ * The environment variables CCO_BRANCHES, CCO_GRAPH_TICKS and CCO_OVERLAP
+ * (0 or 1) force a schedule, CCO_AUTOTUNE=0 keeps the default (2 branches,
+ * 16 ticks, no overlap).
  */
 int cco_schedule_reset(void);
 

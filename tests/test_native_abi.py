@@ -40,7 +40,7 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts_match_header():
     assert ctypes.sizeof(_native.DescentSettingsC) == 9 * 8
     assert ctypes.sizeof(_native.LBFGSSettingsC) == 8 + 8 + 8 * 8 + 7 * 8
-    assert ctypes.sizeof(_native.RelaxOutC) == 16 * 8
+    assert ctypes.sizeof(_native.RelaxOutC) == 17 * 8
 
 
 def test_abi_version_and_errors():

@@ -329,3 +329,29 @@ def test_small_descent_lanes_run_in_one_persistent_launch():
         one = relax_device(en, s0[i:i + 1].contiguous(), st)
         for k in ("s", "energy", "n_evals", "n_iters", "status"):
             assert torch.equal(one[k][0], out[k][i]), (i, k)
+
+
+@pytest.mark.parametrize("branches,overlap", [(1, 0), (2, 0), (2, 1), (3, 1)])
+def test_tick_schedules_give_the_same_bits(monkeypatch, branches, overlap):
+    """Every tick schedule the tuner may pick - one graph branch, several, and
+    the overlap form (branches half a tick apart, update kernels at high stream
+    priority) - advances every lane through the same kernels: the results are
+    bit-identical to the default schedule's."""
+    import torch
+
+    from xla_cco.minimize import relax_device
+
+    box = cubic_box(300, 2)
+    ks = enumerate_kvectors(box.basis, 0.0, k_outer_from_ka(ka_from_chi(0.4, 0.05, 2), 0.05, 2))
+    en = make_stealthy_energy(box, ks)
+    s0 = torch.from_numpy(np.random.default_rng(3).uniform(size=(48, 300, 2))).cuda()
+    st = LBFGSSettings(energy_tol=1e-20)
+    monkeypatch.setenv("CCO_AUTOTUNE", "0")
+    base = relax_device(en, s0, st)
+    monkeypatch.setenv("CCO_BRANCHES", str(branches))
+    monkeypatch.setenv("CCO_OVERLAP", str(overlap))
+    out = relax_device(en, s0, st)
+    assert out["schedule"][0] == branches and out["overlap"] == bool(overlap)
+    for k in ("s", "energy", "grad_norm", "n_evals", "n_iters", "status"):
+        assert torch.equal(base[k], out[k]), k
+    assert (out["energy"] < 1e-20).all()

@@ -291,9 +291,17 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     const bool allow = d >= 2 && !(env && atoi(env) == 0);
     int c0 = 0, c1 = 0;      // widest group prefix windows
     double computed = 0.0;   // grid cells the blocks multiply
+    // d = 2 folds the last axis: columns are c = |n|, a run [a, b] covers
+    // [ca, cb] (its folded range), and one cell (run, c) yields C(c) and C(-c)
+    const bool fold = d == 2;
+    const int cols = fold ? kGemmColsF : kGemmCols;
+    auto fa = [fold](const GemmRun& g) {
+      return !fold ? g.a : (g.a <= 0 && g.b >= 0) ? 0 : std::min(std::abs(g.a), std::abs(g.b));
+    };
+    auto fb = [fold](const GemmRun& g) { return !fold ? g.b : std::max(std::abs(g.a), std::abs(g.b)); };
     std::vector<GemmRun> sorted = runs;
-    std::stable_sort(sorted.begin(), sorted.end(), [](const GemmRun& x, const GemmRun& y) {
-      return (x.b - x.a) > (y.b - y.a);
+    std::stable_sort(sorted.begin(), sorted.end(), [&](const GemmRun& x, const GemmRun& y) {
+      return (fb(x) - fa(x)) > (fb(y) - fa(y));
     });
     for (size_t r0 = 0; r0 < sorted.size(); r0 += kGemmRows) {
       const int nrun = (int)std::min<size_t>(kGemmRows, sorted.size() - r0);
@@ -301,8 +309,8 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
       int gm0 = 1 << 30, gM0 = -(1 << 30), gm1 = 1 << 30, gM1 = -(1 << 30);
       for (int r = 0; r < nrun; ++r) {
         const GemmRun& g = sorted[r0 + r];
-        lo = std::min(lo, g.a);
-        hi = std::max(hi, g.b);
+        lo = std::min(lo, fa(g));
+        hi = std::max(hi, fb(g));
         gm0 = std::min(gm0, g.n0);
         gM0 = std::max(gM0, g.n0);
         gm1 = std::min(gm1, g.n1);
@@ -315,13 +323,14 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
       const int run0 = (int)grun.size();
       for (int r = 0; r < nrun; ++r) grun.push_back(sorted[r0 + r]);
       // warps whose 6 rows lie past the group's runs skip their products
-      computed += (double)((nrun + 5) / 6 * 6) * kGemmCols * ((hi - lo) / kGemmCols + 1);
-      for (int w = lo; w <= hi; w += kGemmCols) {
+      // (output slots: a folded cell holds two)
+      computed += (double)((nrun + 5) / 6 * 6) * cols * ((hi - lo) / cols + 1) * (fold ? 2 : 1);
+      for (int w = lo; w <= hi; w += cols) {
         GemmBlock b{};
         b.run0 = run0;
         b.nrun = nrun;
         b.lo = w;
-        b.nb = std::min(kGemmCols, hi - w + 1);
+        b.nb = std::min(cols, hi - w + 1);
         b.m0 = gm0;
         b.c0 = gc0;
         b.m1 = d >= 3 ? gm1 : 0;
@@ -345,7 +354,7 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     bool found = false;
     for (int rounds = 1; !found; ++rounds)
       for (int L = 8; L <= kGemmMaxRun && !found; ++L) {
-        const int u0 = (c0 + L - 1) / L, u1 = (c1 + L - 1) / L, uz = (kGemmCols + L - 1) / L;
+        const int u0 = (c0 + L - 1) / L, u1 = (c1 + L - 1) / L, uz = (cols + L - 1) / L;
         if (u0 + u1 + uz <= per_round * rounds) {
           P.gL = L;
           P.gu0 = u0;

@@ -201,7 +201,7 @@ size_t eval_smem1(const ProbDev& p) {
 size_t eval_smemG(const ProbDev& p) {
   if (!p.gemm) return 0;
   if (p.d == 2)   // two table sets (prefix, last axis) and two root sets
-    return (size_t)kGemmChunk * (2 * (p.gs0 + kGemmZStride) + 2 * p.d) * sizeof(double2);
+    return (size_t)kGemmChunk * (2 * (p.gs0 + kGemmZStrideF) + 2 * p.d) * sizeof(double2);
   const int s1 = p.d == 3 ? p.gs1 : 0;
   return (size_t)kGemmChunk * (p.gs0 + s1 + kGemmZStride + kGemmRows + 2 * p.d) *
          sizeof(double2);

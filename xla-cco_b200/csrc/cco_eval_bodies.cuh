@@ -804,19 +804,24 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
 }
 
 // d = 2: the A rows are a gather from the prefix table (A[r][j] = T0[j][n0(r)]),
-// so there is no A phase. The tables are double-buffered: while the CTA
+// so there is no A phase. The last axis is folded: the block's columns are
+// c = |n|, and with A = a + ib and z^c = u + iv the four sums P1 = sum a u,
+// P2 = sum b v, P3 = sum a v, P4 = sum b u give C(c) = (P1 - P2) + i (P3 + P4)
+// and C(-c) = A conj(z^c) summed = (P1 + P2) + i (P4 - P3): four FMAs per
+// cell and particle for two k-set rows. Each thread accumulates 3 runs x 2
+// columns (tn, tn + 16). The tables are double-buffered: while the CTA
 // multiplies chunk c it fills chunk c + 1 (and the roots of chunk c + 2), one
 // barrier per chunk. Rows past the group's runs read the zero column c0.
 __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int tile, int blk,
                                    double2* smem) {
-  constexpr int KC = kGemmChunk, D = 2;
+  constexpr int KC = kGemmChunk, D = 2, ZS = kGemmZStrideF;
   const GemmBlock B = P.gblk[blk];
   const int j0 = tile * kPass1Tile;
   const int nj = min(kPass1Tile, P.N - j0);
   const int c0 = B.c0, s0 = P.gs0;           // s0 > P.gc0 >= c0: column P.gc0 holds zeros
   const int zc = P.gc0;
-  const int buf = KC * (s0 + kGemmZStride);   // one table set
-  double2* R = smem + 2 * buf;                // [2][KC * D] roots
+  const int buf = KC * (s0 + ZS);            // one table set
+  double2* R = smem + 2 * buf;               // [2][KC * D] roots
   const int tr = threadIdx.x >> 4, tn = threadIdx.x & 15;
   const bool rows_live = 6 * (threadIdx.x >> 5) < B.nrun;   // this warp's rows 6w .. 6w + 5
   int off[3];
@@ -825,11 +830,11 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
     const int r = 3 * tr + i;
     off[i] = r < B.nrun ? P.grun[B.run0 + r].n0 - B.m0 : zc;
   }
-  double2 acc[3][3];
+  double p1[3][2], p2[3][2], p3[3][2], p4[3][2];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) acc[i][c] = make_double2(0.0, 0.0);
+    for (int q = 0; q < 2; ++q) p1[i][q] = p2[i][q] = p3[i][q] = p4[i][q] = 0.0;
   const int L = P.gL, u0 = P.gu0, uz = P.guz;
   const int nch = (nj + KC - 1) / KC;
   auto fill = [&](int c) {   // tables of chunk c into buffer c & 1 (roots in R[c & 1])
@@ -846,8 +851,8 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
           fill_powers(T0 + j * s0, L * q, min(L, c0 - L * q), B.m0, live ? sj[0] : 0.0, zs[j * D]);
       } else {
         const int qq = q - u0;
-        fill_powers(Z + j * kGemmZStride, L * qq, min(L, kGemmCols - L * qq), B.lo,
-                    live ? sj[1] : 0.0, zs[j * D + 1]);
+        fill_powers(Z + j * ZS, L * qq, min(L, kGemmColsF - L * qq), B.lo, live ? sj[1] : 0.0,
+                    zs[j * D + 1]);
       }
     }
     if (threadIdx.x < KC) T0[threadIdx.x * s0 + zc] = make_double2(0.0, 0.0);
@@ -865,19 +870,19 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
     const double2* Z = T0 + KC * s0;
     const int kc = rows_live ? min(KC, nj - c * KC) : 0;
     for (int j = 0; j < kc; ++j) {
-      double2 a[3], z[3];
+      double2 a[3], z[2];
 #pragma unroll
       for (int i = 0; i < 3; ++i) a[i] = T0[j * s0 + off[i]];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) z[q] = Z[j * kGemmZStride + tn + 16 * q];
+      for (int q = 0; q < 2; ++q) z[q] = Z[j * ZS + tn + 16 * q];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          acc[i][q].x = fma(a[i].x, z[q].x, acc[i][q].x);
-          acc[i][q].x = fma(-a[i].y, z[q].y, acc[i][q].x);
-          acc[i][q].y = fma(a[i].x, z[q].y, acc[i][q].y);
-          acc[i][q].y = fma(a[i].y, z[q].x, acc[i][q].y);
+        for (int q = 0; q < 2; ++q) {
+          p1[i][q] = fma(a[i].x, z[q].x, p1[i][q]);
+          p2[i][q] = fma(a[i].y, z[q].y, p2[i][q]);
+          p3[i][q] = fma(a[i].x, z[q].y, p3[i][q]);
+          p4[i][q] = fma(a[i].y, z[q].x, p4[i][q]);
         }
     }
     __syncthreads();
@@ -889,10 +894,15 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
     if (r < B.nrun) {
       const GemmRun g = P.grun[B.run0 + r];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
+      for (int q = 0; q < 2; ++q) {
         const int col = tn + 16 * q;
-        const int n = B.lo + col;
-        if (col < B.nb && n >= g.a && n <= g.b) out[g.kstart + (n - g.a)] = acc[i][q];
+        const int cv = B.lo + col;
+        if (col < B.nb) {
+          if (cv >= g.a && cv <= g.b)
+            out[g.kstart + (cv - g.a)] = make_double2(p1[i][q] - p2[i][q], p3[i][q] + p4[i][q]);
+          if (cv > 0 && -cv >= g.a && -cv <= g.b)
+            out[g.kstart + (-cv - g.a)] = make_double2(p1[i][q] + p2[i][q], p4[i][q] - p3[i][q]);
+        }
       }
     }
   }

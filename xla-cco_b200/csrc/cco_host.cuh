@@ -262,6 +262,11 @@ struct EvalSet {
 struct Schedule {
   int branches = 2;
   int graph_ticks = 16;
+  // overlap: branch b > 0 starts half a tick late (after branch 0's first
+  // evaluation) and every branch's update kernels run on a high-priority
+  // stream, so the HBM-bound update of one branch takes SM slots as the
+  // FP64-bound evaluation of another frees them
+  int overlap = 0;
 };
 constexpr int kMaxBranches = 4;
 constexpr int kInflight = 3;    // graphs in flight before the host checks completion
@@ -321,6 +326,7 @@ struct TickPlan {
   cudaGraphExec_t exec = nullptr;
   int build(const LaneTable& T, const Schedule& sch, cudaStream_t st);
   cudaError_t tick(cudaStream_t s, int b, const EvalSide* side = nullptr) const;
+  cudaError_t update(cudaStream_t s, int b) const;
   int launches_per_tick() const;
   void release(cudaStream_t st);
 };
@@ -333,7 +339,7 @@ struct RunStats {
 
 // Runs tick graphs until no lane of T is RUNNING (CCO_ERR_ROUNDS past
 // max_ticks), compacting the lane table as lanes finish. The schedule is
-// forced by CCO_BRANCHES / CCO_GRAPH_TICKS, cached for the shape class, or
+// forced by CCO_BRANCHES / CCO_GRAPH_TICKS / CCO_OVERLAP, cached for the shape class, or
 // tuned online on the live lanes; CCO_COMPACT=0 keeps the full table.
 int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* stats);
 

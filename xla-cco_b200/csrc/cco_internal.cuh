@@ -51,6 +51,10 @@ static_assert(sizeof(SegHdr) == 32, "segment header is two 16-byte loads");
 // a (group, window) is a block, one CTA per (lane, tile, block).
 constexpr int kGemmRows = 24, kGemmCols = 48, kGemmChunk = 16, kGemmThreads = 128;
 constexpr int kGemmZStride = kGemmCols + 1;   // odd row stride: table writes spread over banks
+// d = 2 folds the last axis: a block's columns are |n| (kGemmColsF of them)
+// and the four real products of A z^|n| give both C(n) and C(-n).
+constexpr int kGemmColsF = 32;
+constexpr int kGemmZStrideF = kGemmColsF + 1;
 constexpr int kGemmMaxPrefix = 128;   // table entries per prefix axis
 constexpr int kGemmMaxRun = 16;       // longest power chain between FP64 sincospi seeds
 struct GemmRun {

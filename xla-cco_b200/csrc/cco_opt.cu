@@ -253,7 +253,7 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
       double2 xo, dv, go, gn;
     };
     const double* gsrc = probe ? v.pg : v.glo;
-    lb_words<4>(
+    lb_words<2>(
         h2,
         [&](int e) { return Words{ld2(x, e), ld2(v.dir, e), ld2(g, e), ld2(gsrc, e)}; },
         [&](int e, const Words& w) {
@@ -411,7 +411,7 @@ __global__ void k_lbfgs_init(LbArgs A, const double* __restrict__ s0) {
 // Probe kernel: one CTA per lane. Starts the line search of a direction
 // built by the previous tick's passes, consumes this tick's probe and either
 // places the next probe or ends the iteration.
-__global__ void __launch_bounds__(kUpdThreads) k_lbfgs_probe(LbArgs A) {
+__global__ void __launch_bounds__(kUpdThreads, 2) k_lbfgs_probe(LbArgs A) {
   __shared__ LbShared sh;
   const int lane = blockIdx.x;
   const LaneRef R = A.lanes[lane];

@@ -145,6 +145,22 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
   for (int b = 0; b < nbr && e == cudaSuccess; ++b)
     e = cudaEventCreateWithFlags(&join[b], cudaEventDisableTiming);
+  // overlap schedules: per-branch high-priority update streams (kernel nodes
+  // take the capturing stream's priority; the graph runs with node priorities)
+  const bool overlap = sch.overlap && nbr > 1;
+  cudaStream_t up[kMaxBranches] = {};
+  cudaEvent_t ev_done[kMaxBranches] = {}, up_done[kMaxBranches] = {};
+  cudaEvent_t phase = nullptr;
+  if (overlap && e == cudaSuccess) {
+    int least = 0, greatest = 0;
+    e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    for (int b = 0; b < nbr && e == cudaSuccess; ++b) {
+      e = cudaStreamCreateWithPriority(&up[b], cudaStreamNonBlocking, greatest);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_done[b], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&up_done[b], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&phase, cudaEventDisableTiming);
+  }
   // the capture streams must see the uploads made on `st`
   cudaEvent_t ready = nullptr;
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
@@ -156,8 +172,21 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
     e = cudaEventRecord(fork, cap[0]);
     for (int b = 1; b < nbr && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(cap[b], fork, 0);
     for (int t = 0; t < sch.graph_ticks && e == cudaSuccess; ++t)
-      for (int b = 0; b < nbr && e == cudaSuccess; ++b)
-        e = tick(cap[b], b, side[b].fork ? &side[b] : nullptr);
+      for (int b = 0; b < nbr && e == cudaSuccess; ++b) {
+        const EvalSide* sd = side[b].fork ? &side[b] : nullptr;
+        if (!overlap) {
+          e = tick(cap[b], b, sd);
+          continue;
+        }
+        if (t == 0 && b > 0) e = cudaStreamWaitEvent(cap[b], phase, 0);
+        if (e == cudaSuccess) e = eval_launch(ev[b].plan, cap[b], sd);
+        if (e == cudaSuccess && t == 0 && b == 0) e = cudaEventRecord(phase, cap[0]);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_done[b], cap[b]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(up[b], ev_done[b], 0);
+        if (e == cudaSuccess) e = update(up[b], b);
+        if (e == cudaSuccess) e = cudaEventRecord(up_done[b], up[b]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(cap[b], up_done[b], 0);
+      }
     for (int b = 1; b < nbr && e == cudaSuccess; ++b) {
       e = cudaEventRecord(join[b], cap[b]);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(cap[0], join[b], 0);
@@ -165,11 +194,15 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
     cudaError_t e2 = cudaStreamEndCapture(cap[0], &graph);
     if (e == cudaSuccess) e = e2;
   }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e == cudaSuccess)
+    e = cudaGraphInstantiate(&exec, graph, overlap ? cudaGraphInstantiateFlagUseNodePriority : 0);
   if (graph) cudaGraphDestroy(graph);
   for (int b = 0; b < nbr; ++b) {
     if (cap[b]) cudaStreamDestroy(cap[b]);
     if (join[b]) cudaEventDestroy(join[b]);
+    if (up[b]) cudaStreamDestroy(up[b]);
+    if (ev_done[b]) cudaEventDestroy(ev_done[b]);
+    if (up_done[b]) cudaEventDestroy(up_done[b]);
     for (int u = 0; u < 2; ++u) {
       if (side[b].aux[u]) cudaStreamDestroy(side[b].aux[u]);
       if (side[b].join[u]) cudaEventDestroy(side[b].join[u]);
@@ -177,6 +210,7 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
     if (side[b].fork) cudaEventDestroy(side[b].fork);
   }
   if (fork) cudaEventDestroy(fork);
+  if (phase) cudaEventDestroy(phase);
   if (ready) cudaEventDestroy(ready);
   if (e != cudaSuccess) return cuda_fail(e, "tick graph capture");
   return CCO_OK;
@@ -185,6 +219,10 @@ int TickPlan::build(const LaneTable& T, const Schedule& sch, cudaStream_t st) {
 cudaError_t TickPlan::tick(cudaStream_t s, int b, const EvalSide* side) const {
   cudaError_t e = eval_launch(ev[b].plan, s, side);
   if (e != cudaSuccess) return e;
+  return update(s, b);
+}
+
+cudaError_t TickPlan::update(cudaStream_t s, int b) const {
   if (method == Method::Flow) return flow_update(fl[b], s);
   if (method == Method::Md) return md_update(md[b], s);
   return method == Method::Descent ? descent_update(ds[b], s) : lbfgs_update(lb[b], s);
@@ -222,7 +260,9 @@ void LaneTable::release(cudaStream_t st) {
 // ------------------------------------------------------------ the tick driver
 namespace {
 
-// Candidate schedules of the online tuner: branch counts 1..4.
+// Candidate schedules of the online tuner: branch counts 1..4, and two or
+// three branches in overlap (update kernels at high priority, branches half a
+// tick apart).
 std::vector<Schedule> candidates(int B) {
   std::vector<Schedule> c;
   for (int nb = 1; nb <= kMaxBranches; ++nb) {
@@ -230,6 +270,14 @@ std::vector<Schedule> candidates(int B) {
     Schedule s;
     s.branches = nb;
     s.graph_ticks = 16;
+    c.push_back(s);
+  }
+  for (int nb = 2; nb <= 3; ++nb) {
+    if (B / nb < 8) break;
+    Schedule s;
+    s.branches = nb;
+    s.graph_ticks = 16;
+    s.overlap = 1;
     c.push_back(s);
   }
   return c;
@@ -327,6 +375,7 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
   bool done = false;
 
   const int force_br = env_int("CCO_BRANCHES", 0), force_gt = env_int("CCO_GRAPH_TICKS", 0);
+  const int force_ov = env_int("CCO_OVERLAP", -1);
   const bool tune = env_int("CCO_AUTOTUNE", 1) != 0;
   const bool compact = env_int("CCO_COMPACT", 1) != 0;
 
@@ -363,9 +412,10 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
     C.md.lanes = C.d_refs;
     C.md.B = (int)C.refs.size();
     Schedule s;
-    if (force_br > 0 || force_gt > 0) {
+    if (force_br > 0 || force_gt > 0 || force_ov >= 0) {
       if (force_br > 0) s.branches = force_br;
       if (force_gt > 0) s.graph_ticks = force_gt;
+      if (force_ov >= 0) s.overlap = force_ov;
     } else if (!schedule_cached(C.probs, C.shape.method, &s) && tune) {
       defer_tune = C.shape.method == Method::Lbfgs && ticks < kTuneAfterTicks;
       if (!defer_tune) {
@@ -648,6 +698,7 @@ int relax_descent_set(cco_problem* const* probs, int B, cudaStream_t st, const d
   out->ticks = rs.ticks;
   out->launches = rs.launches + 3 + pr.launches;
   out->branches = rs.schedule.branches;
+  out->overlap = rs.schedule.overlap;
   out->graph_ticks = rs.schedule.graph_ticks;
   pr.release(st);
   T.release(st);
@@ -717,6 +768,7 @@ int relax_lbfgs_set(cco_problem* const* probs, int B, cudaStream_t st, const dou
   out->ticks = rs.ticks;
   out->launches = rs.launches + 3;
   out->branches = rs.schedule.branches;
+  out->overlap = rs.schedule.overlap;
   out->graph_ticks = rs.schedule.graph_ticks;
   T.release(st);
   cudaFreeAsync(records, st);

@@ -78,6 +78,8 @@ class RelaxOutC(ctypes.Structure):
         ("launches", ctypes.c_int64),
         ("branches", ctypes.c_int32),
         ("graph_ticks", ctypes.c_int32),
+        ("overlap", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

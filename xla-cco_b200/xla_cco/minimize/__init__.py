@@ -109,6 +109,7 @@ def _call_relax(fn: str, first: Any, dev: Any, b: int, s0_ptr: int, cset: Any, c
     out["ticks"] = int(co.ticks)
     out["launches"] = int(co.launches)
     out["schedule"] = (int(co.branches), int(co.graph_ticks))
+    out["overlap"] = bool(co.overlap)
 
 
 def relax_device(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSSettings],
@@ -210,6 +211,7 @@ def relax_external(energy: Any, s0: Any, settings: Union[DescentSettings, LBFGSS
     out["ticks"] = ticks
     out["launches"] = 0
     out["schedule"] = (0, 0)
+    out["overlap"] = False
     return out
 
 
