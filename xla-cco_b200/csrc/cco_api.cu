@@ -281,20 +281,20 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     }
   }
   // GEMM pass 1: runs grouped kGemmRows at a time by length, each group's
-  // last-axis range cut into kGemmCols windows. Used when at least half of
-  // the computed grid cells (rows counted by the warp's 6) are k-set rows
+  // last-axis range cut into column windows. Used when the blocks cost at
+  // most 8 FMAs per k-set row and particle: m >= cells / 2, cells counted with
+  // the warps' 6-row granularity (a folded d = 2 cell serves two rows)
   // (CCO_PASS1_GEMM=0 turns it off).
   std::vector<GemmRun> grun;
   std::vector<GemmBlock> gblk;
   {
     const char* env = getenv("CCO_PASS1_GEMM");
     const bool allow = d >= 2 && !(env && atoi(env) == 0);
-    int c0 = 0, c1 = 0;      // widest group prefix windows
-    double computed = 0.0;   // grid cells the blocks multiply
     // d = 2 folds the last axis: columns are c = |n|, a run [a, b] covers
-    // [ca, cb] (its folded range), and one cell (run, c) yields C(c) and C(-c)
+    // [ca, cb] (its folded range), and one cell (run, c) yields C(c) and C(-c).
+    // Its window width is 16 cq columns (cq = 1..3), the width that computes
+    // the fewest cells for this k-set (the widest on ties: fewer blocks).
     const bool fold = d == 2;
-    const int cols = fold ? kGemmColsF : kGemmCols;
     auto fa = [fold](const GemmRun& g) {
       return !fold ? g.a : (g.a <= 0 && g.b >= 0) ? 0 : std::min(std::abs(g.a), std::abs(g.b));
     };
@@ -303,41 +303,63 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     std::stable_sort(sorted.begin(), sorted.end(), [&](const GemmRun& x, const GemmRun& y) {
       return (fb(x) - fa(x)) > (fb(y) - fa(y));
     });
-    for (size_t r0 = 0; r0 < sorted.size(); r0 += kGemmRows) {
-      const int nrun = (int)std::min<size_t>(kGemmRows, sorted.size() - r0);
-      int lo = 1 << 30, hi = -(1 << 30);
-      int gm0 = 1 << 30, gM0 = -(1 << 30), gm1 = 1 << 30, gM1 = -(1 << 30);
-      for (int r = 0; r < nrun; ++r) {
-        const GemmRun& g = sorted[r0 + r];
-        lo = std::min(lo, fa(g));
-        hi = std::max(hi, fb(g));
-        gm0 = std::min(gm0, g.n0);
-        gM0 = std::max(gM0, g.n0);
-        gm1 = std::min(gm1, g.n1);
-        gM1 = std::max(gM1, g.n1);
+    int c0 = 0, c1 = 0;      // widest group prefix windows
+    double computed = 0.0;   // grid cells the blocks multiply (4 FMAs per particle each)
+    auto group = [&](int cols) {
+      grun.clear();
+      gblk.clear();
+      c0 = c1 = 0;
+      computed = 0.0;
+      for (size_t r0 = 0; r0 < sorted.size(); r0 += kGemmRows) {
+        const int nrun = (int)std::min<size_t>(kGemmRows, sorted.size() - r0);
+        int lo = 1 << 30, hi = -(1 << 30);
+        int gm0 = 1 << 30, gM0 = -(1 << 30), gm1 = 1 << 30, gM1 = -(1 << 30);
+        for (int r = 0; r < nrun; ++r) {
+          const GemmRun& g = sorted[r0 + r];
+          lo = std::min(lo, fa(g));
+          hi = std::max(hi, fb(g));
+          gm0 = std::min(gm0, g.n0);
+          gM0 = std::max(gM0, g.n0);
+          gm1 = std::min(gm1, g.n1);
+          gM1 = std::max(gM1, g.n1);
+        }
+        // each group's prefix tables cover only its own prefixes
+        const int gc0 = gM0 - gm0 + 1, gc1 = d >= 3 ? gM1 - gm1 + 1 : 0;
+        c0 = std::max(c0, gc0);
+        c1 = std::max(c1, gc1);
+        const int run0 = (int)grun.size();
+        for (int r = 0; r < nrun; ++r) grun.push_back(sorted[r0 + r]);
+        // warps whose 6 rows lie past the group's runs skip their products
+        computed += (double)((nrun + 5) / 6 * 6) * cols * ((hi - lo) / cols + 1);
+        for (int w = lo; w <= hi; w += cols) {
+          GemmBlock b{};
+          b.run0 = run0;
+          b.nrun = nrun;
+          b.lo = w;
+          b.nb = std::min(cols, hi - w + 1);
+          b.m0 = gm0;
+          b.c0 = gc0;
+          b.m1 = d >= 3 ? gm1 : 0;
+          b.c1 = gc1;
+          gblk.push_back(b);
+        }
       }
-      // each group's prefix tables cover only its own prefixes
-      const int gc0 = gM0 - gm0 + 1, gc1 = d >= 3 ? gM1 - gm1 + 1 : 0;
-      c0 = std::max(c0, gc0);
-      c1 = std::max(c1, gc1);
-      const int run0 = (int)grun.size();
-      for (int r = 0; r < nrun; ++r) grun.push_back(sorted[r0 + r]);
-      // warps whose 6 rows lie past the group's runs skip their products
-      // (output slots: a folded cell holds two)
-      computed += (double)((nrun + 5) / 6 * 6) * cols * ((hi - lo) / cols + 1) * (fold ? 2 : 1);
-      for (int w = lo; w <= hi; w += cols) {
-        GemmBlock b{};
-        b.run0 = run0;
-        b.nrun = nrun;
-        b.lo = w;
-        b.nb = std::min(cols, hi - w + 1);
-        b.m0 = gm0;
-        b.c0 = gc0;
-        b.m1 = d >= 3 ? gm1 : 0;
-        b.c1 = gc1;
-        gblk.push_back(b);
+    };
+    int cols = kGemmCols;
+    if (fold) {
+      int best = 1;
+      double best_cells = 0.0;
+      for (int cq = 1; cq <= kGemmFoldMaxCq; ++cq) {
+        group(16 * cq);
+        if (cq == 1 || computed <= best_cells) {
+          best = cq;
+          best_cells = computed;
+        }
       }
+      cols = 16 * best;
+      P.gcq = best;
     }
+    group(cols);
     const double cells = computed;
     P.gemm = allow && !runs.empty() && c0 <= kGemmMaxPrefix && c1 <= kGemmMaxPrefix &&
              (double)m >= 0.5 * cells;

@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kGemmThreads, 4) k_pass1_gemm(EvalPlan plan) {
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
   if constexpr (D == 2)
-    pass1_gemm_body_d2(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
+    pass1_gemm_d2(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
   else
     pass1_gemm_body<D>(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
 }
@@ -201,7 +201,8 @@ size_t eval_smem1(const ProbDev& p) {
 size_t eval_smemG(const ProbDev& p) {
   if (!p.gemm) return 0;
   if (p.d == 2)   // two table sets (prefix, last axis) and two root sets
-    return (size_t)kGemmChunk * (2 * (p.gs0 + kGemmZStrideF) + 2 * p.d) * sizeof(double2);
+    return (size_t)kGemmChunk * (2 * (p.gs0 + gemm_fold_zstride(p.gcq)) + 2 * p.d) *
+           sizeof(double2);
   const int s1 = p.d == 3 ? p.gs1 : 0;
   return (size_t)kGemmChunk * (p.gs0 + s1 + kGemmZStride + kGemmRows + 2 * p.d) *
          sizeof(double2);

@@ -808,13 +808,15 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
 // c = |n|, and with A = a + ib and z^c = u + iv the four sums P1 = sum a u,
 // P2 = sum b v, P3 = sum a v, P4 = sum b u give C(c) = (P1 - P2) + i (P3 + P4)
 // and C(-c) = A conj(z^c) summed = (P1 + P2) + i (P4 - P3): four FMAs per
-// cell and particle for two k-set rows. Each thread accumulates 3 runs x 2
-// columns (tn, tn + 16). The tables are double-buffered: while the CTA
+// cell and particle for two k-set rows. Each thread accumulates 3 runs x CQ
+// columns (tn, tn + 16, ...). The tables are double-buffered: while the CTA
 // multiplies chunk c it fills chunk c + 1 (and the roots of chunk c + 2), one
 // barrier per chunk. Rows past the group's runs read the zero column c0.
+// CQ: columns per thread (tn, tn + 16, ...), the problem's window is 16 CQ.
+template <int CQ>
 __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int tile, int blk,
                                    double2* smem) {
-  constexpr int KC = kGemmChunk, D = 2, ZS = kGemmZStrideF;
+  constexpr int KC = kGemmChunk, D = 2, ZS = gemm_fold_zstride(CQ), W = 16 * CQ;
   const GemmBlock B = P.gblk[blk];
   const int j0 = tile * kPass1Tile;
   const int nj = min(kPass1Tile, P.N - j0);
@@ -830,11 +832,11 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
     const int r = 3 * tr + i;
     off[i] = r < B.nrun ? P.grun[B.run0 + r].n0 - B.m0 : zc;
   }
-  double p1[3][2], p2[3][2], p3[3][2], p4[3][2];
+  double p1[3][CQ], p2[3][CQ], p3[3][CQ], p4[3][CQ];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int q = 0; q < 2; ++q) p1[i][q] = p2[i][q] = p3[i][q] = p4[i][q] = 0.0;
+    for (int q = 0; q < CQ; ++q) p1[i][q] = p2[i][q] = p3[i][q] = p4[i][q] = 0.0;
   const int L = P.gL, u0 = P.gu0, uz = P.guz;
   const int nch = (nj + KC - 1) / KC;
   auto fill = [&](int c) {   // tables of chunk c into buffer c & 1 (roots in R[c & 1])
@@ -851,7 +853,7 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
           fill_powers(T0 + j * s0, L * q, min(L, c0 - L * q), B.m0, live ? sj[0] : 0.0, zs[j * D]);
       } else {
         const int qq = q - u0;
-        fill_powers(Z + j * ZS, L * qq, min(L, kGemmColsF - L * qq), B.lo, live ? sj[1] : 0.0,
+        fill_powers(Z + j * ZS, L * qq, min(L, W - L * qq), B.lo, live ? sj[1] : 0.0,
                     zs[j * D + 1]);
       }
     }
@@ -870,15 +872,15 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
     const double2* Z = T0 + KC * s0;
     const int kc = rows_live ? min(KC, nj - c * KC) : 0;
     for (int j = 0; j < kc; ++j) {
-      double2 a[3], z[2];
+      double2 a[3], z[CQ];
 #pragma unroll
       for (int i = 0; i < 3; ++i) a[i] = T0[j * s0 + off[i]];
 #pragma unroll
-      for (int q = 0; q < 2; ++q) z[q] = Z[j * ZS + tn + 16 * q];
+      for (int q = 0; q < CQ; ++q) z[q] = Z[j * ZS + tn + 16 * q];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
+        for (int q = 0; q < CQ; ++q) {
           p1[i][q] = fma(a[i].x, z[q].x, p1[i][q]);
           p2[i][q] = fma(a[i].y, z[q].y, p2[i][q]);
           p3[i][q] = fma(a[i].x, z[q].y, p3[i][q]);
@@ -894,7 +896,7 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
     if (r < B.nrun) {
       const GemmRun g = P.grun[B.run0 + r];
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
+      for (int q = 0; q < CQ; ++q) {
         const int col = tn + 16 * q;
         const int cv = B.lo + col;
         if (col < B.nb) {
@@ -906,6 +908,14 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
       }
     }
   }
+}
+
+// The folded d = 2 body at the problem's window width.
+__device__ __forceinline__ void pass1_gemm_d2(const ProbDev& P, const EvalLane& ln, int tile,
+                                              int blk, double2* smem) {
+  if (P.gcq == 1) pass1_gemm_body_d2<1>(P, ln, tile, blk, smem);
+  else if (P.gcq == 2) pass1_gemm_body_d2<2>(P, ln, tile, blk, smem);
+  else pass1_gemm_body_d2<3>(P, ln, tile, blk, smem);
 }
 
 }  // namespace

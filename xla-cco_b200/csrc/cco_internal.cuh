@@ -51,10 +51,11 @@ static_assert(sizeof(SegHdr) == 32, "segment header is two 16-byte loads");
 // a (group, window) is a block, one CTA per (lane, tile, block).
 constexpr int kGemmRows = 24, kGemmCols = 48, kGemmChunk = 16, kGemmThreads = 128;
 constexpr int kGemmZStride = kGemmCols + 1;   // odd row stride: table writes spread over banks
-// d = 2 folds the last axis: a block's columns are |n| (kGemmColsF of them)
-// and the four real products of A z^|n| give both C(n) and C(-n).
-constexpr int kGemmColsF = 32;
-constexpr int kGemmZStrideF = kGemmColsF + 1;
+// d = 2 folds the last axis: a block's columns are |n| (16 cq of them, cq
+// per problem, 1..kGemmFoldMaxCq) and the four real products of A z^|n|
+// give both C(n) and C(-n).
+constexpr int kGemmFoldMaxCq = 3;
+__host__ __device__ constexpr int gemm_fold_zstride(int cq) { return 16 * cq + 1; }
 constexpr int kGemmMaxPrefix = 128;   // table entries per prefix axis
 constexpr int kGemmMaxRun = 16;       // longest power chain between FP64 sincospi seeds
 struct GemmRun {
@@ -86,6 +87,7 @@ struct ProbDev {
   int ngblk, gm0, gc0, gm1, gc1;   // GEMM blocks; gc0, gc1: the widest group prefix windows
   int gs0, gs1;              // their shared-memory row strides (odd)
   int gL, gu0, gu1, guz;     // table fill: gL entries per unit; units per particle per table
+  int gcq, gpad_;            // d = 2: folded window of 16 gcq columns
   const GemmBlock* gblk;
   const GemmRun* grun;
   double vol;                // V

@@ -260,9 +260,10 @@ void LaneTable::release(cudaStream_t st) {
 // ------------------------------------------------------------ the tick driver
 namespace {
 
-// Candidate schedules of the online tuner: branch counts 1..4, and two or
-// three branches in overlap (update kernels at high priority, branches half a
-// tick apart).
+// Candidate schedules of the online tuner: branch counts 1..4. (The overlap
+// form, CCO_OVERLAP=1, measured slower than plain branches on the 256-lane
+// d = 2 relax - 906 vs 955 relaxations/s at two branches - and is not a
+// candidate.)
 std::vector<Schedule> candidates(int B) {
   std::vector<Schedule> c;
   for (int nb = 1; nb <= kMaxBranches; ++nb) {
@@ -270,14 +271,6 @@ std::vector<Schedule> candidates(int B) {
     Schedule s;
     s.branches = nb;
     s.graph_ticks = 16;
-    c.push_back(s);
-  }
-  for (int nb = 2; nb <= 3; ++nb) {
-    if (B / nb < 8) break;
-    Schedule s;
-    s.branches = nb;
-    s.graph_ticks = 16;
-    s.overlap = 1;
     c.push_back(s);
   }
   return c;
