@@ -1002,9 +1002,11 @@ def run_cli(args) -> None:
 
 
 def run_profile(args) -> None:
-    """Kernel-level profiling driver (run under ncu): no timing, no JSON.
+    """Kernel-level profiling driver (run under ncu).
     --profile-shape N,d,chi profiles another system than the headline one.
-    Without ncu it prints the device time per evaluation (eval mode)."""
+    Without ncu it prints the device time per evaluation (eval mode) or per
+    relaxation and tick (relax mode, CUDA events; the first rep includes the
+    schedule tuning)."""
     import torch
 
     from xla_cco import LBFGSSettings
@@ -1036,7 +1038,17 @@ def run_profile(args) -> None:
                           "ms_per_eval": ms, "tflops": tf}), flush=True)
     else:
         for _ in range(args.reps):
-            relax_device(energy, s_dev, LBFGSSettings(energy_tol=TOL))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out = relax_device(energy, s_dev, LBFGSSettings(energy_tol=TOL))
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            ticks = int(out["ticks"])
+            print(json.dumps({"profile": "relax", "n": n, "d": d, "batch": args.batch, "ms": ms,
+                              "ticks": ticks, "us_per_tick": 1e3 * ms / max(ticks, 1),
+                              "evals_per_lane": [int(v) for v in out["n_evals"].tolist()][:8],
+                              "schedule": list(out["schedule"])}), flush=True)
     torch.cuda.synchronize()
 
 
