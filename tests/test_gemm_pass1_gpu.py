@@ -20,10 +20,13 @@ from xla_cco.kvectors import enumerate_kvectors, k_outer_from_ka, ka_from_chi
 
 pytestmark = pytest.mark.gpu
 
-# dense k-sets that take the GEMM form (d = 2 incl. a 108-entry prefix table, d = 3)
-CASES = [(2, 1000, 0.40, 5), (2, 600, 0.49, 3), (2, 20000, 0.45, 1), (3, 20000, 0.45, 1)]
-# sparse ones that keep the per-segment kernel
-SEGMENT_ONLY = [(2, 333, 0.30), (3, 4000, 0.45), (1, 500, 0.40)]
+# k-sets that take the (folded) GEMM form: d = 2 with window widths 16 and 32
+# columns and a 108-entry prefix table, d = 3 with one and several run groups
+CASES = [(2, 1000, 0.40, 5), (2, 600, 0.49, 3), (2, 333, 0.30, 3), (2, 20000, 0.45, 1),
+         (3, 4000, 0.45, 2), (3, 20000, 0.45, 1)]
+# sparse ones (folded cells above 8 FMAs per k-set row) and 1-D ones keep the
+# per-segment kernel
+SEGMENT_ONLY = [(3, 400, 0.30), (3, 120, 0.30), (1, 500, 0.40)]
 
 
 def _energy(n, d, chi):

@@ -283,22 +283,21 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   // GEMM pass 1: runs grouped kGemmRows at a time by length, each group's
   // last-axis range cut into column windows. Used when the blocks cost at
   // most 8 FMAs per k-set row and particle: m >= cells / 2, cells counted with
-  // the warps' 6-row granularity (a folded d = 2 cell serves two rows)
+  // the warps' 6-row granularity (a folded cell serves two rows)
   // (CCO_PASS1_GEMM=0 turns it off).
   std::vector<GemmRun> grun;
   std::vector<GemmBlock> gblk;
   {
     const char* env = getenv("CCO_PASS1_GEMM");
     const bool allow = d >= 2 && !(env && atoi(env) == 0);
-    // d = 2 folds the last axis: columns are c = |n|, a run [a, b] covers
+    // The last axis is folded: columns are c = |n|, a run [a, b] covers
     // [ca, cb] (its folded range), and one cell (run, c) yields C(c) and C(-c).
     // Its window width is 16 cq columns (cq = 1..3), the width that computes
     // the fewest cells for this k-set (the widest on ties: fewer blocks).
-    const bool fold = d == 2;
-    auto fa = [fold](const GemmRun& g) {
-      return !fold ? g.a : (g.a <= 0 && g.b >= 0) ? 0 : std::min(std::abs(g.a), std::abs(g.b));
+    auto fa = [](const GemmRun& g) {
+      return (g.a <= 0 && g.b >= 0) ? 0 : std::min(std::abs(g.a), std::abs(g.b));
     };
-    auto fb = [fold](const GemmRun& g) { return !fold ? g.b : std::max(std::abs(g.a), std::abs(g.b)); };
+    auto fb = [](const GemmRun& g) { return std::max(std::abs(g.a), std::abs(g.b)); };
     std::vector<GemmRun> sorted = runs;
     std::stable_sort(sorted.begin(), sorted.end(), [&](const GemmRun& x, const GemmRun& y) {
       return (fb(x) - fa(x)) > (fb(y) - fa(y));
@@ -345,20 +344,17 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
         }
       }
     };
-    int cols = kGemmCols;
-    if (fold) {
-      int best = 1;
-      double best_cells = 0.0;
-      for (int cq = 1; cq <= kGemmFoldMaxCq; ++cq) {
-        group(16 * cq);
-        if (cq == 1 || computed <= best_cells) {
-          best = cq;
-          best_cells = computed;
-        }
+    int best = 1;
+    double best_cells = 0.0;
+    for (int cq = 1; cq <= kGemmFoldMaxCq; ++cq) {
+      group(16 * cq);
+      if (cq == 1 || computed <= best_cells) {
+        best = cq;
+        best_cells = computed;
       }
-      cols = 16 * best;
-      P.gcq = best;
     }
+    const int cols = 16 * best;
+    P.gcq = best;
     group(cols);
     const double cells = computed;
     P.gemm = allow && !runs.empty() && c0 <= kGemmMaxPrefix && c1 <= kGemmMaxPrefix &&

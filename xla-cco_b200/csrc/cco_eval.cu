@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(kGemmThreads, 4) k_pass1_gemm(EvalPlan plan) {
   if constexpr (D == 2)
     pass1_gemm_d2(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
   else
-    pass1_gemm_body<D>(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
+    pass1_gemm_d3(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
 }
 
 // One kernel per dimension D and arithmetic keeps each kernel's code small:
@@ -204,7 +204,7 @@ size_t eval_smemG(const ProbDev& p) {
     return (size_t)kGemmChunk * (2 * (p.gs0 + gemm_fold_zstride(p.gcq)) + 2 * p.d) *
            sizeof(double2);
   const int s1 = p.d == 3 ? p.gs1 : 0;
-  return (size_t)kGemmChunk * (p.gs0 + s1 + kGemmZStride + kGemmRows + 2 * p.d) *
+  return (size_t)kGemmChunk * (p.gs0 + s1 + gemm_fold_zstride(p.gcq) + kGemmRows + 2 * p.d) *
          sizeof(double2);
 }
 

@@ -702,17 +702,49 @@ __device__ __forceinline__ void chunk_roots(double2* zs, const double* s, int jb
   }
 }
 
-// Pass 1 of one (lane, tile, block) as a complex GEMM over the tile's
-// particles, kGemmChunk at a time: the tables of the chunk (prefix powers
-// per axis, last-axis powers for the block's window) and the A rows are
-// built in shared memory, then every thread accumulates a 3 x 3 tile of
-// C[run][n] (runs 3 tr .. 3 tr + 2, columns tn, tn + 16, tn + 32) with four
-// FMAs per complex product. Each grid cell of the k-set is written once.
-// The roots z of the next chunk are formed while the A rows are built.
-template <int D>
+// The outputs of a folded block: cell (run 3 tr + i, column lo + tn + 16 q)
+// holds C(c) = (P1 - P2) + i (P3 + P4) and C(-c) = (P1 + P2) + i (P4 - P3);
+// each lands in its run's row if the run contains that n.
+template <int CQ>
+__device__ __forceinline__ void gemm_fold_store(const ProbDev& P, const EvalLane& ln, int tile,
+                                                const GemmBlock& B, int tr, int tn,
+                                                const double (&p1)[3][CQ],
+                                                const double (&p2)[3][CQ],
+                                                const double (&p3)[3][CQ],
+                                                const double (&p4)[3][CQ]) {
+  double2* out = ln.part + (size_t)tile * P.M;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int r = 3 * tr + i;
+    if (r < B.nrun) {
+      const GemmRun g = P.grun[B.run0 + r];
+#pragma unroll
+      for (int q = 0; q < CQ; ++q) {
+        const int col = tn + 16 * q;
+        const int cv = B.lo + col;
+        if (col < B.nb) {
+          if (cv >= g.a && cv <= g.b)
+            out[g.kstart + (cv - g.a)] = make_double2(p1[i][q] - p2[i][q], p3[i][q] + p4[i][q]);
+          if (cv > 0 && -cv >= g.a && -cv <= g.b)
+            out[g.kstart + (-cv - g.a)] = make_double2(p1[i][q] + p2[i][q], p4[i][q] - p3[i][q]);
+        }
+      }
+    }
+  }
+}
+
+// Pass 1 of one (lane, tile, block) of a 3-D k-set as a complex GEMM over
+// the tile's particles, kGemmChunk at a time: the tables of the chunk (prefix
+// powers per axis, last-axis powers for the block's window) and the A rows
+// (A = T0 T1, the runs' prefix phases) are built in shared memory. The last
+// axis is folded as in the d = 2 body: columns are c = |n2| and the four sums
+// P1..P4 of a cell give C(c) and C(-c). Each thread accumulates 3 runs x CQ
+// columns (tn, tn + 16, ...). Each k-set row is written once. The roots z of
+// the next chunk are formed while the A rows are built.
+template <int D, int CQ>
 __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, int blk,
                                 double2* smem) {
-  constexpr int KC = kGemmChunk;
+  constexpr int KC = kGemmChunk, ZS = gemm_fold_zstride(CQ), W = 16 * CQ;
   const GemmBlock B = P.gblk[blk];
   const int j0 = tile * kPass1Tile;
   const int nj = min(kPass1Tile, P.N - j0);
@@ -720,15 +752,15 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
   const int s0 = P.gs0, s1 = D == 3 ? P.gs1 : 0;
   double2* T0 = smem;                       // [KC][s0]
   double2* T1 = T0 + KC * s0;               // [KC][s1]
-  double2* Z = T1 + KC * s1;                // [KC][kGemmZStride]
-  double2* A = Z + KC * kGemmZStride;       // [KC][kGemmRows]
+  double2* Z = T1 + KC * s1;                // [KC][ZS]
+  double2* A = Z + KC * ZS;                 // [KC][kGemmRows]
   double2* R = A + KC * kGemmRows;          // [2][KC * D] roots, double-buffered
   const int tr = threadIdx.x >> 4, tn = threadIdx.x & 15;
-  double2 acc[3][3];
+  double p1[3][CQ], p2[3][CQ], p3[3][CQ], p4[3][CQ];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) acc[i][c] = make_double2(0.0, 0.0);
+    for (int q = 0; q < CQ; ++q) p1[i][q] = p2[i][q] = p3[i][q] = p4[i][q] = 0.0;
   const int L = P.gL, u0 = P.gu0, u1 = D == 3 ? P.gu1 : 0, uz = P.guz;
   chunk_roots<D>(R, ln.s, j0, min(KC, nj));
   int buf = 0;
@@ -751,8 +783,8 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
                       zs[j * D + 1]);
       } else {
         const int qq = q - u0 - u1;
-        fill_powers(Z + j * kGemmZStride, L * qq, min(L, kGemmCols - L * qq), B.lo,
-                    live ? sj[D - 1] : 0.0, zs[j * D + D - 1]);
+        fill_powers(Z + j * ZS, L * qq, min(L, W - L * qq), B.lo, live ? sj[D - 1] : 0.0,
+                    zs[j * D + D - 1]);
       }
     }
     __syncthreads();
@@ -771,36 +803,23 @@ __device__ void pass1_gemm_body(const ProbDev& P, const EvalLane& ln, int tile, 
     __syncthreads();
     const int kr = 6 * (threadIdx.x >> 5) < B.nrun ? kc : 0;   // warps past the runs skip
     for (int j = 0; j < kr; ++j) {
-      double2 a[3], z[3];
+      double2 a[3], z[CQ];
 #pragma unroll
       for (int i = 0; i < 3; ++i) a[i] = A[j * kGemmRows + 3 * tr + i];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) z[c] = Z[j * kGemmZStride + tn + 16 * c];
+      for (int q = 0; q < CQ; ++q) z[q] = Z[j * ZS + tn + 16 * q];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          acc[i][c].x = fma(a[i].x, z[c].x, acc[i][c].x);
-          acc[i][c].x = fma(-a[i].y, z[c].y, acc[i][c].x);
-          acc[i][c].y = fma(a[i].x, z[c].y, acc[i][c].y);
-          acc[i][c].y = fma(a[i].y, z[c].x, acc[i][c].y);
+        for (int q = 0; q < CQ; ++q) {
+          p1[i][q] = fma(a[i].x, z[q].x, p1[i][q]);
+          p2[i][q] = fma(a[i].y, z[q].y, p2[i][q]);
+          p3[i][q] = fma(a[i].x, z[q].y, p3[i][q]);
+          p4[i][q] = fma(a[i].y, z[q].x, p4[i][q]);
         }
     }
   }
-  double2* out = ln.part + (size_t)tile * P.M;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const int r = 3 * tr + i;
-    if (r < B.nrun) {
-      const GemmRun g = P.grun[B.run0 + r];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int col = tn + 16 * c;
-        const int n = B.lo + col;
-        if (col < B.nb && n >= g.a && n <= g.b) out[g.kstart + (n - g.a)] = acc[i][c];
-      }
-    }
-  }
+  gemm_fold_store<CQ>(P, ln, tile, B, tr, tn, p1, p2, p3, p4);
 }
 
 // d = 2: the A rows are a gather from the prefix table (A[r][j] = T0[j][n0(r)]),
@@ -889,25 +908,15 @@ __device__ void pass1_gemm_body_d2(const ProbDev& P, const EvalLane& ln, int til
     }
     __syncthreads();
   }
-  double2* out = ln.part + (size_t)tile * P.M;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const int r = 3 * tr + i;
-    if (r < B.nrun) {
-      const GemmRun g = P.grun[B.run0 + r];
-#pragma unroll
-      for (int q = 0; q < CQ; ++q) {
-        const int col = tn + 16 * q;
-        const int cv = B.lo + col;
-        if (col < B.nb) {
-          if (cv >= g.a && cv <= g.b)
-            out[g.kstart + (cv - g.a)] = make_double2(p1[i][q] - p2[i][q], p3[i][q] + p4[i][q]);
-          if (cv > 0 && -cv >= g.a && -cv <= g.b)
-            out[g.kstart + (-cv - g.a)] = make_double2(p1[i][q] + p2[i][q], p4[i][q] - p3[i][q]);
-        }
-      }
-    }
-  }
+  gemm_fold_store<CQ>(P, ln, tile, B, tr, tn, p1, p2, p3, p4);
+}
+
+// The folded 3-D body at the problem's window width.
+__device__ __forceinline__ void pass1_gemm_d3(const ProbDev& P, const EvalLane& ln, int tile,
+                                              int blk, double2* smem) {
+  if (P.gcq == 1) pass1_gemm_body<3, 1>(P, ln, tile, blk, smem);
+  else if (P.gcq == 2) pass1_gemm_body<3, 2>(P, ln, tile, blk, smem);
+  else pass1_gemm_body<3, 3>(P, ln, tile, blk, smem);
 }
 
 // The folded d = 2 body at the problem's window width.

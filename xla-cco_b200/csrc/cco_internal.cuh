@@ -46,15 +46,15 @@ static_assert(sizeof(SegHdr) == 32, "segment header is two 16-byte loads");
 // Pass 1 as a complex GEMM (problems where it is efficient, FP64 lanes): the
 // density of a particle tile on the grid (run r, last-axis n) is
 // C[r][n] = sum_j A[r][j] Z[n][j] with A the run's prefix phase and Z the
-// last-axis power z_j^n. Runs are grouped kGemmRows at a time (sorted by
-// length) and each group's last-axis range is cut into windows of kGemmCols;
-// a (group, window) is a block, one CTA per (lane, tile, block).
-constexpr int kGemmRows = 24, kGemmCols = 48, kGemmChunk = 16, kGemmThreads = 128;
-constexpr int kGemmZStride = kGemmCols + 1;   // odd row stride: table writes spread over banks
-// d = 2 folds the last axis: a block's columns are |n| (16 cq of them, cq
-// per problem, 1..kGemmFoldMaxCq) and the four real products of A z^|n|
-// give both C(n) and C(-n).
+// last-axis power z_j^n. The last axis is folded: a block's columns are
+// c = |n|, and the four real products of A z^c give both C(c) and C(-c).
+// Runs are grouped kGemmRows at a time (sorted by folded length) and each
+// group's folded range is cut into windows of 16 cq columns (cq per problem,
+// 1..kGemmFoldMaxCq); a (group, window) is a block, one CTA per (lane, tile,
+// block).
+constexpr int kGemmRows = 24, kGemmChunk = 16, kGemmThreads = 128;
 constexpr int kGemmFoldMaxCq = 3;
+// odd row stride of the last-axis table: table writes spread over banks
 __host__ __device__ constexpr int gemm_fold_zstride(int cq) { return 16 * cq + 1; }
 constexpr int kGemmMaxPrefix = 128;   // table entries per prefix axis
 constexpr int kGemmMaxRun = 16;       // longest power chain between FP64 sincospi seeds

@@ -58,7 +58,7 @@ __device__ void persist_eval(const ProbDev& P, const EvalLane& ln, double2* smem
       const int items = P.ntile1 * P.ngblk;
       for (int it = 0; it < items; ++it) {
         if constexpr (D == 2) pass1_gemm_d2(P, ln, it / P.ngblk, it % P.ngblk, smem);
-        else pass1_gemm_body<D>(P, ln, it / P.ngblk, it % P.ngblk, smem);
+        else pass1_gemm_d3(P, ln, it / P.ngblk, it % P.ngblk, smem);
         __syncthreads();
       }
     }
