@@ -270,6 +270,7 @@ struct Schedule {
 };
 constexpr int kMaxBranches = 4;
 constexpr int kInflight = 3;    // graphs in flight before the host checks completion
+constexpr int kMaxInflight = 16;   // CCO_INFLIGHT bound (and the round bounds' slack)
 
 // Lane ranges [bounds[b], bounds[b + 1]) of the branches, balanced by the
 // evaluation work (N M) of each lane.

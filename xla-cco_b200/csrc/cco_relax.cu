@@ -335,10 +335,12 @@ int tune_schedule(const LaneTable& C, cudaStream_t st, int64_t max_ticks, int64_
   if (rc != CCO_OK) return rc;
   if (e != cudaSuccess) return cuda_fail(e, "schedule tuning");
   Schedule s = cand[best];
-  // graphs of about 3 ms of device work: launch overhead amortised, and the
-  // few graphs that run past the last lane's completion stay short
+  // graphs of about 8 ms of device work: with three in flight the device has
+  // ~20 ms queued, so a host thread descheduled on a busy host does not leave
+  // it idle; the graphs that run past the last lane's completion cost little
+  // (their kernels exit at once for finished lanes)
   const double tick_ms = ms[best] < 1e29f ? ms[best] : 0.2;
-  const int gt = (int)std::lround(3.0 / std::max(tick_ms, 1e-3));
+  const int gt = (int)std::lround(8.0 / std::max(tick_ms, 1e-3));
   s.graph_ticks = std::max(4, std::min(32, gt));
   *out = s;
   return CCO_OK;
@@ -354,13 +356,14 @@ int tune_schedule(const LaneTable& C, cudaStream_t st, int64_t max_ticks, int64_
 // compaction looks up or re-tunes the schedule for the smaller table.
 int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* stats) {
   const int B = (int)T.refs.size();
-  constexpr int kSlots = kInflight + 1;
+  const int inflight = std::max(1, std::min(kMaxInflight, env_int("CCO_INFLIGHT", kInflight)));
+  const int kSlots = inflight + 1;
   int64_t* d_status = nullptr;
   int64_t* h_status = pinned_status((size_t)kSlots * B);
   if (!h_status) return fail(CCO_ERR_OOM, "pinned status buffer");
   CCO_CUDA(pool_alloc(&d_status, sizeof(int64_t) * kSlots * B, st));
-  cudaEvent_t ev[kSlots];
-  int ver[kSlots] = {}, rows[kSlots] = {};
+  cudaEvent_t ev[kMaxInflight + 1];
+  int ver[kMaxInflight + 1] = {}, rows[kMaxInflight + 1] = {};
   for (int i = 0; i < kSlots; ++i) CCO_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
   int64_t ticks = 0, launches = 0;
   int rc = CCO_OK;
@@ -475,7 +478,7 @@ int run_lane_table(LaneTable& T, cudaStream_t st, int64_t max_ticks, RunStats* s
     ver[slot] = version;
     rows[slot] = n;
     ++launched;
-    if (e == cudaSuccess && launched - checked > kInflight) rc = land();
+    if (e == cudaSuccess && launched - checked > inflight) rc = land();
     if (rc == CCO_OK && e == cudaSuccess && !done && defer_tune && ticks >= kTuneAfterTicks) {
       P.release(st);   // the deferred tuning, on the same table
       rc = start();
@@ -677,7 +680,7 @@ int relax_descent_set(cco_problem* const* probs, int B, cudaStream_t st, const d
   a.B = B;
   a.lanes = T.d_refs;
   CCO_CUDA(descent_init(a, s0, st));
-  const int64_t max_ticks = 1 + a.max_iters + 4 * (kInflight + 1) * 32;
+  const int64_t max_ticks = 1 + a.max_iters + 4 * (kMaxInflight + 1) * 32;
   RunStats rs;
   PersistRun pr;
   rc = pr.start(T, st, max_ticks);
@@ -749,7 +752,7 @@ int relax_lbfgs_set(cco_problem* const* probs, int B, cudaStream_t st, const dou
   CCO_CUDA(lbfgs_init(A, s0, st));
   const int64_t max_ticks =
       1 + (int64_t)cfg->n_rescales * (cfg->max_evals_per_pass + cfg->max_linesearch_steps + 1) +
-      4 * (kInflight + 1) * 32;
+      4 * (kMaxInflight + 1) * 32;
   RunStats rs;
   rc = run_lane_table(T, st, max_ticks, &rs);
   if (rc == CCO_OK) {
@@ -965,7 +968,7 @@ extern "C" int cco_gradient_flow(cco_problem* const* problems, void* stream, int
     CCO_CUDA(upload(&d_dt0, v, st));
   }
   CCO_CUDA(flow_init(a, s0, d_mats, d_dt0, st));
-  const int64_t max_ticks = 2 + 6 * 4 * cfg->max_steps + 4 * (kInflight + 1) * 32;
+  const int64_t max_ticks = 2 + 6 * 4 * cfg->max_steps + 4 * (kMaxInflight + 1) * 32;
   RunStats rs;
   rc = run_lane_table(T, st, max_ticks, &rs);
   if (rc == CCO_OK) {
@@ -1050,7 +1053,7 @@ extern "C" int cco_md_run(cco_problem* const* problems, void* stream, int batch,
   CCO_CUDA(upload(&d_keys, std::vector<uint32_t>(keys, keys + 2 * (size_t)batch), st));
   if (acc0) CCO_CUDA(upload(&d_acc, std::vector<double>(acc0, acc0 + batch), st));
   CCO_CUDA(md_init(a, r0, v0, d_mats, d_keys, d_acc, st));
-  const int64_t max_ticks = 2 + cfg->n_steps + 4 * (kInflight + 1) * 32;
+  const int64_t max_ticks = 2 + cfg->n_steps + 4 * (kMaxInflight + 1) * 32;
   RunStats rs;
   rc = run_lane_table(T, st, max_ticks, &rs);
   if (rc == CCO_OK) {
@@ -1189,7 +1192,7 @@ extern "C" int cco_md_segment(cco_problem* p, void* stream, int batch, const dou
   if (e == cudaSuccess) e = md_seg_init(a, d_mats, st);
   if (e != cudaSuccess) rc = cuda_fail(e, "md segment setup");
   RunStats rs;
-  if (rc == CCO_OK) rc = run_lane_table(T, st, 2 + cfg->n_steps + 4 * (kInflight + 1) * 32, &rs);
+  if (rc == CCO_OK) rc = run_lane_table(T, st, 2 + cfg->n_steps + 4 * (kMaxInflight + 1) * 32, &rs);
   if (rc == CCO_OK) {
     e = md_seg_finalize(a, st);
     if (e != cudaSuccess) rc = cuda_fail(e, "md segment finalize");
