@@ -282,8 +282,9 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
   }
   // GEMM pass 1: runs grouped kGemmRows at a time by length, each group's
   // last-axis range cut into column windows. Used when the blocks cost at
-  // most 8 FMAs per k-set row and particle: m >= cells / 2, cells counted with
-  // the warps' 6-row granularity (a folded cell serves two rows)
+  // most 8 FMAs per k-set row and particle (4 for d = 3): m >= cells / 2
+  // (m >= cells), cells counted with the warps' 6-row granularity (a folded
+  // cell serves two rows)
   // (CCO_PASS1_GEMM=0 turns it off).
   std::vector<GemmRun> grun;
   std::vector<GemmBlock> gblk;
@@ -357,8 +358,13 @@ int cco_problem_create(int device, int d, int n_particles, int m, const int32_t*
     P.gcq = best;
     group(cols);
     const double cells = computed;
+    // d = 3 builds an A phase per chunk and only broke even with the
+    // per-segment kernel at about 3.5 FMAs per row (d=3 N=4000 chi=0.45: 1.480
+    // vs 1.481 ms per 32-lane evaluation; at 6.2 FMAs, N=2000 chi=0.20, it lost
+    // 4%), so 3-D k-sets take the GEMM form only at <= 4 FMAs per row
+    const double need = d == 3 ? 1.0 : 0.5;
     P.gemm = allow && !runs.empty() && c0 <= kGemmMaxPrefix && c1 <= kGemmMaxPrefix &&
-             (double)m >= 0.5 * cells;
+             (double)m >= need * cells;
     P.ngblk = (int)gblk.size();
     P.gm0 = 0;
     P.gc0 = c0;
