@@ -99,6 +99,13 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        # nvidia-smi's own start-up (driver and NVML initialisation) takes the
+        # driver for a moment; let it finish before the caller starts timing,
+        # so the timed region sees the steady 200 ms polling only
+        t0 = time.perf_counter()
+        while not self.lines and time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.02)
+        time.sleep(0.25)
 
     def _read(self) -> None:
         for line in self.proc.stdout:

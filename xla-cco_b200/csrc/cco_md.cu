@@ -213,52 +213,17 @@ __device__ __forceinline__ int record_slot(const MdArgs& a, int64_t step) {
 __device__ void observe_step(const MdArgs& a, const LaneRef& R, const MdView& w, MdState& S,
                              int d, double* red) {
   __shared__ double rcm[3];
-  __shared__ int snap_slot, trace_row;
   if (a.corrected) center_of_mass(R, w, d, rcm, red);
-  const bool wind = S.step % a.wind_every == 0;
-  if (threadIdx.x == 0) {
-    snap_slot = a.n_rec > 0 ? record_slot(a, S.step) : -1;
-    trace_row = (a.trace_every > 0 && a.trace_cap > 0 && S.step % a.trace_every == 0 &&
-                 S.trace_count < a.trace_cap) ? (int)S.trace_count : -1;
-  }
-  __syncthreads();
-  const int js = snap_slot, jt = trace_row;
   const size_t lane = (size_t)R.idx;
-  for (int c = threadIdx.x; c < a.w; c += blockDim.x) {
-    const double2 old = make_double2(w.rho_prev[2 * c], w.rho_prev[2 * c + 1]);
-    const bool active = c < a.nc || wind;
-    double2 nw = old;
-    if (active) nw = wave_rho(a, w, c, d, rcm);
-    const double delta = atan2(nw.y * old.x - nw.x * old.y, nw.x * old.x + nw.y * old.y);
-    const double s_old = (old.x * old.x + old.y * old.y) / R.n;
-    const double s_new = (nw.x * nw.x + nw.y * nw.y) / R.n;
-    const bool ok = active && s_old > a.phase_floor && s_new > a.phase_floor;
-    const double2 rp = active ? nw : old;
-    w.rho_prev[2 * c] = rp.x;
-    w.rho_prev[2 * c + 1] = rp.y;
-    if (ok) {
-      w.wind_abs[c] += fabs(delta);
-      w.wind_net[c] += delta;
-      w.n_valid[c] += 1.0;
-    }
-    w.sum_s[c] += (rp.x * rp.x + rp.y * rp.y) / R.n;
-    if (js >= 0) {
-      const size_t o = (lane * a.n_rec + js) * a.w + c;
-      a.io.snap_wind_abs[o] = w.wind_abs[c];
-      a.io.snap_wind_net[o] = w.wind_net[c];
-      a.io.snap_rho[2 * o] = rp.x;
-      a.io.snap_rho[2 * o + 1] = rp.y;
-    }
-    if (jt >= 0) {
-      const size_t o = (lane * a.trace_cap + jt) * a.w + c;
-      a.io.trace_rho[2 * o] = rp.x;
-      a.io.trace_rho[2 * o + 1] = rp.y;
-    }
-  }
-  if (js >= 0)
-    for (int e = threadIdx.x; e < R.nd; e += blockDim.x)
-      a.io.snap_r[(lane * a.n_rec + js) * R.nd + e] = w.r[e];
   if (threadIdx.x == 0) {
+    const int js = a.n_rec > 0 ? record_slot(a, S.step) : -1;
+    const int jt = (a.trace_every > 0 && a.trace_cap > 0 && S.step % a.trace_every == 0 &&
+                    S.trace_count < a.trace_cap) ? (int)S.trace_count : -1;
+    for (int q = 0; q < 3; ++q) S.obs_rcm[q] = a.corrected && q < d ? rcm[q] : 0.0;
+    S.obs_pending = 1;
+    S.obs_wind = S.step % a.wind_every == 0 ? 1 : 0;
+    S.obs_snap = js;
+    S.obs_trace = jt;
     if (js >= 0) {
       const size_t o = lane * a.n_rec + js;
       a.io.snap_step[o] = S.step;
@@ -272,6 +237,11 @@ __device__ void observe_step(const MdArgs& a, const LaneRef& R, const MdView& w,
       S.trace_count += 1;
     }
   }
+  __syncthreads();
+  // the positions of a snapshot, before the next step's drift moves them
+  if (S.obs_snap >= 0)
+    for (int e = threadIdx.x; e < R.nd; e += blockDim.x)
+      a.io.snap_r[(lane * a.n_rec + S.obs_snap) * R.nd + e] = w.r[e];
 }
 
 // Rows of rho_prev marked pending (NaN) get the current densities (the first
@@ -294,9 +264,15 @@ __global__ void __launch_bounds__(kUpdThreads) k_md_update(MdArgs a, double c, d
   const int lane = blockIdx.x;
   const LaneRef R = a.lanes[lane];
   const MdView w = md_view(R.rec, R.ld, a.w);
-  if (threadIdx.x == 0) S = *w.st;
+  if (threadIdx.x == 0) {
+    S = *w.st;
+    S.obs_pending = 0;   // the previous step's waves were observed by the last tick
+  }
   __syncthreads();
-  if (S.status != CCO_STATUS_RUNNING) return;
+  if (S.status != CCO_STATUS_RUNNING) {
+    if (threadIdx.x == 0 && w.st->obs_pending) w.st->obs_pending = 0;
+    return;
+  }
   const int d = R.nd / R.n;
   forces(R, w, S, d);
   __syncthreads();
@@ -379,6 +355,53 @@ __global__ void __launch_bounds__(kUpdThreads) k_md_update(MdArgs a, double c, d
   }
   __syncthreads();
   if (threadIdx.x == 0) *w.st = S;
+}
+
+// Per-wave observables of the step k_md_update just finished (segment runs),
+// one thread per wave over (lane, wave chunk) blocks: the wave's density
+// times exp(-i k . R_cm), the winding increment (atan2 of the phase change),
+// running sums, and the snapshot and trace rows. Waves are independent, so
+// spreading a lane's waves over blocks changes no result.
+__global__ void __launch_bounds__(kUpdThreads) k_md_observe(MdArgs a) {
+  const LaneRef R = a.lanes[blockIdx.x];
+  const MdView w = md_view(R.rec, R.ld, a.w);
+  const MdState* S = w.st;
+  if (!S->obs_pending) return;
+  const int c = blockIdx.y * blockDim.x + threadIdx.x;
+  if (c >= a.w) return;
+  const int d = R.nd / R.n;
+  const int js = S->obs_snap, jt = S->obs_trace;
+  const bool wind = S->obs_wind != 0;
+  const size_t lane = (size_t)R.idx;
+  const double2 old = make_double2(w.rho_prev[2 * c], w.rho_prev[2 * c + 1]);
+  const bool active = c < a.nc || wind;
+  double2 nw = old;
+  if (active) nw = wave_rho(a, w, c, d, S->obs_rcm);
+  const double delta = atan2(nw.y * old.x - nw.x * old.y, nw.x * old.x + nw.y * old.y);
+  const double s_old = (old.x * old.x + old.y * old.y) / R.n;
+  const double s_new = (nw.x * nw.x + nw.y * nw.y) / R.n;
+  const bool ok = active && s_old > a.phase_floor && s_new > a.phase_floor;
+  const double2 rp = active ? nw : old;
+  w.rho_prev[2 * c] = rp.x;
+  w.rho_prev[2 * c + 1] = rp.y;
+  if (ok) {
+    w.wind_abs[c] += fabs(delta);
+    w.wind_net[c] += delta;
+    w.n_valid[c] += 1.0;
+  }
+  w.sum_s[c] += (rp.x * rp.x + rp.y * rp.y) / R.n;
+  if (js >= 0) {
+    const size_t o = (lane * a.n_rec + js) * a.w + c;
+    a.io.snap_wind_abs[o] = w.wind_abs[c];
+    a.io.snap_wind_net[o] = w.wind_net[c];
+    a.io.snap_rho[2 * o] = rp.x;
+    a.io.snap_rho[2 * o + 1] = rp.y;
+  }
+  if (jt >= 0) {
+    const size_t o = (lane * a.trace_cap + jt) * a.w + c;
+    a.io.trace_rho[2 * o] = rp.x;
+    a.io.trace_rho[2 * o + 1] = rp.y;
+  }
 }
 
 // Fresh densities of the unconstrained waves at the probe positions (the
@@ -557,6 +580,10 @@ cudaError_t md_update(const MdArgs& a, cudaStream_t st) {
     k_md_waves<<<grid, kUpdThreads, 0, st>>>(a);
   }
   k_md_update<<<a.B, kUpdThreads, 0, st>>>(a, c, noise_var);
+  if (a.w > 0) {
+    const dim3 grid(a.B, (a.w + kUpdThreads - 1) / kUpdThreads);
+    k_md_observe<<<grid, kUpdThreads, 0, st>>>(a);
+  }
   return cudaGetLastError();
 }
 

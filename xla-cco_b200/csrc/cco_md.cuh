@@ -24,6 +24,11 @@ struct MdState {
   double temperature, time;    // segment runs: per-lane T, elapsed time
   double sum_kinetic, sum_phi, sum_phi2;
   double drift_limit;          // |E - e0| bound (< 0: no guard)
+  // observables of the step just finished, for k_md_observe (segment runs)
+  double obs_rcm[3];           // centre of mass at that step
+  int32_t obs_pending;         // 1: k_md_observe has this step's waves to do
+  int32_t obs_wind;            // the step was a wind step (unconstrained waves fresh)
+  int32_t obs_snap, obs_trace; // snapshot slot and trace row (-1: none)
 };
 constexpr int kMdHead = 64;
 static_assert(sizeof(MdState) <= (kMdHead - 1) * sizeof(double), "MdState outgrew its slot");

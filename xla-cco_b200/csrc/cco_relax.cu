@@ -230,9 +230,11 @@ cudaError_t TickPlan::update(cudaStream_t s, int b) const {
 
 int TickPlan::launches_per_tick() const {
   // the evaluation kernels each branch's plan issues + the update kernels
-  // (L-BFGS: probe, pass A, scalar, pass B; MD segments: + the wave sums)
+  // (L-BFGS: probe, pass A, scalar, pass B; MD segments: + the wave sums and
+  // the per-wave observables)
   const int md_waves = method == Method::Md && md[0].w > md[0].nc ? 1 : 0;
-  const int upd = method == Method::Lbfgs ? 4 : 1 + md_waves;
+  const int md_obs = method == Method::Md && md[0].w > 0 ? 1 : 0;
+  const int upd = method == Method::Lbfgs ? 4 : 1 + md_waves + md_obs;
   int n = 0;
   for (int b = 0; b < nbr; ++b) n += eval_kernels(ev[b].plan) + upd;
   return n;
