@@ -438,7 +438,8 @@ int cco_md_segment(cco_problem* p, void* stream, int batch, const double* basis,
  * results never depend on the schedule. This forgets every cached schedule.
  * The environment variables CCO_BRANCHES, CCO_GRAPH_TICKS and CCO_OVERLAP
  * (0 or 1) force a schedule, CCO_AUTOTUNE=0 keeps the default (2 branches,
- * 16 ticks, no overlap).
+ * 16 ticks, no overlap). CCO_INFLIGHT (1..16, default 3) sets how many
+ * graphs the driver keeps queued ahead of its completion checks.
  */
 int cco_schedule_reset(void);
 
