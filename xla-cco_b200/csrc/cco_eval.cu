@@ -98,14 +98,14 @@ __global__ void __launch_bounds__(kReduceChunk) k_reduce(EvalPlan plan) {
     const double2* __restrict__ col = ln.part + k;
     double2 t = col[0];
     int q = 1;
-    // eight tile rows in flight per step, added in tile order (the same sums
-    // as one row at a time; a lane of few wide tiles is latency-bound here)
-    for (; q + 8 <= nt; q += 8) {
-      double2 o[8];
+    // sixteen tile rows in flight per step, added in tile order (the same sums
+    // as one row at a time; a lone lane of many tiles is latency-bound here)
+    for (; q + 16 <= nt; q += 16) {
+      double2 o[16];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) o[u] = col[(size_t)(q + u) * M];
+      for (int u = 0; u < 16; ++u) o[u] = col[(size_t)(q + u) * M];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < 16; ++u) {
         t.x += o[u].x;
         t.y += o[u].y;
       }

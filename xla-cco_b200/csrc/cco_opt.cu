@@ -242,6 +242,7 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
   const bool fail = outcome == LS_FAIL;
   const double Rs = L.R;
   const double f_old = L.f;
+  double ss_acc = 0.0;   // this thread's part of |g|^2 when the point moves
   __syncthreads();
   if (!fail) {
     const bool probe = outcome == LS_ACCEPT_PROBE;
@@ -264,6 +265,7 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
           st2(x, e, xn);
           st2(s, e, make_double2(xn.x / Rs, xn.y / Rs));
           st2(g, e, gn);
+          ss_acc += gn.x * gn.x + gn.y * gn.y;   // |g|^2, words in the same order as below
         });
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -277,12 +279,14 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
     L.last_step = L.alpha;
   }
   __syncthreads();
-  // |g_s| = |g_x| R
-  double ss = 0.0;
-  for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-    const double2 gv = ld2(g, e);
-    ss += gv.x * gv.x + gv.y * gv.y;
-  }
+  // |g_s| = |g_x| R; an accepted point summed its new g while storing it
+  // (thread t over the words t, t + blockDim.x, ... in both cases)
+  double ss = ss_acc;
+  if (fail)
+    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
+      const double2 gv = ld2(g, e);
+      ss += gv.x * gv.x + gv.y * gv.y;
+    }
   ss = block_sum(ss, sh.red);
   if (threadIdx.x == 0) {
     L.stag = (L.f < f_old) ? 0 : L.stag + 1;
