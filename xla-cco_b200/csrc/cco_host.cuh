@@ -268,7 +268,7 @@ struct Schedule {
   // FP64-bound evaluation of another frees them
   int overlap = 0;
 };
-constexpr int kMaxBranches = 4;
+constexpr int kMaxBranches = 8;
 constexpr int kInflight = 3;    // graphs in flight before the host checks completion
 constexpr int kMaxInflight = 16;   // CCO_INFLIGHT bound (and the round bounds' slack)
 

@@ -262,14 +262,15 @@ void LaneTable::release(cudaStream_t st) {
 // ------------------------------------------------------------ the tick driver
 namespace {
 
-// Candidate schedules of the online tuner: branch counts 1..4. (The overlap
-// form, CCO_OVERLAP=1, measured slower than plain branches on the 256-lane
-// d = 2 relax - 906 vs 955 relaxations/s at two branches - and is not a
-// candidate.)
+// Candidate schedules of the online tuner: 1, 2, 3, 4, 6 or 8 branches of
+// at least 8 lanes. (On the 256-lane d = 2 relax: 260, 268, 254 and 256 ms
+// per relaxation at 3, 4, 6 and 8 branches. The overlap form, CCO_OVERLAP=1,
+// measured slower than plain branches - 906 vs 955 relaxations/s at two
+// branches - and is not a candidate.)
 std::vector<Schedule> candidates(int B) {
   std::vector<Schedule> c;
-  for (int nb = 1; nb <= kMaxBranches; ++nb) {
-    if (nb > 1 && B / nb < 8) break;
+  for (int nb : {1, 2, 3, 4, 6, 8}) {
+    if (nb > kMaxBranches || (nb > 1 && B / nb < 8)) break;
     Schedule s;
     s.branches = nb;
     s.graph_ticks = 16;
