@@ -595,6 +595,10 @@ struct EvalWS {
       plan.d_off2[D] = D >= p->d ? plan.n_items2 : 0;
       plan.d_offG[D] = D >= p->d ? plan.n_itemsG : 0;
     }
+    // one problem: its GEMM items are all of its window width
+    for (int D = 2; D <= 3; ++D)
+      for (int c = 0; c <= kGemmFoldMaxCq; ++c)
+        plan.q_offG[D - 2][c] = (D == p->d && c >= p->host.gcq) ? plan.n_itemsG : 0;
     plan.smemG = p->smemG;
     plan.dyn_prec = prec == PREC_FP32 ? 1 : 0;
     plan.max_d = p->d;

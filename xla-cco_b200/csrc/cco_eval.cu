@@ -41,20 +41,43 @@ namespace cco {
 
 namespace {
 
-template <int D>
+// One kernel per (dimension, window width): each holds one body, so the
+// instruction cache serves one folded product loop.
+template <int D, int CQ>
 __global__ void __launch_bounds__(kGemmThreads, 4) k_pass1_gemm(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
-  const EvalItem it = plan.itemsG[plan.d_offG[D - 1] + blockIdx.x];
+  const EvalItem it = plan.itemsG[plan.q_offG[D - 2][CQ - 1] + blockIdx.x];
   const EvalLane ln = plan.lanes[it.lane];
   if (!lane_active(ln.status)) return;
   if (plan.dyn_prec && lane_prec(ln) == PREC_FP32) return;   // the FP32 body handles it
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
   if constexpr (D == 2)
-    pass1_gemm_d2(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
+    pass1_gemm_body_d2<CQ>(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
   else
-    pass1_gemm_d3(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
+    pass1_gemm_body<D, CQ>(sp, ln, it.tile / sp.ngblk, it.tile % sp.ngblk, smem);
+}
+
+template <int D>
+void launch_gemm(const EvalPlan& plan, cudaStream_t s) {
+  const int* q = plan.q_offG[D - 2];
+  if (q[1] > q[0]) k_pass1_gemm<D, 1><<<q[1] - q[0], kGemmThreads, plan.smemG, s>>>(plan);
+  if (q[2] > q[1]) k_pass1_gemm<D, 2><<<q[2] - q[1], kGemmThreads, plan.smemG, s>>>(plan);
+  if (q[3] > q[2]) k_pass1_gemm<D, 3><<<q[3] - q[2], kGemmThreads, plan.smemG, s>>>(plan);
+}
+
+template <int D>
+cudaError_t configure_gemm() {
+  cudaError_t e = cudaFuncSetAttribute(k_pass1_gemm<D, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       227 * 1024 - 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_pass1_gemm<D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024 - 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_pass1_gemm<D, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024 - 1024);
+  return e;
 }
 
 // One kernel per dimension D and arithmetic keeps each kernel's code small:
@@ -260,11 +283,8 @@ void launch_d(const EvalPlan& plan, bool pass2, cudaStream_t stream) {
 }  // namespace
 
 cudaError_t eval_configure() {
-  cudaError_t e = cudaFuncSetAttribute(k_pass1_gemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       227 * 1024 - 1024);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_pass1_gemm<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             227 * 1024 - 1024);
+  cudaError_t e = configure_gemm<2>();
+  if (e == cudaSuccess) e = configure_gemm<3>();
   if (e == cudaSuccess) e = configure_d<1, false>();
   if (e == cudaSuccess) e = configure_d<2, false>();
   if (e == cudaSuccess) e = configure_d<3, false>();
@@ -286,13 +306,11 @@ void launch_dim(const EvalPlan& plan, bool pass2, int D, cudaStream_t s) {
   } else if (D == 2) {
     launch_d<2, false>(plan, pass2, s);
     if (plan.dyn_prec) launch_d<2, true>(plan, pass2, s);
-    const int n = plan.d_offG[2] - plan.d_offG[1];
-    if (!pass2 && n > 0) k_pass1_gemm<2><<<n, kGemmThreads, plan.smemG, s>>>(plan);
+    if (!pass2) launch_gemm<2>(plan, s);
   } else {
     launch_d<3, false>(plan, pass2, s);
     if (plan.dyn_prec) launch_d<3, true>(plan, pass2, s);
-    const int n = plan.d_offG[3] - plan.d_offG[2];
-    if (!pass2 && n > 0) k_pass1_gemm<3><<<n, kGemmThreads, plan.smemG, s>>>(plan);
+    if (!pass2) launch_gemm<3>(plan, s);
   }
 }
 

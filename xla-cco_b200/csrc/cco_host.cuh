@@ -174,7 +174,8 @@ struct EvalSet {
     std::vector<const cco_problem*> uniq;
     std::vector<ProbDev> pv;
     std::vector<EvalLane> lv;
-    std::vector<EvalItem> g1[3], g2[3], gG[3];   // items grouped by d
+    std::vector<EvalItem> g1[3], g2[3];   // items grouped by d
+    std::vector<EvalItem> gG[3][kGemmFoldMaxCq];   // GEMM items by d and window width
     size_t smem1 = 0, smem2 = 0, smem2f = 0, smemG = 0;
     int max_d = 1, max_m = 1;
     for (int i = lo; i < hi; ++i) {
@@ -195,7 +196,7 @@ struct EvalSet {
       lv.push_back(eval_lane(R, refs[i], p, u));
       if (p->host.gemm) {
         const int ntG = p->host.ntile1 * p->host.ngblk;
-        for (int t = 0; t < ntG; ++t) gG[p->d - 1].push_back(EvalItem{j, t});
+        for (int t = 0; t < ntG; ++t) gG[p->d - 1][p->host.gcq - 1].push_back(EvalItem{j, t});
       }
       // the per-segment pass 1: FP32 lanes, and problems without the GEMM form
       if (!p->host.gemm || may_fp32) {
@@ -210,7 +211,11 @@ struct EvalSet {
     for (int D = 0; D < 3; ++D) {
       i1.insert(i1.end(), g1[D].begin(), g1[D].end());
       i2.insert(i2.end(), g2[D].begin(), g2[D].end());
-      iG.insert(iG.end(), gG[D].begin(), gG[D].end());
+      for (int c = 0; c < kGemmFoldMaxCq; ++c) {
+        if (D >= 1) plan.q_offG[D - 1][c] = (int)iG.size();
+        iG.insert(iG.end(), gG[D][c].begin(), gG[D][c].end());
+      }
+      if (D >= 1) plan.q_offG[D - 1][kGemmFoldMaxCq] = (int)iG.size();
       plan.d_off1[D + 1] = (int)i1.size();
       plan.d_off2[D + 1] = (int)i2.size();
       plan.d_offG[D + 1] = (int)iG.size();

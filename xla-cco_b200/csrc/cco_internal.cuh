@@ -198,6 +198,9 @@ struct EvalPlan {
   const EvalItem* itemsG;   // GEMM pass-1 items (lane, tile * ngblk + block), grouped by d
   int n_itemsG;
   int d_offG[4];
+  // within dimension D's GEMM items (D = 2, 3): those of window width 16 cq at
+  // [q_offG[D - 2][cq - 1], q_offG[D - 2][cq]) (one kernel per (D, cq))
+  int q_offG[2][kGemmFoldMaxCq + 1];
   size_t smemG;
   int dyn_prec;             // 1: lanes may be FP32 (the FP32 pass kernels launch too), 0: FP64 only
   int max_d;                // largest d in the plan (template dispatch)
@@ -247,7 +250,8 @@ inline int eval_kernels(const EvalPlan& p) {
   const int per = p.dyn_prec ? 2 : 1;   // FP64 and FP32 pass kernels
   for (int D = 1; D <= 3; ++D) {
     n += per * (p.d_off1[D] > p.d_off1[D - 1]);
-    n += p.d_offG[D] > p.d_offG[D - 1];
+    if (D >= 2)
+      for (int c = 0; c < kGemmFoldMaxCq; ++c) n += p.q_offG[D - 2][c + 1] > p.q_offG[D - 2][c];
     if (p.want_grad) n += per * (p.d_off2[D] > p.d_off2[D - 1]);
   }
   return n;
