@@ -331,7 +331,7 @@ def test_small_descent_lanes_run_in_one_persistent_launch():
             assert torch.equal(one[k][0], out[k][i]), (i, k)
 
 
-@pytest.mark.parametrize("branches,overlap", [(1, 0), (2, 0), (2, 1), (3, 1)])
+@pytest.mark.parametrize("branches,overlap", [(1, 0), (2, 0), (2, 1), (3, 1), (6, 0)])
 def test_tick_schedules_give_the_same_bits(monkeypatch, branches, overlap):
     """Every tick schedule the tuner may pick - one graph branch, several, and
     the overlap form (branches half a tick apart, update kernels at high stream
