@@ -736,7 +736,7 @@ def run_serve(args) -> None:
         r.energy.problem_handle(0, r.n)
     settings = LBFGSSettings(energy_tol=TOL, precision=args.serve_precision)
     sampler = ClockSampler(0)
-    with RelaxServer(settings, hbm_budget_bytes=150 << 30) as srv:
+    with RelaxServer(settings, hbm_budget_bytes=150 << 30, branches=args.serve_branches) as srv:
         # warm-up: a few requests through the pool before the stream starts
         for t in [srv.submit(r.energy, r.s0) for r in reqs[: args.warmup]]:
             srv.result(t)
@@ -1088,6 +1088,8 @@ def main() -> None:
     ap.add_argument("--precision-batch", type=int, default=64)
     ap.add_argument("--serve-precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-branches", type=int, default=0,
+                    help="graph branches of the serving pool (0: its own choice by live lanes)")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)
