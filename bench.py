@@ -1008,6 +1008,42 @@ def run_cli(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def kernel_timeline(call, n: int, d: int, batch: int) -> dict:
+    """Kernel records (CUPTI, through torch.profiler) of one relaxation call:
+    µs per launch per kernel, the span from the first kernel's start to the
+    last one's end, and the time at least one kernel ran, per tick."""
+    import re
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        out = call()
+        torch.cuda.synchronize()
+    rec = sorted((e.time_range.start, e.time_range.end, e.name) for e in prof.events()
+                 if e.device_type == torch.autograd.DeviceType.CUDA)  # fmt: skip
+    per: dict = {}
+    for t0, t1, name in rec:
+        m = re.search(r"(k_\w+|Memcpy \w+)(<[^>]*>)?", name)
+        key = m.group(0) if m else name[:40]
+        c = per.setdefault(key, [0, 0.0])
+        c[0] += 1
+        c[1] += t1 - t0
+    busy, cs, ce = 0.0, rec[0][0], rec[0][1]
+    for t0, t1, _ in rec[1:]:
+        if t0 > ce:
+            busy += ce - cs
+            cs, ce = t0, t1
+        else:
+            ce = max(ce, t1)
+    busy += ce - cs
+    ticks = max(int(out["ticks"]), 1)
+    return {"profile": "timeline", "n": n, "d": d, "batch": batch, "ticks": ticks,
+            "span_us_per_tick": (rec[-1][1] - rec[0][0]) / ticks, "busy_us_per_tick": busy / ticks,
+            "us_per_launch": {k: round(v[1] / v[0], 2)
+                              for k, v in sorted(per.items(), key=lambda kv: -kv[1][1])}}  # fmt: skip
+
+
 def run_profile(args) -> None:
     """Kernel-level profiling driver (run under ncu).
     --profile-shape N,d,chi profiles another system than the headline one.
@@ -1043,6 +1079,14 @@ def run_profile(args) -> None:
         tf = args.batch * n * m * F_PAIR[d] / (ms * 1e-3) / 1e12
         print(json.dumps({"profile": "eval", "n": n, "d": d, "m": m, "batch": args.batch,
                           "ms_per_eval": ms, "tflops": tf}), flush=True)
+    elif args.timeline:
+        # CUPTI kernel records of one relaxation (after one untimed run):
+        # per-kernel time per launch and the device's busy share of the span
+        settings = LBFGSSettings(energy_tol=TOL, max_evals_per_pass=args.timeline_evals)
+        relax_device(energy, s_dev, settings)
+        torch.cuda.synchronize()
+        print(json.dumps(kernel_timeline(lambda: relax_device(energy, s_dev, settings), n, d,
+                                         args.batch)), flush=True)
     else:
         for _ in range(args.reps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -1073,6 +1117,10 @@ def main() -> None:
                     help="profiling driver for ncu: run the kernels only")  # fmt: skip
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--profile-shape", default=None, help="N,d,chi of the profiled system")
+    ap.add_argument("--timeline", action="store_true",
+                    help="relax profiling: CUPTI kernel records of one relaxation (torch.profiler)")
+    ap.add_argument("--timeline-evals", type=int, default=300,
+                    help="max_evals_per_pass of the --timeline relaxation")
     ap.add_argument("--md-lanes", type=int, default=64)
     ap.add_argument("--md-steps", type=int, default=2000)
     ap.add_argument("--workload", choices=["batch", "descent", "mixed", "serve", "precision", "md", "analysis",

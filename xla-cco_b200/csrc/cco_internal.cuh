@@ -52,7 +52,7 @@ static_assert(sizeof(SegHdr) == 32, "segment header is two 16-byte loads");
 // group's folded range is cut into windows of 16 cq columns (cq per problem,
 // 1..kGemmFoldMaxCq); a (group, window) is a block, one CTA per (lane, tile,
 // block).
-constexpr int kGemmRows = 24, kGemmChunk = 16, kGemmThreads = 128;
+constexpr int kGemmRows = 24, kGemmChunk = 32, kGemmThreads = 128;
 constexpr int kGemmFoldMaxCq = 3;
 // odd row stride of the last-axis table: table writes spread over banks
 __host__ __device__ constexpr int gemm_fold_zstride(int cq) { return 16 * cq + 1; }

@@ -508,9 +508,23 @@ __global__ void __launch_bounds__(kUpdThreads, 2) k_lbfgs_probe(LbArgs A) {
     // one probe of the line search
     const double Rs = L.R;
     double dp = 0.0;
-    for (int e = threadIdx.x; e < h2; e += blockDim.x) {
-      const double2 pv = ld2(v.pg, e), dv = ld2(v.dir, e);
-      dp += (pv.x / Rs) * dv.x + (pv.y / Rs) * dv.y;
+    {
+      // eight words per thread in flight, added in the order of a one-word loop
+      constexpr int U = 8;
+      for (int e0 = threadIdx.x; e0 < h2; e0 += U * blockDim.x) {
+        double2 pv[U], dv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int e = e0 + u * (int)blockDim.x;
+          if (e < h2) {
+            pv[u] = ld2(v.pg, e);
+            dv[u] = ld2(v.dir, e);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (e0 + u * (int)blockDim.x < h2) dp += (pv[u].x / Rs) * dv[u].x + (pv[u].y / Rs) * dv[u].y;
+      }
     }
     dp = block_sum(dp, sh.red);
     if (threadIdx.x == 0) {
