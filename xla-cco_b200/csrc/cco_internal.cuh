@@ -217,10 +217,12 @@ struct EvalPlan {
 // 2 kPass1ChunkSegs segments are split, where one thread already owns one
 // segment (no in-CTA particle slices), so every segment's sum is computed
 // exactly as unsplit: the chunking changes where the work runs, not the bits.
+// A tile is cut into no more chunks than it takes to give each thread of a
+// 128-thread CTA one segment (ceil(nseg / 128)).
 constexpr int kPass1ChunkSegs = 128;
 __host__ __device__ __forceinline__ int pass1_chunks(const ProbDev& p, int plan_chunks) {
   if (p.nseg1 < 2 * kPass1ChunkSegs) return 1;
-  const int most = p.nseg1 / kPass1ChunkSegs;
+  const int most = (p.nseg1 + kPass1ChunkSegs - 1) / kPass1ChunkSegs;
   return plan_chunks < most ? plan_chunks : most;
 }
 
