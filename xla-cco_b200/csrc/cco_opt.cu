@@ -731,7 +731,9 @@ __global__ void __launch_bounds__(kUpdThreads) k_lbfgs_scalar(LbArgs A) {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int t = t0 + u * blockDim.x;
-        int q = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+        // row of packed index t: an FP32 estimate, made exact by the two
+        // integer corrections below (t < m (m + 1) / 2 is far below 2^24)
+        int q = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
         while (q * (q + 1) / 2 > t) --q;
         while ((q + 1) * (q + 2) / 2 <= t) ++q;
         const int p = t - q * (q + 1) / 2;
