@@ -150,10 +150,8 @@ __global__ void __launch_bounds__(kReduceChunk) k_reduce(EvalPlan plan) {
   if (threadIdx.x == 0) ln.part[k0] = make_double2(e, 0.0);
 }
 
-// Energy (one warp per lane): the chunk energies summed in a fixed order.
-__global__ void k_energy(EvalPlan plan) {
-  const EvalLane ln = plan.lanes[blockIdx.x];
-  if (!lane_active(ln.status)) return;
+// Energy of one lane (one warp): the chunk energies summed in a fixed order.
+__device__ __forceinline__ void lane_energy(const EvalPlan& plan, const EvalLane& ln) {
   const ProbDev& P = plan.probs[ln.prob];
   const int nc = reduce_chunks(P.M);
   double e = 0.0;
@@ -163,14 +161,25 @@ __global__ void k_energy(EvalPlan plan) {
   if (threadIdx.x == 0) *ln.f = e / P.vol;
 }
 
+// Energy-only evaluations (no pass 2): one warp per lane. With the gradient,
+// the first warp of each lane's first pass-2 tile sums it instead (one launch
+// fewer per evaluation, the same sum).
+__global__ void k_energy(EvalPlan plan) {
+  const EvalLane ln = plan.lanes[blockIdx.x];
+  if (!lane_active(ln.status)) return;
+  lane_energy(plan, ln);
+}
+
 template <int D, bool F32>
 __global__ void __launch_bounds__(kPass2Threads, 4) k_pass2(EvalPlan plan) {
   extern __shared__ double2 smem[];
   __shared__ ProbDev sp;
   const EvalItem it = plan.items2[plan.d_off2[D - 1] + blockIdx.x];
   const EvalLane ln = plan.lanes[it.lane];
-  if (!lane_active(ln.status) || ln.g == nullptr) return;
+  if (!lane_active(ln.status)) return;
   if ((lane_prec(ln) == PREC_FP32) != F32) return;   // the other kernel's lane
+  if (it.tile == 0 && threadIdx.x < 32) lane_energy(plan, ln);
+  if (ln.g == nullptr) return;
   if (threadIdx.x == 0) sp = plan.probs[ln.prob];
   __syncthreads();
   if (D == 1 && !F32) {
@@ -361,7 +370,7 @@ cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream, const EvalSid
   if (e != cudaSuccess) return e;
   if (plan.n_lanes > 0) {
     k_reduce<<<dim3(plan.red_chunks, plan.n_lanes), kReduceChunk, 0, stream>>>(plan);
-    k_energy<<<plan.n_lanes, 32, 0, stream>>>(plan);
+    if (!plan.want_grad) k_energy<<<plan.n_lanes, 32, 0, stream>>>(plan);
   }
   if (plan.want_grad) {
     e = launch_pass_all(plan, true, stream, side);

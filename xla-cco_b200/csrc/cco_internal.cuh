@@ -246,9 +246,10 @@ struct EvalSide {
 cudaError_t eval_launch(const EvalPlan& plan, cudaStream_t stream,
                         const EvalSide* side = nullptr);
 // Kernels one eval_launch of a plan issues: per dimension the per-segment and
-// GEMM pass-1 kernels and the pass-2 kernel that have items, plus reduce and energy.
+// GEMM pass-1 kernels and the pass-2 kernel that have items, plus the reduction (and
+// the energy kernel when there is no pass 2).
 inline int eval_kernels(const EvalPlan& p) {
-  int n = p.n_lanes > 0 ? 2 : 0;
+  int n = p.n_lanes > 0 ? (p.want_grad ? 1 : 2) : 0;   // reduce (+ energy without pass 2)
   const int per = p.dyn_prec ? 2 : 1;   // FP64 and FP32 pass kernels
   for (int D = 1; D <= 3; ++D) {
     n += per * (p.d_off1[D] > p.d_off1[D - 1]);
