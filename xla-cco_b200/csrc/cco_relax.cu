@@ -297,41 +297,60 @@ int64_t* pinned_status(size_t count) {
   return buf;
 }
 
-// Online tuning: one graph per candidate on the live lanes C, timed with
+// Online tuning: graphs of each candidate on the live lanes C, timed with
 // events, then the fastest per tick. Every candidate advances every lane by
 // the same ticks, so results do not depend on which schedule wins.
 int tune_schedule(const LaneTable& C, cudaStream_t st, int64_t max_ticks, int64_t* ticks,
                   int64_t* launches, Schedule* out) {
+  // Two rounds, the second in reverse order, each candidate timed once per
+  // round: the lanes' work drifts while they advance (histories fill, rescale
+  // passes restart them), and the mean of a forward and a backward visit
+  // cancels a drift that is linear in time.
   const std::vector<Schedule> cand = candidates((int)C.refs.size());
-  std::vector<cudaEvent_t> t0(cand.size(), nullptr), t1(cand.size(), nullptr);
-  std::vector<float> ms(cand.size(), 1e30f);
+  const size_t nc = cand.size();
+  std::vector<cudaEvent_t> t0(2 * nc, nullptr), t1(2 * nc, nullptr);
+  std::vector<int> ran(2 * nc, 0);
   int rc = CCO_OK;
   cudaError_t e = cudaSuccess;
-  for (size_t c = 0; c < cand.size() && e == cudaSuccess; ++c) {
+  for (size_t c = 0; c < 2 * nc && e == cudaSuccess; ++c) {
     e = cudaEventCreate(&t0[c]);
     if (e == cudaSuccess) e = cudaEventCreate(&t1[c]);
   }
-  for (size_t c = 0; c < cand.size() && rc == CCO_OK && e == cudaSuccess && *ticks < max_ticks; ++c) {
+  for (size_t v = 0; v < 2 * nc && rc == CCO_OK && e == cudaSuccess && *ticks < max_ticks; ++v) {
+    const size_t c = v < nc ? v : 2 * nc - 1 - v;
     TickPlan P;
     P.method = C.shape.method;
     rc = P.build(C, cand[c], st);
     if (rc != CCO_OK) break;
-    e = cudaEventRecord(t0[c], st);
+    e = cudaEventRecord(t0[v], st);
     if (e == cudaSuccess) e = cudaGraphLaunch(P.exec, st);
-    if (e == cudaSuccess) e = cudaEventRecord(t1[c], st);
+    if (e == cudaSuccess) e = cudaEventRecord(t1[v], st);
+    ran[v] = e == cudaSuccess;
     *ticks += cand[c].graph_ticks;
     *launches += (int64_t)cand[c].graph_ticks * P.launches_per_tick();
     P.release(st);
   }
   if (rc == CCO_OK && e == cudaSuccess) e = cudaStreamSynchronize(st);
+  std::vector<float> sum(nc, 0.f);
+  std::vector<int> cnt(nc, 0);
+  for (size_t v = 0; v < 2 * nc && e == cudaSuccess && rc == CCO_OK; ++v) {
+    if (!ran[v]) continue;
+    const size_t c = v < nc ? v : 2 * nc - 1 - v;
+    float x = 0.f;
+    if (cudaEventElapsedTime(&x, t0[v], t1[v]) == cudaSuccess) {
+      sum[c] += x / cand[c].graph_ticks;
+      cnt[c] += 1;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  std::vector<float> ms(nc, 1e30f);
   int best = 0;
-  for (size_t c = 0; c < cand.size() && e == cudaSuccess && rc == CCO_OK; ++c) {
-    float v = 0.f;
-    if (cudaEventElapsedTime(&v, t0[c], t1[c]) == cudaSuccess) ms[c] = v / cand[c].graph_ticks;
-    else cudaGetLastError();
+  for (size_t c = 0; c < nc; ++c) {
+    if (cnt[c] > 0) ms[c] = sum[c] / cnt[c];
     if (ms[c] < ms[best]) best = (int)c;
   }
-  for (size_t c = 0; c < cand.size(); ++c) {
+  for (size_t c = 0; c < 2 * nc; ++c) {
     if (t0[c]) cudaEventDestroy(t0[c]);
     if (t1[c]) cudaEventDestroy(t1[c]);
   }
