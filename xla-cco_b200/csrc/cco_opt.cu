@@ -254,7 +254,7 @@ __device__ void lb_end_iteration(const LbArgs& A, int lane, const LaneRef& R, co
       double2 xo, dv, go, gn;
     };
     const double* gsrc = probe ? v.pg : v.glo;
-    lb_words<2>(
+    lb_words<4>(
         h2,
         [&](int e) { return Words{ld2(x, e), ld2(v.dir, e), ld2(g, e), ld2(gsrc, e)}; },
         [&](int e, const Words& w) {
